@@ -1,0 +1,295 @@
+#!/usr/bin/env python
+"""Benchmark of the NSGA-III generation hot path on B200.
+
+Workload (the configuration the headline metric is quoted on): NSGA-III on
+DTLZ1, M=3 objectives, D=7 FP32 variables, population N=32768 (merged 65536),
+Das-Dennis directions with H=254 partitions (32640 directions), SBX eta=30
+pc=1, polynomial mutation eta=20 pm=1/D, tournament mating.  Synthetic data:
+the initial population is drawn uniformly in [0,1]^D from the seed.
+
+One step = one generation (mating, SBX+PM, DTLZ1 evaluation, environmental
+selection).  Every step is timed with CUDA events on the algorithm's stream;
+between timed steps the L2 cache is flushed by writing a 256 MiB buffer
+(outside the timed intervals).  Multi-GPU: one independent replica per GPU
+(the path does not shard), value = total generations/s,
+max-over-ranks time.
+
+`--impl reference` times the CPU restatement of the reference path (oracle/)
+on the host cores, same metric and workload (the reference itself has no CPU
+implementation and no B200 build of its own GPU path runs here unmodified).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "cuda-moea_b200"))
+sys.path.insert(0, str(ROOT))
+
+METRIC = "NSGA-III gen/s @N=32768,M=3; batched instance-gen/s vs plain, identical ranks"
+WORKLOAD = "NSGA-III DTLZ1 M=3 D=7 N=32768, Das-Dennis H=254 (32640 directions), 1 generation per step"
+N_POP, D_VAR, M_OBJ, PARTITIONS = 32768, 7, 3, 254
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_generation_time(n: int, threads: int, seed: int = 1):
+    """One CPU generation of the restated reference path (oracle, OpenMP)."""
+    import numpy as np
+    from oracle import oracle as O
+    O.build()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    rng = np.random.default_rng(seed)
+    x = rng.random((n, D_VAR)).astype(np.float32)
+    f, cv = O.evaluate("DTLZ1", x, M_OBJ)
+    refs = O.reference_directions(1, PARTITIONS, M_OBJ)
+    bounds = np.tile([0.0, 1.0], D_VAR).astype(np.float32)
+    fronts, _ = O.ndsort(cv, f, n)
+    ideal = f.min(1).astype(np.float32)
+    t0 = time.perf_counter()
+    seed64 = O.derive_seed(2887)
+    mate = O.philox_stream(seed64, 0, 2, n)
+    cand = np.stack([mate[:, 0] % n, mate[:, 1] % n], 1).astype(np.int32)
+    pidx = O.tournament(cand, fronts, cv)
+    cx = O.philox_stream(seed64, 0, 3, (n // 2) * D_VAR)
+    unit = lambda u: (u >> 8).astype(np.float32) * np.float32(1.0 / 16777216.0)
+    off = O.sbx(x, pidx, bounds, np.stack([unit(cx[:, 0]), unit(cx[:, 1])], 1),
+                (cx[:, 2] & 1).astype(np.int32), unit(cx[:, 3]), 30.0, 1.0, 0.0, n)
+    mu = O.philox_stream(seed64, 0, 4, n * D_VAR // 2)
+    um = np.stack([unit(mu[:, 0]), unit(mu[:, 1]), unit(mu[:, 2]), unit(mu[:, 3])], 1).reshape(-1, 2)
+    off = O.pm(off, bounds, um[: n * D_VAR], 20.0, 1.0)
+    of, ocv = O.evaluate("DTLZ1", off, M_OBJ)
+    O.nsga3_select(np.concatenate([cv, ocv]), np.concatenate([f, of], 1), refs, seed64, 0, ideal)
+    return time.perf_counter() - t0
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    budget = float(os.environ.get("MOEA_REFERENCE_BUDGET_S", "150"))
+    times = [cpu_generation_time(N_POP, threads, seed=1)]
+    while len(times) < args.steps and sum(times) + times[0] < budget:
+        times.append(cpu_generation_time(N_POP, threads, seed=len(times) + 1))
+    total = sum(times)
+    value = len(times) / total
+    sample = (f"{len(times)} full generation(s) of the workload on the CPU oracle "
+              f"(OpenMP, {threads} threads); warm-up skipped; time-boxed to {budget:.0f} s")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "gen/s",
+        "n_gpus": args.gpus, "steps": len(times), "warmup": 0,
+        "ms_per_step": 1000.0 * total / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "population": N_POP, "directions": 32640,
+                   "device": "host CPU"},
+        "cpu_baseline": {"value": value, "unit": "gen/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "gen/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--population", type=int, default=N_POP)
+    ap.add_argument("--seed", type=int, default=2887)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=40.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    import torch.distributed as dist
+    import cuda_moea as cm
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    N = args.population
+    gens = args.warmup + args.steps + 1 + args.steps + 1
+    algo = cm.NSGA3(population_size=N, max_generations=gens, problem=cm.DTLZ1(D_VAR, M_OBJ),
+                    reference_directions=cm.DasDennisDirections(PARTITIONS), seed=args.seed + rank,
+                    print_progress=False, device=local)
+    stream = torch.cuda.current_stream()
+    algo.initialize()
+    for _ in range(args.warmup):
+        algo.step()
+    torch.cuda.synchronize()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    # ---- timed region: device time of K generations
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for e0, e1 in events:
+            flush.fill_(1)
+            e0.record(stream)
+            algo.step()
+            e1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    total_ms = sum(e0.elapsed_time(e1) for e0, e1 in events)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * args.steps / (max_ms / 1000.0)
+    graph_on, kernels = algo.graph_info
+
+    # ---- end to end through the public API: host population in, results out
+    pop = algo.population
+    h_vars = torch.empty((N, D_VAR), dtype=torch.float32, pin_memory=True)
+    h_vars.copy_(pop.variables)
+    h_objs = torch.empty((N, M_OBJ), dtype=torch.float32, pin_memory=True)
+    h_cv = torch.empty(N, dtype=torch.float32, pin_memory=True)
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for e0, e1 in ev2:
+        flush.fill_(1)
+        e0.record(stream)
+        p = algo.population_view()
+        p.variables.copy_(h_vars, non_blocking=True)
+        algo.step()
+        p = algo.population_view()
+        h_objs.copy_(p.objectives, non_blocking=True)
+        h_cv.copy_(p.constraints, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        h_vars.copy_(p.variables)
+    e2e_ms = sum(e0.elapsed_time(e1) for e0, e1 in ev2)
+    t2 = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps / (float(t2.item()) / 1000.0)
+
+    # ---- per-stage device times of one generation (direct launches, events)
+    stages = algo.profile_step()
+    stage_ms = {}
+    for name, ms in stages:
+        stage_ms[name] = stage_ms.get(name, 0.0) + ms
+    n_mix = 2 * N
+    dom_ms = stage_ms.get("ndsort.dominance_tiles", float("nan"))
+    # algorithmic bytes of the dominance stage: the relation of the lower
+    # triangle, one bit per ordered pair (p before q), written once
+    dom_bytes = n_mix * (n_mix - 1) / 2 / 8
+    hbm, peak_kind = _peaks()
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms == dom_ms else None
+    pair_rate = (n_mix * n_mix) / (dom_ms / 1e3) if dom_ms == dom_ms else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        t_cpu = cpu_generation_time(N, threads)
+        cpu = {"value": 1.0 / t_cpu, "unit": "gen/s", "cores": threads, "kind": "port",
+               "sample": f"1 full generation of the workload on the CPU oracle (OpenMP, {threads} threads)"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "gen/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "population": N, "merged": n_mix, "directions": 32640,
+                       "l2": "flushed (256 MiB write) before every timed generation",
+                       "parallelism": f"replicas x{world}", "cuda_graph": graph_on},
+            "clocks": clocks.summary(),
+            "e2e": {"value": e2e_value, "unit": "gen/s",
+                    "h2d_bytes_per_step": N * D_VAR * 4, "d2h_bytes_per_step": N * (M_OBJ + 1) * 4},
+            "gpu_launches": kernels * args.steps,
+            "stages_ms": stage_ms,
+            "roofline": {"kernel": "nds_tiles (dominance rows)", "bound": "hbm",
+                         "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": (achieved / hbm) if achieved else None, "peak_source": peak_kind,
+                         "traffic": None, "pair_tests_per_s": pair_rate},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

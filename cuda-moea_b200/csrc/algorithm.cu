@@ -1,0 +1,791 @@
+// The generational algorithm loop behind the NSGA3 / RVEA entry points.
+//
+// Reference: EvolutionaryAlgorithm (python/csrc/native/src/algorithm/algorithm.cu:104-432),
+// the strategy defaults of AlgorithmFactory (src/factory/algorithm_factory.cu:25-118),
+// NSGA3EnvironmentSelector (src/selection/nsga3/nsga3_environment_selector.cu) and
+// RVEAEnvironmentSelector (src/selection/rvea/rvea_environment_selector.cu).
+//
+// Differences in mechanism (not in results):
+//  - one stream; every per-generation quantity the reference keeps on the host
+//    (generation index, RVEA active count, niching RNG offset, APD penalty,
+//    constraint activation) lives in device memory, so a generation is a fixed
+//    sequence of launches with no host synchronisation and can be captured
+//    once into a CUDA graph per population-slot parity and replayed;
+//  - the merged parent+offspring population is never materialised (SplitPop);
+//  - buffers are allocated once at initialisation (no per-generation pool
+//    allocation, dynamic_workspace.cu:3-125).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace moea {
+
+int workspace_init(Workspace& ws, int device, int n_max, int m_max, int h_max);
+void workspace_free(Workspace& ws);
+int workspace_check_status(Workspace& ws, cudaStream_t stream);
+int run_nsga3_select(Workspace& ws, const SplitPop& pop, int M, int N, const float* refs, int H,
+                     uint64_t seed, float* ideal_last, int* survivors, int* survivor_fronts,
+                     int assoc_mode, cudaStream_t stream, const SplitPop* sort_pop);
+int run_quantize_cv(const float* cv, float* out, int n, float eps, float clip, float log_alpha,
+                    int bins, cudaStream_t stream);
+int run_problem(int kind, const float* x, int N, int D, int M, float* objs, float* cv,
+                cudaStream_t s);
+int validate_problem(int kind, int D, int M);
+int run_mating(const float* cv, const int* rank, const int* d_active, int active, int n_off,
+               uint64_t seed, const int* d_gen, uint32_t gen, int* pidx, cudaStream_t stream);
+int run_variation(const float* parents, const int* pidx, const float* bounds, float* off,
+                  int n_off, int D, float sbx_eta0, float sbx_eta1, float sbx_prob, float copy_prob,
+                  int mutate, float pm_eta0, float pm_eta1, float pm_prob, int total,
+                  uint64_t seed, const int* d_gen, uint32_t gen, cudaStream_t stream);
+int run_init_uniform(float* vars, const float* bounds, int N, int D, uint64_t seed,
+                     cudaStream_t stream);
+int run_rvea_translate(const SplitPop& pop, int M, float* t, int t_stride, float* zmin,
+                       cudaStream_t s);
+int run_rvea_partition(const float* t, int t_stride, int n, const float* refs, int M, int K,
+                       const int* d_active, int n_active, int n_parent, float* theta, int* idx,
+                       cudaStream_t s);
+int run_rvea_gamma(const float* refs, int M, int K, float* gamma, cudaStream_t s);
+int run_rvea_apd(const float* t, int t_stride, int n, const float* theta, const float* gamma,
+                 const int* idx, int M, int K, const float* ps_table, const int* d_gen,
+                 float ps_host, float* apd, cudaStream_t s);
+float rvea_penalty_scale(int M, int gen, int max_gen, float alpha);
+int run_rvea_elitism(Workspace& ws, const int* idx, const SplitPop& pop, const float* apd, int N,
+                     int K, int* survivors, int* d_active, cudaStream_t s);
+int run_rvea_update(const SplitPop& pop, const float* vars_a, const float* vars_b,
+                    const int* survivors, const int* d_active, int N, int D, int M, float* vars,
+                    float* objs, float* cv, cudaStream_t s);
+int run_rvea_adapt(const float* v0, const float* objs, int stride, const int* d_active,
+                   int n_active, int M, int K, float* range_tmp, float* v, cudaStream_t s);
+int das_dennis(int mode, int n, int M, std::vector<float>& out);
+int normalize_user_directions(std::vector<float>& v, int M, int count);
+
+namespace {
+
+__global__ void gather_next(const float* __restrict__ vars_a, const float* __restrict__ vars_b,
+                            SplitPop pop, const int* __restrict__ surv, const int* __restrict__ fronts,
+                            int N, int D, int M, float* __restrict__ vars, float* __restrict__ objs,
+                            float* __restrict__ cv, int* __restrict__ rank)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < (long long)N * D) {
+        const int r = (int)(e / D), d = (int)(e % D);
+        const int s = surv[r];
+        vars[e] = (s < pop.n_a) ? vars_a[(size_t)s * D + d] : vars_b[(size_t)(s - pop.n_a) * D + d];
+    }
+    if (e < N) {
+        const int r = (int)e;
+        const int s = surv[r];
+        for (int m = 0; m < M; ++m) objs[(size_t)m * N + r] = pop.obj(m, s);
+        cv[r] = pop.cvv(s);
+        if (rank) rank[r] = fronts[s];
+    }
+}
+
+__global__ void bump_generation(int* gen) { *gen += 1; }
+
+__global__ void zero_cv_if_inactive(float* cv, int n, const int* __restrict__ active_table,
+                                    const int* __restrict__ d_gen)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && !active_table[*d_gen]) cv[i] = 0.0f;
+}
+
+__global__ void zero_front_pick(const int* __restrict__ fronts, int n, int* __restrict__ flags)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flags[i] = fronts[i] == 0 ? 1 : 0;
+}
+
+template <class T>
+int dmalloc(T** p, size_t count)
+{
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * (count > 0 ? count : 1));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(e == cudaErrorMemoryAllocation ? MOEA_ERR_OUT_OF_MEMORY : MOEA_ERR_CUDA,
+                         "cudaMalloc: %s", cudaGetErrorString(e));
+    }
+    return MOEA_OK;
+}
+
+}  // namespace
+}  // namespace moea
+
+using namespace moea;
+
+struct moea_algorithm {
+    moea_algorithm_config cfg{};
+    std::vector<float> lower, upper, user_dirs, init_pop;
+    int N = 0, D = 0, M = 0, T = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    Workspace ws;
+    bool ws_ready = false;
+
+    float* vars[3] = {};
+    float* objs[3] = {};
+    float* cv[3] = {};
+    int* rank[3] = {};
+    float* cv_sort[2] = {};  // quantised violations of parents / offspring
+    int P = 0, O = 1, X = 2;
+    float* bounds = nullptr;
+    int* parent_idx = nullptr;
+    float* refs = nullptr;
+    float* refs0 = nullptr;
+    float* gamma = nullptr;
+    int H = 0;
+    float* ideal_last = nullptr;
+    bool ideal_ready = false;
+    int* d_gen = nullptr;
+    int* d_active = nullptr;
+    float* ps_table = nullptr;
+    int* cv_table = nullptr;
+    float* t_buf = nullptr;
+    float* theta = nullptr;
+    float* apd = nullptr;
+    int* part_idx = nullptr;
+    float* zmin = nullptr;
+    int* survivors = nullptr;
+    int* frontzero = nullptr;
+    int frontzero_count = 0;
+    uint64_t seed = 0;
+    uint32_t epoch = 0;
+    int generation = 0;
+    bool initialized = false;
+    double total_ms = 0.0;
+    int last_prepared_target = -2;
+    cudaGraphExec_t graph[2] = {};
+    bool graph_failed = false;
+    int graph_kernels = 0;
+
+    void drop_graphs()
+    {
+        for (auto& g : graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+
+    ~moea_algorithm() { release(); }
+
+    void release()
+    {
+        for (auto& g : graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        void* ptrs[] = {vars[0], vars[1], vars[2], objs[0], objs[1], objs[2], cv[0], cv[1], cv[2],
+                        rank[0], rank[1], rank[2], cv_sort[0], cv_sort[1], bounds, parent_idx, refs,
+                        refs0, gamma, ideal_last, d_gen, d_active, ps_table, cv_table, t_buf, theta,
+                        apd, part_idx, zmin, survivors, frontzero};
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+        std::memset(vars, 0, sizeof(vars));
+        std::memset(objs, 0, sizeof(objs));
+        std::memset(cv, 0, sizeof(cv));
+        std::memset(rank, 0, sizeof(rank));
+        cv_sort[0] = cv_sort[1] = nullptr;
+        bounds = refs = refs0 = gamma = ideal_last = ps_table = t_buf = theta = apd = zmin = nullptr;
+        parent_idx = d_gen = d_active = cv_table = part_idx = survivors = frontzero = nullptr;
+        if (ws_ready) { workspace_free(ws); ws_ready = false; }
+        if (own_stream && stream) { cudaStreamDestroy(stream); stream = nullptr; }
+    }
+
+    bool nsga3() const { return cfg.algorithm == MOEA_NSGA3; }
+    bool constrained() const { return cfg.problem_kind >= 9 && cfg.problem_kind <= 15; }
+
+    // MOEAStdTestEvaluator::is_cv_active (dtlz_kernels.cu:1302-1312)
+    bool cv_active(int eval_iter) const
+    {
+        if (cfg.constraint_activation_ratio <= 0.0f) return true;
+        if (eval_iter < 0 || T <= 0) return false;
+        const float progress = static_cast<float>(eval_iter + 1) / static_cast<float>(T);
+        return progress >= cfg.constraint_activation_ratio;
+    }
+    bool cv_switch_node(int target) const
+    {
+        if (target < 0 || last_prepared_target == target) return false;
+        if (target == 0) return cv_active(0);
+        return !cv_active(target - 1) && cv_active(target);
+    }
+
+    int evaluate(int slot, int gen_index)
+    {
+        if (cfg.problem_kind == 0) {
+            const int rc = cfg.evaluate(cfg.evaluate_user, vars[slot], objs[slot], cv[slot], N, D, M,
+                                        gen_index, T, (void*)stream);
+            if (rc != 0) return set_error(MOEA_ERR_CALLBACK, "problem evaluate callback failed (%d)", rc);
+            return MOEA_OK;
+        }
+        MOEA_TRY(run_problem(cfg.problem_kind, vars[slot], N, D, M, objs[slot], cv[slot], stream));
+        if (constrained() && cfg.problem_kind != 15 && !cv_active(gen_index))
+            MOEA_CUDA_TRY(cudaMemsetAsync(cv[slot], 0, sizeof(float) * N, stream));
+        return MOEA_OK;
+    }
+
+    // NSGA3EnvironmentSelector::prepare (nsga3_environment_selector.cu:236-287)
+    int prepare()
+    {
+        if (!nsga3()) return MOEA_OK;
+        const float* cvp = cv[P];
+        if (cfg.cv_bins > 0) {
+            MOEA_TRY(run_quantize_cv(cv[P], cv_sort[0], N, cfg.feasibility_epsilon, cfg.cv_clip_upper,
+                                     cfg.cv_log_alpha, cfg.cv_bins, stream));
+            cvp = cv_sort[0];
+        }
+        MOEA_TRY(run_ndsort(ws, merged_view(objs[P], cvp, N), M, N, rank[P], stream));
+        if (!ideal_ready) {
+            MOEA_TRY(run_ideal(objs[P], N, M, N, nullptr, ideal_last, stream));
+            ideal_ready = true;
+        }
+        return MOEA_OK;
+    }
+
+    int directions_init()
+    {
+        std::vector<float> host;
+        int count = 0;
+        if (cfg.directions == MOEA_DIRS_USER) {
+            if (!cfg.h_user_directions || cfg.user_direction_count < 1)
+                return set_error(MOEA_ERR_INVALID_ARGUMENT, "User directions must have shape (objective_count, count)");
+            count = cfg.user_direction_count;
+            host = user_dirs;
+            if (cfg.normalize_user_directions) MOEA_TRY(normalize_user_directions(host, M, count));
+        } else if (cfg.directions == MOEA_DIRS_ADAPTIVE) {
+            if (!(cfg.adapt_frequency > 0.0f && cfg.adapt_frequency <= 1.0f))
+                return set_error(MOEA_ERR_INVALID_ARGUMENT, "RVEA reference adaptation frequency must be in (0, 1]");
+            count = das_dennis(2, N, M, host);
+        } else {
+            count = das_dennis(cfg.partitions > 0 ? 1 : 0, cfg.partitions > 0 ? cfg.partitions : N, M, host);
+        }
+        if (count < 1) return set_error(MOEA_ERR_INVALID_ARGUMENT, "no reference directions for N=%d M=%d", N, M);
+        H = count;
+        MOEA_TRY(dmalloc(&refs, (size_t)M * H));
+        MOEA_TRY(dmalloc(&refs0, (size_t)M * H));
+        MOEA_TRY(dmalloc(&gamma, (size_t)H));
+        MOEA_CUDA_TRY(cudaMemcpyAsync(refs, host.data(), sizeof(float) * host.size(), cudaMemcpyHostToDevice, stream));
+        MOEA_CUDA_TRY(cudaMemcpyAsync(refs0, host.data(), sizeof(float) * host.size(), cudaMemcpyHostToDevice, stream));
+        MOEA_CUDA_TRY(cudaStreamSynchronize(stream));
+        if (!nsga3()) MOEA_TRY(run_rvea_gamma(refs, M, H, gamma, stream));
+        return MOEA_OK;
+    }
+
+    int validate()
+    {
+        if (cfg.population_size <= 0 || cfg.max_generations <= 0)
+            return set_error(MOEA_ERR_INVALID_ARGUMENT, "Algorithm requires positive population_size and max_generations");
+        if (cfg.algorithm != MOEA_NSGA3 && cfg.algorithm != MOEA_RVEA)
+            return set_error(MOEA_ERR_INVALID_ARGUMENT, "algorithm must be NSGA3 or RVEA");
+        if (cfg.dimension <= 0 || cfg.objectives <= 0)
+            return set_error(MOEA_ERR_INVALID_ARGUMENT, "Problem must provide positive dimensions");
+        if (cfg.objectives > kMaxObjectives)
+            return set_error(MOEA_ERR_UNSUPPORTED, "at most %d objectives are supported", kMaxObjectives);
+        if (cfg.problem_kind == 0 && !cfg.evaluate)
+            return set_error(MOEA_ERR_INVALID_ARGUMENT, "callback problem without an evaluate function");
+        if (cfg.problem_kind != 0) MOEA_TRY(validate_problem(cfg.problem_kind, cfg.dimension, cfg.objectives));
+        if (nsga3()) {
+            if (cfg.population_size % 2 != 0)
+                return set_error(MOEA_ERR_INVALID_ARGUMENT, "The current NSGA-III CUDA backend requires an even population size");
+            if (!(cfg.sparse_ratio > 0.0f))
+                return set_error(MOEA_ERR_INVALID_ARGUMENT, "NSGA-III sparse_ratio must be positive");
+            if (cfg.cv_bins > 0) {
+                const bool ok = std::isfinite(cfg.cv_clip_upper) && cfg.cv_clip_upper > 0.0f &&
+                                std::isfinite(cfg.cv_log_alpha) && cfg.cv_log_alpha >= 0.0f &&
+                                std::isfinite(cfg.feasibility_epsilon) && cfg.feasibility_epsilon >= 0.0f &&
+                                (cfg.cv_log_alpha == 0.0f ||
+                                 (std::log1p(cfg.cv_log_alpha * cfg.cv_clip_upper) > 0.0f));
+                if (!ok) return set_error(MOEA_ERR_INVALID_ARGUMENT, "Invalid NSGA-III CV quantization configuration");
+            }
+        } else if (!(cfg.rvea_alpha > 0.0f)) {
+            return set_error(MOEA_ERR_INVALID_ARGUMENT, "RVEA alpha must be positive");
+        }
+        if (cfg.sbx_eta_initial <= 0.0f || cfg.sbx_eta_final <= 0.0f || cfg.sbx_probability < 0.0f ||
+            cfg.sbx_probability > 1.0f || cfg.sbx_copy_probability < 0.0f || cfg.sbx_copy_probability > 1.0f)
+            return set_error(MOEA_ERR_INVALID_ARGUMENT, "Invalid SBX configuration");
+        if (cfg.mutation && (cfg.pm_eta_initial <= 0.0f || cfg.pm_eta_final <= 0.0f ||
+                             cfg.pm_probability < 0.0f || cfg.pm_probability > 1.0f))
+            return set_error(MOEA_ERR_INVALID_ARGUMENT, "Invalid polynomial-mutation configuration");
+        if (cfg.mating == MOEA_MATING_CALLBACK && !cfg.mate)
+            return set_error(MOEA_ERR_INVALID_ARGUMENT, "callback mating without a function");
+        // only the NSGA-III selector provides ranks (mating_selection.cu:80-86)
+        if (cfg.mating == MOEA_MATING_TOURNAMENT && !nsga3())
+            return set_error(MOEA_ERR_INVALID_ARGUMENT, "TournamentMating requires a rank array for every parent");
+        return MOEA_OK;
+    }
+
+    int initialize()
+    {
+        if (initialized) return MOEA_OK;
+        MOEA_TRY(validate());
+        N = cfg.population_size;
+        D = cfg.dimension;
+        M = cfg.objectives;
+        T = cfg.max_generations;
+        MOEA_CUDA_TRY(cudaSetDevice(cfg.device));
+        if (cfg.stream) {
+            stream = (cudaStream_t)cfg.stream;
+            own_stream = false;
+        } else {
+            MOEA_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+            own_stream = true;
+        }
+        seed = derive_seed(cfg.seed);
+        for (int s = 0; s < 3; ++s) {
+            MOEA_TRY(dmalloc(&vars[s], (size_t)N * D));
+            MOEA_TRY(dmalloc(&objs[s], (size_t)M * N));
+            MOEA_TRY(dmalloc(&cv[s], (size_t)N));
+            MOEA_TRY(dmalloc(&rank[s], (size_t)N));
+            MOEA_CUDA_TRY(cudaMemsetAsync(objs[s], 0, sizeof(float) * M * N, stream));
+            MOEA_CUDA_TRY(cudaMemsetAsync(cv[s], 0, sizeof(float) * N, stream));
+            MOEA_CUDA_TRY(cudaMemsetAsync(rank[s], 0, sizeof(int) * N, stream));
+        }
+        MOEA_TRY(dmalloc(&cv_sort[0], (size_t)N));
+        MOEA_TRY(dmalloc(&cv_sort[1], (size_t)N));
+        MOEA_TRY(dmalloc(&bounds, (size_t)2 * D));
+        MOEA_TRY(dmalloc(&parent_idx, (size_t)N));
+        MOEA_TRY(dmalloc(&ideal_last, (size_t)M));
+        MOEA_TRY(dmalloc(&d_gen, 1));
+        MOEA_TRY(dmalloc(&d_active, 1));
+        MOEA_TRY(dmalloc(&ps_table, (size_t)T + 2));
+        MOEA_TRY(dmalloc(&cv_table, (size_t)T + 2));
+        MOEA_TRY(dmalloc(&t_buf, (size_t)M * 2 * N));
+        MOEA_TRY(dmalloc(&theta, (size_t)2 * N));
+        MOEA_TRY(dmalloc(&apd, (size_t)2 * N));
+        MOEA_TRY(dmalloc(&part_idx, (size_t)2 * N));
+        MOEA_TRY(dmalloc(&zmin, (size_t)M));
+        MOEA_TRY(dmalloc(&survivors, (size_t)2 * N));
+        MOEA_TRY(dmalloc(&frontzero, (size_t)N));
+        std::vector<float> hb(2 * (size_t)D);
+        for (int d = 0; d < D; ++d) {
+            hb[2 * d] = lower.empty() ? 0.0f : lower[d];
+            hb[2 * d + 1] = upper.empty() ? 1.0f : upper[d];
+            if (cfg.problem_kind == 15) {  // CSDP box (dtlz_problem.cu)
+                static const float lo[7] = {0.5f, 0.45f, 0.5f, 0.5f, 0.875f, 0.4f, 0.4f};
+                static const float hi[7] = {1.5f, 1.35f, 1.5f, 1.5f, 2.625f, 1.2f, 1.2f};
+                hb[2 * d] = lo[d];
+                hb[2 * d + 1] = hi[d];
+            }
+        }
+        MOEA_CUDA_TRY(cudaMemcpyAsync(bounds, hb.data(), sizeof(float) * hb.size(), cudaMemcpyHostToDevice, stream));
+        std::vector<float> ps(T + 2);
+        std::vector<int> ct(T + 2);
+        for (int g = 0; g < T + 2; ++g) {
+            ps[g] = rvea_penalty_scale(M, g + 1, T, cfg.rvea_alpha);
+            ct[g] = cv_active(g) ? 1 : 0;
+        }
+        MOEA_CUDA_TRY(cudaMemcpyAsync(ps_table, ps.data(), sizeof(float) * ps.size(), cudaMemcpyHostToDevice, stream));
+        MOEA_CUDA_TRY(cudaMemcpyAsync(cv_table, ct.data(), sizeof(int) * ct.size(), cudaMemcpyHostToDevice, stream));
+        MOEA_TRY(directions_init());
+        MOEA_TRY(workspace_init(ws, cfg.device, 2 * N, M, H));
+        ws_ready = true;
+        if (!init_pop.empty()) {
+            for (int r = 0; r < N; ++r)
+                for (int d = 0; d < D; ++d) {
+                    const float v = init_pop[(size_t)r * D + d];
+                    if (!std::isfinite(v) || v < hb[2 * d] || v > hb[2 * d + 1])
+                        return set_error(MOEA_ERR_INVALID_ARGUMENT,
+                                         "initial_population contains a non-finite or out-of-bounds value");
+                }
+        }
+        MOEA_TRY(start_population());
+        initialized = true;
+        return MOEA_OK;
+    }
+
+    // Random (or given) parents, their evaluation and the first sort.
+    int start_population()
+    {
+        P = 0; O = 1; X = 2;
+        if (!init_pop.empty() && epoch == 0) {
+            MOEA_CUDA_TRY(cudaMemcpyAsync(vars[P], init_pop.data(), sizeof(float) * init_pop.size(),
+                                          cudaMemcpyHostToDevice, stream));
+        } else {
+            MOEA_TRY(run_init_uniform(vars[P], bounds, N, D, seed ^ ((uint64_t)epoch << 48), stream));
+        }
+        MOEA_TRY(evaluate(P, -1));
+        generation = 0;
+        const int zero = 0;
+        MOEA_CUDA_TRY(cudaMemcpyAsync(d_gen, &zero, sizeof(int), cudaMemcpyHostToDevice, stream));
+        MOEA_CUDA_TRY(cudaMemcpyAsync(d_active, &N, sizeof(int), cudaMemcpyHostToDevice, stream));
+        MOEA_CUDA_TRY(cudaMemsetAsync(ws.offset_dev, 0, sizeof(unsigned long long), stream));
+        ideal_ready = false;
+        last_prepared_target = -2;
+        MOEA_TRY(prepare());
+        MOEA_CUDA_TRY(cudaStreamSynchronize(stream));
+        return workspace_check_status(ws, stream);
+    }
+
+    uint64_t gen_seed() const { return seed ^ ((uint64_t)epoch << 48); }
+
+    // Reproduction, evaluation and selection of one generation: the part that
+    // is replayed from a CUDA graph.
+    int generation_body()
+    {
+        const uint64_t s = gen_seed();
+        if (cfg.mating == MOEA_MATING_CALLBACK) {
+            const int rc = cfg.mate(cfg.mate_user, vars[P], objs[P], cv[P], nsga3() ? rank[P] : nullptr,
+                                    nsga3() ? N : active_count_sync(), parent_idx, N, D, M, generation,
+                                    (void*)stream);
+            if (rc != 0) return set_error(MOEA_ERR_CALLBACK, "mating callback failed (%d)", rc);
+        } else {
+            const bool tournament = cfg.mating == MOEA_MATING_TOURNAMENT;
+            MOEA_TRY(run_mating(cv[P], tournament ? rank[P] : nullptr, nsga3() ? nullptr : d_active, N, N,
+                                s, d_gen, 0, parent_idx, stream));
+        }
+        stage_mark("mating", stream);
+        MOEA_TRY(run_variation(vars[P], parent_idx, bounds, vars[O], N, D, cfg.sbx_eta_initial,
+                               cfg.sbx_eta_final, cfg.sbx_probability, cfg.sbx_copy_probability,
+                               cfg.mutation, cfg.pm_eta_initial, cfg.pm_eta_final, cfg.pm_probability, T,
+                               s, d_gen, 0, stream));
+        stage_mark("variation", stream);
+        if (cfg.problem_kind == 0) {
+            MOEA_TRY(evaluate(O, generation));
+        } else {
+            MOEA_TRY(run_problem(cfg.problem_kind, vars[O], N, D, M, objs[O], cv[O], stream));
+            if (constrained() && cfg.problem_kind != 15)
+                zero_cv_if_inactive<<<ceil_div(N, 256), 256, 0, stream>>>(cv[O], N, cv_table, d_gen);
+        }
+        stage_mark("evaluate", stream);
+        SplitPop pop{objs[P], objs[O], cv[P], cv[O], N, N, N, 2 * N};
+        if (nsga3()) {
+            SplitPop sort_pop = pop;
+            if (cfg.cv_bins > 0) {
+                MOEA_TRY(run_quantize_cv(cv[P], cv_sort[0], N, cfg.feasibility_epsilon, cfg.cv_clip_upper,
+                                         cfg.cv_log_alpha, cfg.cv_bins, stream));
+                MOEA_TRY(run_quantize_cv(cv[O], cv_sort[1], N, cfg.feasibility_epsilon, cfg.cv_clip_upper,
+                                         cfg.cv_log_alpha, cfg.cv_bins, stream));
+                sort_pop.cv_a = cv_sort[0];
+                sort_pop.cv_b = cv_sort[1];
+            }
+            MOEA_TRY(run_nsga3_select(ws, pop, M, N, refs, H, seed, ideal_last, survivors, nullptr,
+                                      cfg.association_mode, stream, &sort_pop));
+            gather_next<<<ceil_div((long long)N * D > N ? (long long)N * D : N, 256), 256, 0, stream>>>(
+                vars[P], vars[O], pop, survivors, ws.fronts, N, D, M, vars[X], objs[X], cv[X], rank[X]);
+            MOEA_CUDA_TRY(cudaGetLastError());
+        } else {
+            MOEA_TRY(run_rvea_translate(pop, M, t_buf, 2 * N, zmin, stream));
+            MOEA_TRY(run_rvea_partition(t_buf, 2 * N, 2 * N, refs, M, H, d_active, N, N, theta, part_idx,
+                                        stream));
+            MOEA_TRY(run_rvea_apd(t_buf, 2 * N, 2 * N, theta, gamma, part_idx, M, H, ps_table, d_gen, 0.0f,
+                                  apd, stream));
+            MOEA_TRY(run_rvea_elitism(ws, part_idx, pop, apd, N, H, survivors, d_active, stream));
+            MOEA_TRY(run_rvea_update(pop, vars[P], vars[O], survivors, d_active, N, D, M, vars[X], objs[X],
+                                     cv[X], stream));
+        }
+        bump_generation<<<1, 1, 0, stream>>>(d_gen);
+        MOEA_CUDA_TRY(cudaGetLastError());
+        stage_mark("survivors", stream);
+        return MOEA_OK;
+    }
+
+    bool graphable() const
+    {
+        return cfg.use_graphs && cfg.problem_kind != 0 && cfg.mating != MOEA_MATING_CALLBACK;
+    }
+
+    int step()
+    {
+        if (!initialized) MOEA_TRY(initialize());
+        if (generation >= T) return MOEA_OK;
+        MOEA_CUDA_TRY(cudaSetDevice(cfg.device));
+        // constraint activation switch: refresh parent violations and re-sort
+        // (problem_evaluator prepare_parent, dtlz_kernels.cu:1361-1394)
+        if (constrained() && cfg.problem_kind != 0 && cv_switch_node(generation)) {
+            MOEA_TRY(run_problem(cfg.problem_kind, vars[P], N, D, M, objs[P], cv[P], stream));
+            last_prepared_target = generation;
+            MOEA_TRY(prepare());
+        }
+        bool done = false;
+        if (graphable() && !graph_failed) {
+            const int parity = (P == 0) ? 0 : 1;
+            if (!graph[parity]) {
+                cudaGraph_t g = nullptr;
+                MOEA_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+                const int st = generation_body();
+                cudaError_t ce = cudaStreamEndCapture(stream, &g);
+                if (st == MOEA_OK && ce == cudaSuccess) {
+                    size_t count = 0;
+                    if (cudaGraphGetNodes(g, nullptr, &count) == cudaSuccess && count > 0) {
+                        std::vector<cudaGraphNode_t> nodes(count);
+                        cudaGraphGetNodes(g, nodes.data(), &count);
+                        int k = 0;
+                        for (auto nd : nodes) {
+                            cudaGraphNodeType ty;
+                            if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++k;
+                        }
+                        graph_kernels = k;
+                    }
+                    ce = cudaGraphInstantiate(&graph[parity], g, 0);
+                }
+                if (g) cudaGraphDestroy(g);
+                if (st != MOEA_OK || ce != cudaSuccess) {
+                    // capture is an optimisation: fall back to direct launches
+                    cudaGetLastError();
+                    graph[parity] = nullptr;
+                    graph_failed = true;
+                }
+            }
+            if (graph[parity]) {
+                MOEA_CUDA_TRY(cudaGraphLaunch(graph[parity], stream));
+                done = true;
+            }
+        }
+        if (!done) MOEA_TRY(generation_body());
+        // RVEA direction adaptation (reference_directions.cu:132-162)
+        if (cfg.directions == MOEA_DIRS_ADAPTIVE) {
+            const int interval = std::max(1, (int)std::lround(cfg.adapt_frequency * T));
+            if ((generation + 1) % interval == 0) {
+                MOEA_TRY(run_rvea_adapt(refs0, objs[X], N, nsga3() ? nullptr : d_active, N, M, H, zmin,
+                                        refs, stream));
+                if (!nsga3()) MOEA_TRY(run_rvea_gamma(refs, M, H, gamma, stream));
+            }
+        }
+        std::swap(P, X);
+        ++generation;
+        return MOEA_OK;
+    }
+
+    int active_count_sync()
+    {
+        if (nsga3() || !initialized) return N;
+        int a = N;
+        cudaMemcpyAsync(&a, d_active, sizeof(int), cudaMemcpyDeviceToHost, stream);
+        cudaStreamSynchronize(stream);
+        return a;
+    }
+
+    // RVEAEnvironmentSelector::finalize: front-0 of the active parents
+    // (front_zero.cu:200-293).
+    int finalize()
+    {
+        if (!initialized) return set_error(MOEA_ERR_STATE, "Algorithm has not been initialized");
+        if (nsga3()) return MOEA_OK;
+        const int active = active_count_sync();
+        frontzero_count = 0;
+        if (active <= 0) return MOEA_OK;
+        MOEA_TRY(run_ndsort(ws, merged_view(objs[P], cv[P], active), M, 1, ws.selected, stream));
+        zero_front_pick<<<ceil_div(active, 256), 256, 0, stream>>>(ws.selected, active, ws.flags);
+        MOEA_TRY(run_flag_compaction(ws, active, frontzero, stream));
+        std::vector<int> flags(active);
+        MOEA_CUDA_TRY(cudaMemcpyAsync(flags.data(), ws.flags, sizeof(int) * active, cudaMemcpyDeviceToHost, stream));
+        MOEA_CUDA_TRY(cudaStreamSynchronize(stream));
+        int c = 0;
+        for (int v : flags) c += v != 0;
+        frontzero_count = c;
+        return workspace_check_status(ws, stream);
+    }
+
+    int reset()
+    {
+        if (!initialized) return MOEA_OK;
+        MOEA_CUDA_TRY(cudaStreamSynchronize(stream));
+        drop_graphs();  // the draws of the new epoch use a different seed
+        ++epoch;
+        if (H > 0) {
+            MOEA_CUDA_TRY(cudaMemcpyAsync(refs, refs0, sizeof(float) * (size_t)M * H, cudaMemcpyDeviceToDevice,
+                                          stream));
+            if (!nsga3()) MOEA_TRY(run_rvea_gamma(refs, M, H, gamma, stream));
+        }
+        total_ms = 0.0;
+        frontzero_count = 0;
+        return start_population();
+    }
+};
+
+extern "C" {
+
+void moea_algorithm_config_defaults(moea_algorithm_config* c, int algorithm)
+{
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->algorithm = algorithm;
+    c->population_size = 1024;
+    c->max_generations = 100;
+    c->device = 0;
+    c->seed = 2887;
+    c->problem_kind = 2;  // DTLZ2
+    c->dimension = 12;
+    c->objectives = 3;
+    c->mating = algorithm == MOEA_NSGA3 ? MOEA_MATING_TOURNAMENT : MOEA_MATING_RANDOM;
+    c->sbx_eta_initial = c->sbx_eta_final = 30.0f;
+    c->sbx_probability = 1.0f;
+    c->sbx_copy_probability = 0.0f;
+    c->mutation = 1;
+    c->pm_eta_initial = c->pm_eta_final = 20.0f;
+    c->pm_probability = 1.0f;
+    c->directions = algorithm == MOEA_NSGA3 ? MOEA_DIRS_DAS_DENNIS : MOEA_DIRS_ADAPTIVE;
+    c->partitions = 0;
+    c->adapt_frequency = 0.1f;
+    c->normalize_user_directions = 1;
+    c->sparse_ratio = 0.5f;
+    c->rvea_alpha = 2.0f;
+    c->use_graphs = 1;
+}
+
+moea_status moea_algorithm_create(const moea_algorithm_config* cfg, moea_algorithm** out)
+{
+    if (!cfg || !out) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    moea_algorithm* a = new (std::nothrow) moea_algorithm();
+    if (!a) return set_error(MOEA_ERR_OUT_OF_MEMORY, "host allocation failed");
+    a->cfg = *cfg;
+    const int D = cfg->dimension, M = cfg->objectives, N = cfg->population_size;
+    if (cfg->h_lower && D > 0) a->lower.assign(cfg->h_lower, cfg->h_lower + D);
+    if (cfg->h_upper && D > 0) a->upper.assign(cfg->h_upper, cfg->h_upper + D);
+    if (cfg->h_user_directions && cfg->user_direction_count > 0 && M > 0)
+        a->user_dirs.assign(cfg->h_user_directions, cfg->h_user_directions + (size_t)M * cfg->user_direction_count);
+    if (cfg->h_initial_population && N > 0 && D > 0)
+        a->init_pop.assign(cfg->h_initial_population, cfg->h_initial_population + (size_t)N * D);
+    a->cfg.h_lower = a->cfg.h_upper = a->cfg.h_user_directions = a->cfg.h_initial_population = nullptr;
+    *out = a;
+    return MOEA_OK;
+}
+
+void moea_algorithm_destroy(moea_algorithm* a)
+{
+    if (!a) return;
+    if (a->stream) cudaStreamSynchronize(a->stream);
+    delete a;
+}
+
+moea_status moea_algorithm_initialize(moea_algorithm* a)
+{
+    if (!a) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL algorithm");
+    const int st = a->initialize();
+    if (st != MOEA_OK && !a->initialized) a->release();
+    return st;
+}
+
+moea_status moea_algorithm_step(moea_algorithm* a)
+{
+    if (!a) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL algorithm");
+    return a->step();
+}
+
+moea_status moea_algorithm_run(moea_algorithm* a, double* h_total_ms)
+{
+    if (!a) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL algorithm");
+    if (!a->initialized) MOEA_TRY(a->initialize());
+    cudaEvent_t e0, e1;
+    MOEA_CUDA_TRY(cudaEventCreate(&e0));
+    MOEA_CUDA_TRY(cudaEventCreate(&e1));
+    MOEA_CUDA_TRY(cudaEventRecord(e0, a->stream));
+    int st = MOEA_OK;
+    while (st == MOEA_OK && a->generation < a->T) st = a->step();
+    cudaEventRecord(e1, a->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != MOEA_OK) return st;
+    a->total_ms = ms;
+    if (h_total_ms) *h_total_ms = ms;
+    return workspace_check_status(a->ws, a->stream);
+}
+
+moea_status moea_algorithm_reset(moea_algorithm* a)
+{
+    if (!a) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL algorithm");
+    return a->reset();
+}
+
+moea_status moea_algorithm_synchronize(moea_algorithm* a)
+{
+    if (!a) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL algorithm");
+    if (!a->initialized) return MOEA_OK;
+    MOEA_CUDA_TRY(cudaStreamSynchronize(a->stream));
+    return workspace_check_status(a->ws, a->stream);
+}
+
+moea_status moea_algorithm_finalize(moea_algorithm* a)
+{
+    if (!a) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL algorithm");
+    return a->finalize();
+}
+
+moea_status moea_algorithm_view(moea_algorithm* a, moea_population_view* v)
+{
+    if (!a || !v) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::memset(v, 0, sizeof(*v));
+    v->size = a->cfg.population_size;
+    v->dimension = a->cfg.dimension;
+    v->objectives = a->cfg.objectives;
+    v->generation = a->generation;
+    v->initialized = a->initialized;
+    v->finished = a->initialized && a->generation >= a->T;
+    v->device = a->cfg.device;
+    v->total_ms = a->total_ms;
+    v->kernels_per_generation = a->graph_kernels;
+    v->graph_active = (a->graph[0] || a->graph[1]) ? 1 : 0;
+    if (!a->initialized) return MOEA_OK;
+    v->d_variables = a->vars[a->P];
+    v->d_objectives = a->objs[a->P];
+    v->d_constraints = a->cv[a->P];
+    if (a->nsga3()) {
+        v->d_auxiliary = a->rank[a->P];
+        v->auxiliary_count = a->N;
+    } else {
+        v->d_auxiliary = a->frontzero;
+        v->auxiliary_count = a->frontzero_count;
+    }
+    v->active_count = a->active_count_sync();
+    return MOEA_OK;
+}
+
+moea_status moea_algorithm_directions(moea_algorithm* a, const float** d_values, int* count)
+{
+    if (!a || !d_values || !count) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL argument");
+    *d_values = a->refs;
+    *count = a->H;
+    return MOEA_OK;
+}
+
+moea_status moea_algorithm_profile_step(moea_algorithm* a, char* h_names, size_t names_cap,
+                                        float* h_ms, int cap, int* h_count)
+{
+    if (!a || !h_ms || !h_count || cap < 1) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!a->initialized) MOEA_TRY(a->initialize());
+    *h_count = 0;
+    if (a->generation >= a->T) return set_error(MOEA_ERR_STATE, "algorithm finished");
+    StageProfile prof;
+    stage_profile() = &prof;
+    stage_mark("start", a->stream);
+    const bool saved = a->graph_failed;
+    a->graph_failed = true;  // direct launches: events between stages
+    const int st = a->step();
+    a->graph_failed = saved;
+    stage_profile() = nullptr;
+    cudaStreamSynchronize(a->stream);
+    int n = 0;
+    size_t used = 0;
+    for (size_t i = 1; i < prof.events.size() && n < cap; ++i) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, prof.events[i - 1], prof.events[i]);
+        h_ms[n++] = ms;
+        if (h_names) {
+            const size_t len = std::strlen(prof.names[i]);
+            if (used + len + 2 <= names_cap) {
+                std::memcpy(h_names + used, prof.names[i], len);
+                used += len;
+                h_names[used++] = '\n';
+                h_names[used] = '\0';
+            }
+        }
+    }
+    for (cudaEvent_t e : prof.events) cudaEventDestroy(e);
+    *h_count = n;
+    if (st != MOEA_OK) return st;
+    return workspace_check_status(a->ws, a->stream);
+}
+
+moea_status moea_algorithm_device_status(moea_algorithm* a, int* h_status)
+{
+    if (!a || !h_status) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL argument");
+    *h_status = 0;
+    if (!a->initialized) return MOEA_OK;
+    MOEA_CUDA_TRY(cudaMemcpy(h_status, a->ws.counters + 6, sizeof(int), cudaMemcpyDeviceToHost));
+    return MOEA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+// Internal declarations shared by the translation units of libmoea_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstddef>
+#include <vector>
+
+#include "common.cuh"
+
+namespace moea {
+
+// Events recorded at stage boundaries while a generation is being profiled.
+struct StageProfile {
+    std::vector<cudaEvent_t> events;
+    std::vector<const char*> names;
+};
+StageProfile*& stage_profile();
+
+// A population split across two buffers ("parents" a and "offspring" b) and
+// addressed as one merged index space [0, n_a + n_b).  The reference copies
+// both halves into merged buffers every generation
+// (nat/src/selection/nsga3/kernels/nsga3_population_update.cu:7-115); here the
+// kernels read through this view instead, so no merge copy exists.
+struct SplitPop {
+    const float* objs_a;
+    const float* objs_b;
+    const float* cv_a;
+    const float* cv_b;
+    int stride_a;  // row stride (points) of objs_a
+    int stride_b;
+    int n_a;
+    int n;         // total points
+
+    __device__ __forceinline__ float obj(int m, int i) const
+    {
+        return i < n_a ? objs_a[(size_t)m * stride_a + i]
+                       : objs_b[(size_t)m * stride_b + (i - n_a)];
+    }
+    __device__ __forceinline__ float cvv(int i) const
+    {
+        return i < n_a ? cv_a[i] : cv_b[i - n_a];
+    }
+};
+
+inline SplitPop merged_view(const float* objs, const float* cv, int n)
+{
+    return SplitPop{objs, objs, cv, cv, n, n, n, n};
+}
+
+// Device scratch for the generation path, sized once for (n_max, m_max, h_max).
+struct Workspace {
+    int device = 0;
+    int n_max = 0;   // merged population capacity (2N)
+    int m_max = 0;
+    int h_max = 0;
+    int words = 0;   // 32-bit words per dominance row = ceil(n_max / 32)
+    size_t bytes = 0;
+
+    // --- non-dominated sort ---
+    uint32_t* rows = nullptr;       // [n_max][words] dominator bits per sorted point
+    uint32_t* key32[2] = {};        // LSD pass keys
+    uint64_t* key64[2] = {};        // final pass keys / niching keys (ping-pong)
+    uint64_t* key0 = nullptr;       // per point: class << 32 | order key of f0 or cv
+    int* perm[2] = {};              // sorted position -> point index
+    float* sorted_f = nullptr;      // [(m_max-1)][n_max] objectives 1..M-1 in sorted order
+    int* qinfo = nullptr;           // per sorted position: dup position | infeasible bit
+    int* head = nullptr;            // run heads
+    int* run_start = nullptr;       // scanned run heads
+    int* blocker = nullptr;         // per sorted position: last known unassigned dominator
+    int* front_sorted = nullptr;    // per sorted position: front index or -1
+    int* front_list = nullptr;      // members of each peeled front, front by front
+    int* counters = nullptr;        // [0] feasible count, [1] list length, [2] max_front,
+                                    // [3] assigned, [4] barrier count, [5] barrier generation,
+                                    // [6] device status, [7..] spare
+    int peel_grid = 0;              // co-resident CTAs of the peel kernel
+    int peel_smem = 0;
+
+    // --- NSGA-III stages ---
+    int* fronts = nullptr;          // fronts of the merged population (point order)
+    int* nds_gidx = nullptr;        // [prior; last] point indices
+    int* sizes = nullptr;           // {N_prior, N_last, N_rem, N_nds}
+    int* chunk_counts = nullptr;    // ordered-compaction partial counts
+    float* nds_objs = nullptr;      // (m_max, n_max) translated objectives of nds points
+    float* norm_part = nullptr;     // ASF / max partials
+    int* norm_part_idx = nullptr;
+    float* rcp_b = nullptr;         // (m_max) reciprocal intercepts
+    int* extreme = nullptr;         // (m_max)
+    float* ideal_tmp = nullptr;     // (m_max)
+    unsigned long long* assoc_best = nullptr;  // packed (d2 bits, j) per nds point
+    int* assoc_idx = nullptr;
+    float* assoc_dist = nullptr;
+    int* rho = nullptr;             // (h_max) niche counts of prior fronts
+    int* sel_vals[2] = {};          // niching sort values
+    int* rank = nullptr;
+    int* selected = nullptr;        // (n_max) selection before ordering
+    int* flags = nullptr;           // (n_max) survivor flags
+    unsigned long long* offset_dev = nullptr;  // niching counter offset
+
+    // --- CUB temporary storage ---
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+};
+
+// ---- per-TU entry points -------------------------------------------------
+// Non-dominated sort of the split view.  Fronts in point order into ws.fronts
+// (or out_fronts when non-null), max front into ws.counters[2].
+int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_fronts,
+               cudaStream_t stream);
+
+// Ordered compaction of the fronts into [prior; last] (ws.nds_gidx, ws.sizes).
+int run_extract(Workspace& ws, const int* fronts, int n, const int* d_max_front, int N,
+                int* nds_gidx, int* sizes, cudaStream_t stream);
+
+// Gather translated objectives of the nds points and run the normalisation;
+// leaves translated values in ws.nds_objs and reciprocal intercepts in ws.rcp_b.
+int run_normalize_split(Workspace& ws, const SplitPop& pop, const int* nds_gidx,
+                        const int* sizes, const float* ideal, int M, cudaStream_t stream);
+
+int run_associate(Workspace& ws, const float* x, int x_stride, const float* scale,
+                  const float* refs, int M, const int* d_n, int n_cap, int H, int* idx,
+                  float* dist, int mode, cudaStream_t stream);
+
+int run_niching(Workspace& ws, uint64_t seed, const int* nds_gidx, const float* dist,
+                const int* idx, const int* sizes, int H, int N, int* selected,
+                cudaStream_t stream);
+
+// ideal_out[m] = fminf(prev[m], min_i objs[m][i]) (prev may be null).
+int run_ideal(const float* objs, int stride, int M, int n, const float* prev, float* ideal_out,
+              cudaStream_t stream);
+
+// Survivor ordering: ascending unique indices from an unordered selection.
+int run_order_selection(Workspace& ws, const int* selected, int count, int n_mix,
+                        int* out_sorted, cudaStream_t stream);
+
+// Ascending indices i < n with ws.flags[i] != 0 into out.
+int run_flag_compaction(Workspace& ws, int n, int* out, cudaStream_t stream);
+
+size_t cub_temp_bytes_needed(int n_max);
+
+}  // namespace moea
+
+struct moea_workspace {
+    moea::Workspace ws;
+};

@@ -1,0 +1,543 @@
+// Constraint-dominance non-dominated sorting for sm_100a.
+//
+// Replaces run_ndsort / run_ndsort_init and the COO / CSR / bitmask paths of
+// CUDA-MOEA (nat/src/selection/nsga3/kernels/non_dominated_sort.cu:158-1574).
+// Same result (front index per point, -1 past the stop rule, index of the last
+// front), different mechanism:
+//
+//  1. Lexicographic sort of the points by (class, f0 | cv, f1, ..., f_{M-1})
+//     with stable LSD radix passes.  Class 0 = feasible, 1 = feasible with a NaN
+//     objective, 2 = infeasible, 3 = infeasible with NaN violation.  In this
+//     order every dominator of a point lies strictly before it, and a feasible
+//     dominator already satisfies f0 <= q0.
+//  2. For every sorted position q, dup[q] is the first position that cannot
+//     dominate q: the start of q's run of identical objective vectors (class 0),
+//     0 (class 1: nothing dominates it), the start of q's run of equal violation
+//     (class 2) or the number of feasible points (class 3).  Then
+//       infeasible q:  p dominates q  <=>  p < dup[q]
+//       feasible q:    p dominates q  <=>  p < dup[q] and f_m(p) <= f_m(q), m >= 1
+//     which is the reference relation (non_dominated_sort.cu:190-239) with one
+//     integer and M-1 float comparisons per pair on the lower triangle only.
+//  3. A tile kernel evaluates that test with warp ballots and stores, for every
+//     q, the bit row of its dominators (sorted positions, 32 per word).
+//  4. One cooperative persistent kernel peels the fronts: q joins front k when
+//     no still-unassigned point is left in its row.  Each point remembers one
+//     unassigned dominator ("blocker"); while that blocker is unassigned the
+//     point is skipped without touching memory, so every row is scanned at most
+//     once over the whole sort.  Fronts are separated by a bounded grid barrier
+//     and the loop stops once `target` points are assigned, like the
+//     reference's front propagation loops (:792-843, :1070-1279).
+#include <cub/cub.cuh>
+
+#include "internal.cuh"
+
+namespace moea {
+namespace {
+
+constexpr int kQB = 128;      // sorted positions (dominatees) per tile CTA
+constexpr int kPW = 32;       // dominator words per tile CTA (1024 positions)
+constexpr int kTileThreads = 256;
+constexpr int kPeelThreads = 512;
+constexpr uint32_t kInfeasibleBit = 0x80000000u;
+
+// ---------------------------------------------------------------------------
+// 1. classification and lexicographic sort
+// ---------------------------------------------------------------------------
+
+__global__ void nds_classify(SplitPop pop, int M, uint64_t* __restrict__ key0,
+                             int* __restrict__ perm, int* __restrict__ feasible_count)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool feasible_class = false;
+    if (i < pop.n) {
+        const float cv = pop.cvv(i);
+        uint32_t cls, val = 0;
+        if (cv == 0.0f) {
+            bool nan = false;
+            for (int m = 0; m < M; ++m) nan |= isnan(pop.obj(m, i));
+            cls = nan ? 1u : 0u;
+            if (!nan) val = float_order_key(pop.obj(0, i));
+        } else {
+            cls = isnan(cv) ? 3u : 2u;
+            if (cls == 2u) val = float_order_key(cv);
+        }
+        key0[i] = ((uint64_t)cls << 32) | val;
+        perm[i] = i;
+        feasible_class = cls <= 1u;
+    }
+    const unsigned fm = __ballot_sync(0xFFFFFFFFu, feasible_class);
+    if ((threadIdx.x & 31) == 0 && fm) atomicAdd(feasible_count, __popc(fm));
+}
+
+// Key of LSD pass m (m >= 1) for the current order.
+__global__ void nds_gather_key(SplitPop pop, int m, const uint64_t* __restrict__ key0,
+                               const int* __restrict__ perm, uint32_t* __restrict__ key)
+{
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= pop.n) return;
+    const int pt = perm[pos];
+    key[pos] = ((key0[pt] >> 32) == 0) ? float_order_key(pop.obj(m, pt)) : 0u;
+}
+
+__global__ void nds_gather_key0(int n, const uint64_t* __restrict__ key0,
+                                const int* __restrict__ perm, uint64_t* __restrict__ key)
+{
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos < n) key[pos] = key0[perm[pos]];
+}
+
+// Sorted copy of objectives 1..M-1 and run heads for the dup computation.
+__global__ void nds_sorted_soa(SplitPop pop, int M, const uint64_t* __restrict__ key0,
+                               const int* __restrict__ perm, float* __restrict__ sf,
+                               int sf_stride, int* __restrict__ head)
+{
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= pop.n) return;
+    const int pt = perm[pos];
+    const uint64_t k0 = key0[pt];
+    const uint32_t cls = (uint32_t)(k0 >> 32);
+    for (int m = 1; m < M; ++m) sf[(size_t)(m - 1) * sf_stride + pos] = pop.obj(m, pt);
+    bool is_head = true;
+    if (pos > 0) {
+        const int pp = perm[pos - 1];
+        const uint64_t k1 = key0[pp];
+        if (k1 == k0) {
+            if (cls == 0u) {
+                bool same = true;
+                for (int m = 1; m < M; ++m)
+                    same &= float_order_key(pop.obj(m, pt)) == float_order_key(pop.obj(m, pp));
+                is_head = !same;
+            } else {
+                is_head = false;
+            }
+        }
+    }
+    head[pos] = is_head ? pos : 0;
+}
+
+__global__ void nds_finalize_rows(int n, const uint64_t* __restrict__ key0,
+                                  const int* __restrict__ perm, const int* __restrict__ run_start,
+                                  const int* __restrict__ feasible_count, int* __restrict__ qinfo,
+                                  int* __restrict__ blocker, int* __restrict__ front_sorted)
+{
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    const uint32_t cls = (uint32_t)(key0[perm[pos]] >> 32);
+    uint32_t d;
+    switch (cls) {
+    case 0u: d = (uint32_t)run_start[pos]; break;
+    case 1u: d = 0u; break;
+    case 2u: d = (uint32_t)run_start[pos] | kInfeasibleBit; break;
+    default: d = (uint32_t)(*feasible_count) | kInfeasibleBit; break;
+    }
+    qinfo[pos] = (int)d;
+    blocker[pos] = -1;
+    front_sorted[pos] = -1;
+}
+
+// ---------------------------------------------------------------------------
+// 2. dominance rows
+// ---------------------------------------------------------------------------
+
+// Number of float4 slots of a q record: objectives 1..M-1 then the dup word.
+template <int M>
+struct QRec {
+    static constexpr int kWords = M;                  // (M-1) floats + 1 dup word
+    static constexpr int kVec = (kWords + 3) / 4;
+};
+
+template <int M, bool kAnyInfeasible>
+__device__ __forceinline__ void tile_word_loop(const float4* __restrict__ sq, const float (&pf)[M > 1 ? M - 1 : 1],
+                                               int p, int lane, uint32_t* __restrict__ out_col,
+                                               int out_stride)
+{
+    constexpr int V = QRec<M>::kVec;
+    for (int qi = 0; qi < kQB; qi += 32) {
+#pragma unroll 8
+        for (int t = 0; t < 32; ++t) {
+            const float4* rec = sq + (qi + t) * V;
+            float w[V * 4];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const float4 r = rec[v];
+                w[4 * v + 0] = r.x; w[4 * v + 1] = r.y; w[4 * v + 2] = r.z; w[4 * v + 3] = r.w;
+            }
+            const uint32_t dinfo = __float_as_uint(w[M - 1]);
+            bool d;
+            if (kAnyInfeasible && (dinfo & kInfeasibleBit)) {
+                d = p < (int)(dinfo & ~kInfeasibleBit);
+            } else {
+                d = p < (int)dinfo;
+#pragma unroll
+                for (int m = 0; m < M - 1; ++m) d &= pf[m] <= w[m];
+            }
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, d);
+            if (lane == 0) out_col[(qi + t) * out_stride] = bal;
+        }
+    }
+}
+
+template <int M>
+__global__ void __launch_bounds__(kTileThreads)
+nds_tiles(const float* __restrict__ sf, int sf_stride, const int* __restrict__ qinfo, int n, int W,
+          uint32_t* __restrict__ rows)
+{
+    constexpr int V = QRec<M>::kVec;
+    const int b = blockIdx.y;
+    const int q0 = b * kQB;
+    if (q0 >= n) return;
+    const int qend = min(q0 + kQB, n);
+    // dominators of the block lie at positions < qend - 1
+    const int nwords = (qend - 1 + 31) >> 5;
+    const int w0 = blockIdx.x * kPW;
+    if (w0 >= nwords) return;
+
+    __shared__ float4 sq[kQB * V];
+    __shared__ uint32_t so[kQB][kPW + 1];
+    __shared__ int s_any_inf;
+    if (threadIdx.x == 0) s_any_inf = 0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < kQB; t += blockDim.x) {
+        const int pos = q0 + t;
+        float w[V * 4];
+#pragma unroll
+        for (int i = 0; i < V * 4; ++i) w[i] = 0.0f;
+        uint32_t dinfo = 0u;
+        if (pos < n) {
+#pragma unroll
+            for (int m = 0; m < M - 1; ++m) w[m] = sf[(size_t)m * sf_stride + pos];
+            dinfo = (uint32_t)qinfo[pos];
+        }
+        w[M - 1] = __uint_as_float(dinfo);
+        if (dinfo & kInfeasibleBit) s_any_inf = 1;
+#pragma unroll
+        for (int v = 0; v < V; ++v) sq[t * V + v] = make_float4(w[4 * v], w[4 * v + 1], w[4 * v + 2], w[4 * v + 3]);
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool any_inf = s_any_inf != 0;
+    for (int wl = warp; wl < kPW; wl += kTileThreads / 32) {
+        const int w = w0 + wl;
+        if (w >= nwords) break;
+        const int p = w * 32 + lane;
+        float pf[M > 1 ? M - 1 : 1];
+#pragma unroll
+        for (int m = 0; m < M - 1; ++m) pf[m] = (p < n) ? sf[(size_t)m * sf_stride + p] : __int_as_float(0x7FC00000);
+        if (any_inf)
+            tile_word_loop<M, true>(sq, pf, p, lane, &so[0][wl], kPW + 1);
+        else
+            tile_word_loop<M, false>(sq, pf, p, lane, &so[0][wl], kPW + 1);
+    }
+    __syncthreads();
+    const int wcount = min(kPW, nwords - w0);
+    for (int r = warp; r < kQB; r += kTileThreads / 32) {
+        const int pos = q0 + r;
+        if (pos >= n) break;
+        if (lane < wcount) rows[(size_t)pos * W + w0 + lane] = so[r][lane];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3. front peeling
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid barrier over co-resident CTAs.  Waits at most ~2 s, then records
+// kDevBarrierTimeout in the status word and returns false.  The last CTA to
+// arrive copies the front-list length (counters[1]) into counters[9] before
+// releasing the others, so every CTA reads the same length after the barrier
+// even when a fast CTA has already started appending the next front.
+__device__ bool grid_barrier(int* counters, unsigned nblocks)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile int* vgen = counters + 5;
+        volatile int* vstatus = counters + 6;
+        const int g = *vgen;
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(counters + 4, 1) == (int)nblocks - 1) {
+            counters[9] = atomicAdd(counters + 1, 0);
+            atomicExch(counters + 4, 0);
+            __threadfence();
+            atomicAdd(counters + 5, 1);
+        } else {
+            const unsigned long long t0 = global_ns();
+            while (*vgen == g) {
+                if (*vstatus != 0) { ok = 0; break; }
+                if (global_ns() - t0 > 2000000000ull) {
+                    atomicExch(counters + 6, kDevBarrierTimeout);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+__global__ void __launch_bounds__(kPeelThreads)
+nds_peel(const uint32_t* __restrict__ rows, int W, int n, int target, const int* __restrict__ qinfo,
+         int* __restrict__ blocker, int* __restrict__ front_sorted, int* __restrict__ list,
+         int* counters)
+{
+    extern __shared__ uint32_t U[];  // unassigned positions, one bit each
+    __shared__ int s_len;
+    for (int w = threadIdx.x; w < W; w += blockDim.x) {
+        const int lo = w * 32;
+        U[w] = (lo + 32 <= n) ? 0xFFFFFFFFu : (lo >= n ? 0u : ((1u << (n - lo)) - 1u));
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    const int gwarp = blockIdx.x * wpb + warp;
+    const int twarps = gridDim.x * wpb;
+    const int ngroups = (n + 31) >> 5;
+    int len_prev = 0, total = 0, k = 0;
+    __syncthreads();
+
+    for (;;) {
+        for (int g = gwarp; g < ngroups; g += twarps) {
+            const int q = g * 32 + lane;
+            const bool alive = q < n && ((U[q >> 5] >> (q & 31)) & 1u);
+            bool need = false;
+            int start_w = -1;
+            if (alive) {
+                const int b = blocker[q];
+                if (b < 0 || !((U[b >> 5] >> (b & 31)) & 1u)) {
+                    need = true;
+                    if (b >= 0) {
+                        start_w = b >> 5;
+                    } else {
+                        const int d = qinfo[q] & 0x7FFFFFFF;
+                        start_w = ((d + 31) >> 5) - 1;
+                    }
+                }
+            }
+            unsigned needm = __ballot_sync(0xFFFFFFFFu, need);
+            bool is_free = false;
+            while (needm) {
+                const int L = __ffs(needm) - 1;
+                needm &= needm - 1;
+                const int qL = g * 32 + L;
+                const int sw = __shfl_sync(0xFFFFFFFFu, start_w, L);
+                int found = -1;
+                for (int w0 = sw; w0 >= 0; w0 -= 32) {
+                    const int w = w0 - lane;
+                    const uint32_t bits = (w >= 0) ? (__ldg(rows + (size_t)qL * W + w) & U[w]) : 0u;
+                    const unsigned nz = __ballot_sync(0xFFFFFFFFu, bits != 0u);
+                    if (nz) {
+                        const int src = __ffs(nz) - 1;
+                        const uint32_t bb = __shfl_sync(0xFFFFFFFFu, bits, src);
+                        found = (w0 - src) * 32 + (31 - __clz(bb));
+                        break;
+                    }
+                }
+                if (lane == L) {
+                    if (found >= 0) blocker[q] = found;
+                    else is_free = true;
+                }
+            }
+            const unsigned fm = __ballot_sync(0xFFFFFFFFu, is_free);
+            if (fm) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(counters + 1, __popc(fm));
+                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                if (is_free) {
+                    list[base + __popc(fm & ((1u << lane) - 1u))] = q;
+                    front_sorted[q] = k;
+                }
+            }
+        }
+        if (!grid_barrier(counters, gridDim.x)) return;
+        if (threadIdx.x == 0) s_len = *((volatile int*)counters + 9);
+        __syncthreads();
+        const int len = s_len;
+        const int ck = len - len_prev;
+        for (int i = threadIdx.x; i < ck; i += blockDim.x) {
+            const int q = __ldcg(list + len_prev + i);
+            atomicAnd(&U[q >> 5], ~(1u << (q & 31)));
+        }
+        __syncthreads();
+        total += ck;
+        len_prev = len;
+        if (total >= target || ck == 0) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                counters[2] = k;
+                counters[3] = total;
+                if (ck == 0 && total < target) atomicExch(counters + 6, kDevPeelInconsistent);
+            }
+            return;
+        }
+        ++k;
+    }
+}
+
+__global__ void nds_scatter_fronts(int n, const int* __restrict__ perm,
+                                   const int* __restrict__ front_sorted, int* __restrict__ fronts)
+{
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos < n) fronts[perm[pos]] = front_sorted[pos];
+}
+
+__global__ void nds_reset_counters(int* counters)
+{
+    if (threadIdx.x < 4) counters[threadIdx.x] = 0;
+    if (threadIdx.x == 4) counters[4] = 0;
+}
+
+template <int M>
+void launch_tiles(const Workspace& ws, int n, cudaStream_t stream)
+{
+    const int nqb = ceil_div(n, kQB);
+    const int maxw = ceil_div(n, 32);
+    dim3 grid(ceil_div(maxw, kPW), nqb);
+    nds_tiles<M><<<grid, kTileThreads, 0, stream>>>(ws.sorted_f, ws.n_max, ws.qinfo, n,
+                                                     ws.words, ws.rows);
+}
+
+}  // namespace
+
+size_t cub_temp_bytes_needed(int n_max)
+{
+    size_t a = 0, b = 0, c = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, a, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                    (int*)nullptr, (int*)nullptr, n_max);
+    cub::DeviceRadixSort::SortPairs(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr,
+                                    (int*)nullptr, (int*)nullptr, n_max);
+    cub::DeviceScan::InclusiveScan(nullptr, c, (int*)nullptr, (int*)nullptr, cub::Max(), n_max);
+    size_t m = a > b ? a : b;
+    return m > c ? m : c;
+}
+
+int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_fronts,
+               cudaStream_t stream)
+{
+    const int n = pop.n;
+    if (n <= 0) return MOEA_OK;
+    if (n > ws.n_max || M < 1 || M > ws.m_max)
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "ndsort: n=%d M=%d exceed the workspace (%d, %d)",
+                         n, M, ws.n_max, ws.m_max);
+    if (target > n) target = n;
+    if (target < 1) target = 1;
+    int* fronts = out_fronts ? out_fronts : ws.fronts;
+    int* feas = ws.counters;
+    const int T = 256, G = ceil_div(n, T);
+
+    nds_reset_counters<<<1, 32, 0, stream>>>(ws.counters);
+    nds_classify<<<G, T, 0, stream>>>(pop, M, ws.key0, ws.perm[0], feas);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    const uint64_t* key0 = ws.key0;
+    int cur = 0;
+    size_t tmp = ws.cub_bytes;
+    for (int m = M - 1; m >= 1; --m) {
+        nds_gather_key<<<G, T, 0, stream>>>(pop, m, key0, ws.perm[cur], ws.key32[0]);
+        MOEA_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp, tmp, ws.key32[0], ws.key32[1],
+                                                      ws.perm[cur], ws.perm[cur ^ 1], n, 0, 32,
+                                                      stream));
+        cur ^= 1;
+    }
+    nds_gather_key0<<<G, T, 0, stream>>>(n, key0, ws.perm[cur], ws.key64[0]);
+    MOEA_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp, tmp, ws.key64[0],
+                                                  ws.key64[1], ws.perm[cur],
+                                                  ws.perm[cur ^ 1], n, 0, 34, stream));
+    cur ^= 1;
+    const int* perm = ws.perm[cur];
+
+    nds_sorted_soa<<<G, T, 0, stream>>>(pop, M, key0, perm, ws.sorted_f, ws.n_max, ws.head);
+    MOEA_CUDA_TRY(cub::DeviceScan::InclusiveScan(ws.cub_tmp, tmp, ws.head, ws.run_start,
+                                                 cub::Max(), n, stream));
+    int* qinfo = ws.qinfo;
+    nds_finalize_rows<<<G, T, 0, stream>>>(n, key0, perm, ws.run_start, feas, qinfo, ws.blocker,
+                                           ws.front_sorted);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    stage_mark("ndsort.lexsort", stream);
+
+    switch (M) {
+    case 1: launch_tiles<1>(ws, n, stream); break;
+    case 2: launch_tiles<2>(ws, n, stream); break;
+    case 3: launch_tiles<3>(ws, n, stream); break;
+    case 4: launch_tiles<4>(ws, n, stream); break;
+    case 5: launch_tiles<5>(ws, n, stream); break;
+    case 6: launch_tiles<6>(ws, n, stream); break;
+    case 7: launch_tiles<7>(ws, n, stream); break;
+    case 8: launch_tiles<8>(ws, n, stream); break;
+    case 9: launch_tiles<9>(ws, n, stream); break;
+    case 10: launch_tiles<10>(ws, n, stream); break;
+    case 11: launch_tiles<11>(ws, n, stream); break;
+    case 12: launch_tiles<12>(ws, n, stream); break;
+    case 13: launch_tiles<13>(ws, n, stream); break;
+    case 14: launch_tiles<14>(ws, n, stream); break;
+    case 15: launch_tiles<15>(ws, n, stream); break;
+    case 16: launch_tiles<16>(ws, n, stream); break;
+    default: return set_error(MOEA_ERR_UNSUPPORTED, "ndsort: M=%d", M);
+    }
+    MOEA_CUDA_TRY(cudaGetLastError());
+    stage_mark("ndsort.dominance_tiles", stream);
+
+    // cooperative peel
+    const int W = ceil_div(n, 32);
+    const int wpb = kPeelThreads / 32;
+    int grid = ceil_div(ceil_div(n, 32), wpb);
+    if (grid > ws.peel_grid) grid = ws.peel_grid;
+    if (grid < 1) grid = 1;
+    const uint32_t* rows = ws.rows;
+    int Wp = ws.words;
+    int nn = n, tt = target;
+    const int* qi = qinfo;
+    int* blk = ws.blocker;
+    int* fs = ws.front_sorted;
+    int* list = ws.front_list;
+    int* ctr = ws.counters;
+    (void)W;
+    void* args[] = {(void*)&rows, (void*)&Wp, (void*)&nn, (void*)&tt, (void*)&qi,
+                    (void*)&blk, (void*)&fs, (void*)&list, (void*)&ctr};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kPeelThreads);
+    cfg.dynamicSmemBytes = (size_t)ws.words * sizeof(uint32_t);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    MOEA_CUDA_TRY(cudaLaunchKernelExC(&cfg, (const void*)nds_peel, args));
+
+    nds_scatter_fronts<<<G, T, 0, stream>>>(n, perm, ws.front_sorted, fronts);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    stage_mark("ndsort.peel", stream);
+    return MOEA_OK;
+}
+
+// Configure the co-resident grid of the peel kernel for this device.
+int configure_peel(Workspace& ws)
+{
+    const size_t smem = (size_t)ws.words * sizeof(uint32_t);
+    if (smem > 48 * 1024)
+        MOEA_CUDA_TRY(cudaFuncSetAttribute(nds_peel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+    int per_sm = 0;
+    MOEA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nds_peel, kPeelThreads,
+                                                                smem));
+    int sms = 0;
+    MOEA_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws.device));
+    if (per_sm < 1)
+        return set_error(MOEA_ERR_UNSUPPORTED, "peel kernel does not fit on an SM (smem %zu)", smem);
+    ws.peel_grid = sms * (per_sm > 2 ? 2 : per_sm);
+    ws.peel_smem = (int)smem;
+    return MOEA_OK;
+}
+
+}  // namespace moea

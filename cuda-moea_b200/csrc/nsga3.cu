@@ -1,0 +1,805 @@
+// NSGA-III selection stages after the non-dominated sort, for sm_100a.
+//
+// Reference stages (paths relative to python/csrc/native/src/selection/nsga3/):
+//   extraction      kernels/non_dominated_sort.cu:1580-1781
+//   ideal point     kernels/ideal_point.cu:13-165
+//   normalisation   kernels/normalization.cu:370-856, 1217-1394, 1593-1636
+//   association     kernels/association.cu:86-188, 397-447, 586-608
+//   niching         kernels/niching.cu:21-400 + core/cuda/cuda_ref_segment_ops.cu
+//   survivor update kernels/nsga3_population_update.cu:119-281
+// Every stage is stream-ordered and reads its sizes from device memory, so a
+// whole generation runs without a host round trip.
+#include <cub/cub.cuh>
+
+#include <cmath>
+
+#include "internal.cuh"
+
+namespace moea {
+namespace {
+
+constexpr int kChunk = 1024;
+
+// ---------------------------------------------------------------------------
+// ordered two-class compaction (ascending index order inside each class)
+// ---------------------------------------------------------------------------
+
+// class of element i: 0 = first group, 1 = second group, -1 = dropped
+struct FrontClass {
+    const int* fronts;
+    const int* max_front;
+    __device__ __forceinline__ int operator()(int i) const
+    {
+        const int f = fronts[i], mf = *max_front;
+        return (f >= 0 && f < mf) ? 0 : (f == mf ? 1 : -1);
+    }
+};
+struct FlagClass {
+    const int* flags;
+    __device__ __forceinline__ int operator()(int i) const { return flags[i] ? 0 : -1; }
+};
+
+__device__ __forceinline__ int block_sum_1024(int v, int* sh)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    int t = 0;
+    if (threadIdx.x < 32) {
+        t = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xFFFFFFFFu, t, o);
+        if (lane == 0) sh[32] = t;
+    }
+    __syncthreads();
+    const int r = sh[32];
+    __syncthreads();
+    return r;
+}
+
+template <class C>
+__global__ void __launch_bounds__(kChunk) compact_count(C cls, int n, int* counts, int nchunks)
+{
+    __shared__ int sh[33];
+    const int i = blockIdx.x * kChunk + threadIdx.x;
+    const int c = (i < n) ? cls(i) : -1;
+    const int a = block_sum_1024(c == 0, sh);
+    const int b = block_sum_1024(c == 1, sh);
+    if (threadIdx.x == 0) {
+        counts[blockIdx.x] = a;
+        counts[nchunks + blockIdx.x] = b;
+    }
+}
+
+template <class C>
+__global__ void __launch_bounds__(kChunk)
+compact_write(C cls, int n, const int* counts, int nchunks, int N, int* out, int* sizes)
+{
+    __shared__ int sh[33];
+    __shared__ int wa[32], wb[32];
+    // offsets of this chunk and totals
+    int pa = 0, pb = 0, ta = 0, tb = 0;
+    for (int c = threadIdx.x; c < nchunks; c += blockDim.x) {
+        const int a = counts[c], b = counts[nchunks + c];
+        ta += a; tb += b;
+        if (c < (int)blockIdx.x) { pa += a; pb += b; }
+    }
+    pa = block_sum_1024(pa, sh);
+    pb = block_sum_1024(pb, sh);
+    ta = block_sum_1024(ta, sh);
+    tb = block_sum_1024(tb, sh);
+    const int i = blockIdx.x * kChunk + threadIdx.x;
+    const int c = (i < n) ? cls(i) : -1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned ma = __ballot_sync(0xFFFFFFFFu, c == 0);
+    const unsigned mb = __ballot_sync(0xFFFFFFFFu, c == 1);
+    if (lane == 0) { wa[warp] = __popc(ma); wb[warp] = __popc(mb); }
+    __syncthreads();
+    int oa = 0, ob = 0;
+    for (int w = 0; w < warp; ++w) { oa += wa[w]; ob += wb[w]; }
+    const unsigned lt = (1u << lane) - 1u;
+    if (c == 0) out[pa + oa + __popc(ma & lt)] = i;
+    if (c == 1) out[ta + pb + ob + __popc(mb & lt)] = i;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && sizes) {
+        sizes[0] = ta;
+        sizes[1] = tb;
+        sizes[2] = N - ta;
+        sizes[3] = ta + tb;
+    }
+}
+
+template <class C>
+int run_compaction(C cls, int n, int* counts, int N, int* out, int* sizes, cudaStream_t stream)
+{
+    const int nchunks = ceil_div(n, kChunk);
+    compact_count<C><<<nchunks, kChunk, 0, stream>>>(cls, n, counts, nchunks);
+    compact_write<C><<<nchunks, kChunk, 0, stream>>>(cls, n, counts, nchunks, N, out, sizes);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// ideal point
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(512)
+ideal_kernel(const float* __restrict__ objs, int stride, int n, const float* prev, float* out)
+{
+    const int m = blockIdx.x;
+    float v = INFINITY;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v = fminf(v, objs[(size_t)m * stride + i]);
+    __shared__ float sh[16];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_down_sync(0xFFFFFFFFu, v, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float r = INFINITY;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fminf(r, sh[w]);
+        out[m] = prev ? fminf(prev[m], r) : r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// normalisation
+// ---------------------------------------------------------------------------
+
+constexpr int kNormThreads = 256;
+
+__device__ __forceinline__ bool asf_better(float v, int i, float cur, int cur_i)
+{
+    return v < cur || (v == cur && i < cur_i);
+}
+
+// Gathers and translates the nds objectives, and reduces per block the ASF
+// argmin of every axis and the per-objective maximum (fallback intercepts).
+template <int M>
+__global__ void __launch_bounds__(kNormThreads)
+norm_gather(SplitPop pop, const int* __restrict__ gidx, const int* __restrict__ sizes,
+            const float* __restrict__ ideal, float* __restrict__ nds, int nds_stride,
+            float* __restrict__ part_val, int* __restrict__ part_idx, float* __restrict__ part_max,
+            int gather)
+{
+    const int n = sizes[3];
+    const int i = blockIdx.x * kNormThreads + threadIdx.x;
+    float v[M];
+    if (i < n) {
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            float t = gather ? pop.obj(m, gidx[i]) : nds[(size_t)m * nds_stride + i];
+            t = t - ideal[m];
+            if (isfinite(t)) t = fmaxf(t, 0.0f);
+            v[m] = t;
+            nds[(size_t)m * nds_stride + i] = t;
+        }
+    }
+    __shared__ float s_val[kNormThreads / 32][M];
+    __shared__ int s_idx[kNormThreads / 32][M];
+    __shared__ float s_max[kNormThreads / 32][M];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+        float a = INFINITY;
+        int ai = -1;
+        float mx = -INFINITY;
+        if (i < n) {
+            float s = -INFINITY;
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                const float t = isnan(v[m]) ? INFINITY : v[m];
+                s = fmaxf(s, t * ((m == j) ? 1.0f : 1e6f));
+            }
+            if (asf_better(s, i, a, ai)) { a = s; ai = i; }
+            mx = isnan(v[j]) ? -INFINITY : v[j];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_down_sync(0xFFFFFFFFu, a, o);
+            const int oi = __shfl_down_sync(0xFFFFFFFFu, ai, o);
+            if (asf_better(ov, oi, a, ai)) { a = ov; ai = oi; }
+            mx = fmaxf(mx, __shfl_down_sync(0xFFFFFFFFu, mx, o));
+        }
+        if (lane == 0) { s_val[warp][j] = a; s_idx[warp][j] = ai; s_max[warp][j] = mx; }
+    }
+    __syncthreads();
+    if (threadIdx.x < M) {
+        const int j = threadIdx.x;
+        float a = INFINITY;
+        int ai = -1;
+        float mx = -INFINITY;
+        for (int w = 0; w < kNormThreads / 32; ++w) {
+            if (asf_better(s_val[w][j], s_idx[w][j], a, ai)) { a = s_val[w][j]; ai = s_idx[w][j]; }
+            mx = fmaxf(mx, s_max[w][j]);
+        }
+        part_val[blockIdx.x * M + j] = a;
+        part_idx[blockIdx.x * M + j] = ai;
+        part_max[blockIdx.x * M + j] = mx;
+    }
+}
+
+__device__ __forceinline__ double warp_sum_d(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
+
+// Intercepts from the extreme points: one-sided Jacobi SVD in FP64 of the
+// matrix whose row r is extreme point r, pseudo-inverse applied to the ones
+// vector with singular values <= 1e-5 dropped, and the reference's
+// ill-conditioning tests and row-maximum fallback
+// (normalization.cu:739-856, 1302-1394).  Run by one block of 256 threads.
+template <int M>
+__global__ void __launch_bounds__(kNormThreads)
+norm_finalize(const float* __restrict__ nds, int nds_stride, const float* __restrict__ part_val,
+              const int* __restrict__ part_idx, const float* __restrict__ part_max, int nblocks,
+              float* __restrict__ rcp_out, int* __restrict__ extreme_out, int* __restrict__ ill_out)
+{
+    __shared__ int s_ext[M];
+    __shared__ float s_max[M];
+    __shared__ double sA[M][M];
+    __shared__ double sV[M][M];
+    __shared__ double s_sigma[M];
+    __shared__ int s_bad;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_bad = 0;
+    for (int j = warp; j < M; j += kNormThreads / 32) {
+        float a = INFINITY;
+        int ai = -1;
+        float mx = -INFINITY;
+        for (int b = lane; b < nblocks; b += 32) {
+            float v = part_val[b * M + j];
+            v = isnan(v) ? INFINITY : v;
+            if (asf_better(v, part_idx[b * M + j], a, ai)) { a = v; ai = part_idx[b * M + j]; }
+            mx = fmaxf(mx, part_max[b * M + j]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_down_sync(0xFFFFFFFFu, a, o);
+            const int oi = __shfl_down_sync(0xFFFFFFFFu, ai, o);
+            if (asf_better(ov, oi, a, ai)) { a = ov; ai = oi; }
+            mx = fmaxf(mx, __shfl_down_sync(0xFFFFFFFFu, mx, o));
+        }
+        if (lane == 0) { s_ext[j] = ai; s_max[j] = mx; }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < M * M; t += blockDim.x) {
+        const int r = t / M, m = t % M;  // row r = extreme point of axis r
+        const int e = s_ext[r];
+        const float val = (e >= 0) ? nds[(size_t)m * nds_stride + e] : INFINITY;
+        if (!isfinite(val)) atomicExch(&s_bad, 1);
+        sA[r][m] = (double)val;
+        sV[r][m] = (r == m) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int bad = s_bad;
+        if (!bad) {
+            for (int sweep = 0; sweep < 60; ++sweep) {
+                int rotated = 0;
+                for (int i = 0; i < M - 1; ++i) {
+                    for (int j = i + 1; j < M; ++j) {
+                        const double x = (lane < M) ? sA[lane][i] : 0.0;
+                        const double y = (lane < M) ? sA[lane][j] : 0.0;
+                        const double al = warp_sum_d(x * x);
+                        const double be = warp_sum_d(y * y);
+                        const double ga = warp_sum_d(x * y);
+                        if (ga == 0.0 || fabs(ga) <= 1e-15 * sqrt(al * be)) continue;
+                        rotated = 1;
+                        const double zeta = (be - al) / (2.0 * ga);
+                        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                        const double c = 1.0 / sqrt(1.0 + t * t);
+                        const double s = c * t;
+                        if (lane < M) {
+                            sA[lane][i] = c * x - s * y;
+                            sA[lane][j] = s * x + c * y;
+                            const double vx = sV[lane][i], vy = sV[lane][j];
+                            sV[lane][i] = c * vx - s * vy;
+                            sV[lane][j] = s * vx + c * vy;
+                        }
+                        __syncwarp();
+                    }
+                }
+                if (!rotated) break;
+            }
+            double smax = 0.0, smin = INFINITY;
+            for (int i = 0; i < M; ++i) {
+                const double x = (lane < M) ? sA[lane][i] : 0.0;
+                const double sg = sqrt(warp_sum_d(x * x));
+                if (lane == 0) s_sigma[i] = sg;
+                if (!isfinite(sg)) bad = 1;
+                smax = fmax(smax, sg);
+                smin = fmin(smin, sg);
+            }
+            if (smin < 1e-10 || smax / smin > 1e6) bad = 1;
+        }
+        __syncwarp();
+        float r = 1.0f;
+        if (lane < M) {
+            if (!bad) {
+                double acc = 0.0;
+                for (int i = 0; i < M; ++i) {
+                    double ut1 = 0.0;
+                    for (int k = 0; k < M; ++k) ut1 += sA[k][i];
+                    const double sg = s_sigma[i];
+                    const double coef = (sg > 1e-5) ? ut1 / (sg * sg) : 0.0;
+                    acc += sV[lane][i] * coef;
+                }
+                r = (float)acc;
+            } else {
+                const float mx = s_max[lane];
+                r = (mx > 1e-10f) ? 1.0f / fmaxf(mx, 1e-6f) : 1.0f;
+            }
+            if (!isfinite(r) || r <= 0.0f) r = 1.0f;
+            rcp_out[lane] = r;
+            if (extreme_out) extreme_out[lane] = s_ext[lane];
+        }
+        if (lane == 0 && ill_out) *ill_out = bad;
+    }
+}
+
+__global__ void norm_scale(float* __restrict__ nds, int stride, const int* __restrict__ d_n, int M,
+                           const float* __restrict__ rcp)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *d_n) return;
+    for (int m = 0; m < M; ++m) nds[(size_t)m * stride + i] = nds[(size_t)m * stride + i] * rcp[m];
+}
+
+template <int M>
+int launch_norm(Workspace& ws, const SplitPop& pop, const int* gidx, const int* sizes,
+                const float* ideal, int gather, int n_cap, int* ill_out, cudaStream_t stream)
+{
+    const int nb = ceil_div(n_cap, kNormThreads);
+    float* pv = ws.norm_part;
+    float* pm = ws.norm_part + (size_t)nb * M;
+    norm_gather<M><<<nb, kNormThreads, 0, stream>>>(pop, gidx, sizes, ideal, ws.nds_objs, ws.n_max,
+                                                    pv, ws.norm_part_idx, pm, gather);
+    norm_finalize<M><<<1, kNormThreads, 0, stream>>>(ws.nds_objs, ws.n_max, pv, ws.norm_part_idx, pm,
+                                                     nb, ws.rcp_b, ws.extreme, ill_out);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+int dispatch_norm(Workspace& ws, const SplitPop& pop, const int* gidx, const int* sizes,
+                  const float* ideal, int M, int gather, int n_cap, int* ill_out,
+                  cudaStream_t stream)
+{
+    switch (M) {
+#define MOEA_NORM_CASE(K) case K: return launch_norm<K>(ws, pop, gidx, sizes, ideal, gather, n_cap, ill_out, stream);
+    MOEA_NORM_CASE(1) MOEA_NORM_CASE(2) MOEA_NORM_CASE(3) MOEA_NORM_CASE(4)
+    MOEA_NORM_CASE(5) MOEA_NORM_CASE(6) MOEA_NORM_CASE(7) MOEA_NORM_CASE(8)
+    MOEA_NORM_CASE(9) MOEA_NORM_CASE(10) MOEA_NORM_CASE(11) MOEA_NORM_CASE(12)
+    MOEA_NORM_CASE(13) MOEA_NORM_CASE(14) MOEA_NORM_CASE(15) MOEA_NORM_CASE(16)
+#undef MOEA_NORM_CASE
+    default: return set_error(MOEA_ERR_UNSUPPORTED, "normalize: M=%d", M);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// association
+// ---------------------------------------------------------------------------
+//
+// For unit directions r_j the perpendicular distance satisfies
+// d2_j = |x|^2 - (x.r_j)^2 up to rounding, so the reference argmin is found
+// among the directions whose dot^2 lies within a rounding margin of the
+// largest dot^2.  Each thread keeps a running max of dot^2 and evaluates the
+// reference's FP32 formula (association.cu:139-170: fmaf dot, contracted
+// residual, fmaf sum of squares) only for those candidates.  Ties keep the
+// smaller index within a thread (ascending j, strict <) and across direction
+// splits through a packed (d2 bits, j) atomicMin, so the result equals the
+// reference argmin exactly.  Margin: |d2_fp32(j) - (|x|^2 - dot_j^2)| is bounded
+// by about (4M+5) eps |x|^2; the kernel uses (16M+64) eps |x|^2.
+
+constexpr int kAssocThreads = 256;
+constexpr int kAssocTile = 1024;
+
+template <int M>
+struct DirTile {
+    static constexpr int kLen = (M <= 4) ? kAssocTile : 512;  // directions per smem tile
+};
+
+template <int M>
+__global__ void __launch_bounds__(kAssocThreads)
+assoc_plain(const float* __restrict__ x, int x_stride, const float* __restrict__ scale,
+            const float* __restrict__ refs, int H, const int* __restrict__ d_n, int split_len,
+            unsigned long long* __restrict__ best_out)
+{
+    constexpr int TL = DirTile<M>::kLen;
+    __shared__ __align__(16) float s_dir[TL * ((M <= 4) ? 4 : M)];
+    const int n = *d_n;
+    const int i = blockIdx.x * kAssocThreads + threadIdx.x;
+    const int j_begin = blockIdx.y * split_len;
+    const int j_end = min(H, j_begin + split_len);
+    if (blockIdx.x * kAssocThreads >= n || j_begin >= j_end) return;
+    const bool valid = i < n;
+    float xr[M];
+    float xx = 0.0f;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        float v = valid ? x[(size_t)m * x_stride + i] : 0.0f;
+        if (scale) v = v * scale[m];
+        xr[m] = v;
+        xx = fmaf(v, v, xx);
+    }
+    const float kEps = 5.9604645e-08f;  // 2^-24
+    float margin = xx * ((16.0f * M + 64.0f) * kEps) + 1e-35f;
+    if (!isfinite(xx)) margin = INFINITY;
+    // coarse pre-pass over a strided subset to start with a tight threshold
+    float maxd = -INFINITY;
+    for (int j = j_begin; j < j_end; j += 61) {
+        float dot = 0.0f;
+#pragma unroll
+        for (int m = 0; m < M; ++m) dot = fmaf(xr[m], __ldg(refs + (size_t)m * H + j), dot);
+        maxd = fmaxf(maxd, dot * dot);
+    }
+    float thr = maxd - margin;
+    if (!(thr == thr)) thr = -INFINITY;
+    float best = INFINITY;
+    int bj = -1;
+    for (int t0 = j_begin; t0 < j_end; t0 += TL) {
+        const int cnt = min(TL, j_end - t0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cnt; t += kAssocThreads) {
+            if (M <= 4) {
+                float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+                d.x = refs[t0 + t];
+                if (M > 1) d.y = refs[(size_t)H + t0 + t];
+                if (M > 2) d.z = refs[(size_t)2 * H + t0 + t];
+                if (M > 3) d.w = refs[(size_t)3 * H + t0 + t];
+                reinterpret_cast<float4*>(s_dir)[t] = d;
+            } else {
+#pragma unroll
+                for (int m = 0; m < M; ++m) s_dir[(size_t)m * TL + t] = refs[(size_t)m * H + t0 + t];
+            }
+        }
+        __syncthreads();
+        if (!valid) continue;
+#pragma unroll 4
+        for (int t = 0; t < cnt; ++t) {
+            float r[M];
+            if (M <= 4) {
+                const float4 d = reinterpret_cast<const float4*>(s_dir)[t];
+                r[0] = d.x;
+                if (M > 1) r[1 % M] = d.y;
+                if (M > 2) r[2 % M] = d.z;
+                if (M > 3) r[3 % M] = d.w;
+            } else {
+#pragma unroll
+                for (int m = 0; m < M; ++m) r[m] = s_dir[(size_t)m * TL + t];
+            }
+            float dot = 0.0f;
+#pragma unroll
+            for (int m = 0; m < M; ++m) dot = fmaf(xr[m], r[m], dot);
+            const float dd = dot * dot;
+            if (dd >= thr) {
+                float d2 = 0.0f;
+#pragma unroll
+                for (int m = 0; m < M; ++m) {
+                    const float res = fmaf(-dot, r[m], xr[m]);
+                    d2 = fmaf(res, res, d2);
+                }
+                if (d2 < best) { best = d2; bj = t0 + t; }
+                if (dd > maxd) {
+                    maxd = dd;
+                    const float nt = maxd - margin;
+                    thr = (nt == nt) ? nt : -INFINITY;
+                }
+            }
+        }
+    }
+    if (valid && best < INFINITY) {
+        const unsigned long long packed =
+            ((unsigned long long)__float_as_uint(best) << 32) | (unsigned)bj;
+        atomicMin(best_out + i, packed);
+    }
+}
+
+__global__ void assoc_reset(unsigned long long* best, int n_cap)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n_cap) best[i] = ~0ull;
+}
+
+__global__ void assoc_finish(const unsigned long long* __restrict__ best, const int* __restrict__ d_n,
+                             int* __restrict__ idx, float* __restrict__ dist)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *d_n) return;
+    const unsigned long long b = best[i];
+    if (b == ~0ull) {
+        idx[i] = -1;
+        dist[i] = INFINITY;
+    } else {
+        idx[i] = (int)(unsigned)(b & 0xFFFFFFFFull);
+        dist[i] = sqrtf(__uint_as_float((unsigned)(b >> 32)));
+    }
+}
+
+template <int M>
+void launch_assoc(const float* x, int x_stride, const float* scale, const float* refs, int H,
+                  const int* d_n, int n_cap, unsigned long long* best, int sms, cudaStream_t stream)
+{
+    const int pb = ceil_div(n_cap, kAssocThreads);
+    int splits = ceil_div(8LL * sms, pb);
+    const int max_splits = ceil_div(H, kAssocTile);
+    if (splits > max_splits) splits = max_splits;
+    if (splits < 1) splits = 1;
+    const int split_len = ceil_div(H, splits);
+    assoc_plain<M><<<dim3(pb, splits), kAssocThreads, 0, stream>>>(x, x_stride, scale, refs, H, d_n,
+                                                                   split_len, best);
+}
+
+// ---------------------------------------------------------------------------
+// niching
+// ---------------------------------------------------------------------------
+
+__global__ void nich_prior(const int* __restrict__ nds_gidx, const int* __restrict__ idx,
+                           const int* __restrict__ sizes, int H, int* __restrict__ rho,
+                           int* __restrict__ selected)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sizes[0]) return;
+    selected[i] = nds_gidx[i];
+    const int r = idx[i];
+    if (r >= 0 && r < H) atomicAdd(rho + r, 1);
+}
+
+__global__ void nich_keys1(const int* __restrict__ idx, const float* __restrict__ dist,
+                           const int* __restrict__ sizes, int n_cap, uint64_t* __restrict__ key,
+                           int* __restrict__ val)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_cap) return;
+    const int np = sizes[0], nl = sizes[1];
+    if (t < nl) {
+        key[t] = ((uint64_t)(uint32_t)idx[np + t] << 32) | __float_as_uint(dist[np + t]);
+    } else {
+        key[t] = ~0ull;
+    }
+    val[t] = t;
+}
+
+__global__ void nich_heads(const uint64_t* __restrict__ key, int n_cap, int* __restrict__ head)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_cap) return;
+    const bool h = (t == 0) || ((uint32_t)(key[t] >> 32) != (uint32_t)(key[t - 1] >> 32));
+    head[t] = h ? t : 0;
+}
+
+// stage 2: rank keys (niching.cu:114-139); stage 3: niching keys (:157-178)
+__global__ void nich_keys23(uint64_t* __restrict__ key, const int* __restrict__ run_start,
+                            const int* __restrict__ sizes, const int* __restrict__ rho, int H,
+                            uint64_t seed, const unsigned long long* __restrict__ offset, int stage)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nl = sizes[1];
+    if (t >= nl) return;
+    const uint32_t ref = (uint32_t)(key[t] >> 32);
+    const int r_i = (int)ref;
+    const int rho_r = (r_i >= 0 && r_i < H) ? rho[r_i] : 0;
+    const int rank = t - run_start[t];
+    if (stage == 2) {
+        const uint32_t rnd = splitmix_u32(*offset + (uint64_t)t, seed);
+        const uint32_t low = (rho_r == 0 && rank == 0) ? 0u : (rnd | 1u);
+        key[t] = ((uint64_t)ref << 32) | low;
+    } else {
+        const uint32_t rnd = splitmix_u32(*offset + (uint64_t)nl + (uint64_t)t, seed);
+        key[t] = ((uint64_t)(uint32_t)(rho_r + rank) << 32) | rnd;
+    }
+}
+
+__global__ void nich_select(const int* __restrict__ vals, const int* __restrict__ nds_gidx,
+                            const int* __restrict__ sizes, int* __restrict__ selected,
+                            unsigned long long* __restrict__ offset)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int np = sizes[0], nl = sizes[1], nrem = sizes[2];
+    if (i < nrem && i < nl) selected[np + i] = nds_gidx[np + vals[i]];
+    if (i == 0) *offset += 2ull * (unsigned long long)nl;
+}
+
+// ---------------------------------------------------------------------------
+// survivors
+// ---------------------------------------------------------------------------
+
+__global__ void flags_set(const int* __restrict__ sel, int count, int* __restrict__ flags)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) flags[sel[i]] = 1;
+}
+
+__global__ void gather_fronts(const int* __restrict__ surv, int N, const int* __restrict__ fronts,
+                              int* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) out[i] = fronts[surv[i]];
+}
+
+int sm_count(int device)
+{
+    static int cached[64] = {0};
+    if (device >= 0 && device < 64 && cached[device]) return cached[device];
+    int s = 148;
+    cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, device);
+    if (device >= 0 && device < 64) cached[device] = s;
+    return s;
+}
+
+}  // namespace
+
+int run_extract(Workspace& ws, const int* fronts, int n, const int* d_max_front, int N,
+                int* nds_gidx, int* sizes, cudaStream_t stream)
+{
+    return run_compaction(FrontClass{fronts, d_max_front}, n, ws.chunk_counts, N, nds_gidx, sizes,
+                          stream);
+}
+
+int run_ideal(const float* objs, int stride, int M, int n, const float* prev, float* ideal_out,
+              cudaStream_t stream)
+{
+    ideal_kernel<<<M, 512, 0, stream>>>(objs, stride, n, prev, ideal_out);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+int run_normalize_split(Workspace& ws, const SplitPop& pop, const int* nds_gidx, const int* sizes,
+                        const float* ideal, int M, cudaStream_t stream)
+{
+    return dispatch_norm(ws, pop, nds_gidx, sizes, ideal, M, 1, pop.n, nullptr, stream);
+}
+
+// Normalisation of a contiguous (M, n) array in place (stage entry point).
+int run_normalize_inplace(Workspace& ws, float* objs, const float* ideal, int M, int n,
+                          float* rcp_out, int* extreme_out, cudaStream_t stream)
+{
+    if (n > ws.n_max || M > ws.m_max || M < 1)
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "normalize: n=%d M=%d exceed the workspace", n, M);
+    // copy into the workspace layout (stride n_max), normalise, copy back scaled
+    for (int m = 0; m < M; ++m)
+        MOEA_CUDA_TRY(cudaMemcpyAsync(ws.nds_objs + (size_t)m * ws.n_max, objs + (size_t)m * n,
+                                      sizeof(float) * n, cudaMemcpyDeviceToDevice, stream));
+    int hs[4] = {0, n, 0, n};
+    MOEA_CUDA_TRY(cudaMemcpyAsync(ws.sizes, hs, sizeof(hs), cudaMemcpyHostToDevice, stream));
+    SplitPop none{};
+    MOEA_TRY(dispatch_norm(ws, none, nullptr, ws.sizes, ideal, M, 0, n, nullptr, stream));
+    norm_scale<<<ceil_div(n, 256), 256, 0, stream>>>(ws.nds_objs, ws.n_max, ws.sizes + 3, M, ws.rcp_b);
+    for (int m = 0; m < M; ++m)
+        MOEA_CUDA_TRY(cudaMemcpyAsync(objs + (size_t)m * n, ws.nds_objs + (size_t)m * ws.n_max,
+                                      sizeof(float) * n, cudaMemcpyDeviceToDevice, stream));
+    MOEA_CUDA_TRY(cudaMemcpyAsync(rcp_out, ws.rcp_b, sizeof(float) * M, cudaMemcpyDeviceToDevice, stream));
+    if (extreme_out)
+        MOEA_CUDA_TRY(cudaMemcpyAsync(extreme_out, ws.extreme, sizeof(int) * M,
+                                      cudaMemcpyDeviceToDevice, stream));
+    return MOEA_OK;
+}
+
+int run_associate(Workspace& ws, const float* x, int x_stride, const float* scale,
+                  const float* refs, int M, const int* d_n, int n_cap, int H, int* idx,
+                  float* dist, int mode, cudaStream_t stream)
+{
+    (void)mode;
+    if (n_cap <= 0) return MOEA_OK;
+    if (H <= 0) return set_error(MOEA_ERR_INVALID_ARGUMENT, "associate: no directions");
+    assoc_reset<<<ceil_div(n_cap, 256), 256, 0, stream>>>(ws.assoc_best, n_cap);
+    const int sms = sm_count(ws.device);
+    switch (M) {
+#define MOEA_ASSOC_CASE(K) case K: launch_assoc<K>(x, x_stride, scale, refs, H, d_n, n_cap, ws.assoc_best, sms, stream); break;
+    MOEA_ASSOC_CASE(1) MOEA_ASSOC_CASE(2) MOEA_ASSOC_CASE(3) MOEA_ASSOC_CASE(4)
+    MOEA_ASSOC_CASE(5) MOEA_ASSOC_CASE(6) MOEA_ASSOC_CASE(7) MOEA_ASSOC_CASE(8)
+    MOEA_ASSOC_CASE(9) MOEA_ASSOC_CASE(10) MOEA_ASSOC_CASE(11) MOEA_ASSOC_CASE(12)
+    MOEA_ASSOC_CASE(13) MOEA_ASSOC_CASE(14) MOEA_ASSOC_CASE(15) MOEA_ASSOC_CASE(16)
+#undef MOEA_ASSOC_CASE
+    default: return set_error(MOEA_ERR_UNSUPPORTED, "associate: M=%d", M);
+    }
+    MOEA_CUDA_TRY(cudaGetLastError());
+    assoc_finish<<<ceil_div(n_cap, 256), 256, 0, stream>>>(ws.assoc_best, d_n, idx, dist);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+int run_niching(Workspace& ws, uint64_t seed, const int* nds_gidx, const float* dist,
+                const int* idx, const int* sizes, int H, int N, int* selected,
+                cudaStream_t stream)
+{
+    const int n_cap = ws.n_max < 2 * N ? ws.n_max : 2 * N;
+    const int T = 256, G = ceil_div(n_cap, T);
+    MOEA_CUDA_TRY(cudaMemsetAsync(ws.rho, 0, sizeof(int) * (size_t)H, stream));
+    nich_prior<<<G, T, 0, stream>>>(nds_gidx, idx, sizes, H, ws.rho, selected);
+    nich_keys1<<<G, T, 0, stream>>>(idx, dist, sizes, n_cap, ws.key64[0], ws.sel_vals[0]);
+    size_t tmp = ws.cub_bytes;
+    for (int stage = 1; stage <= 3; ++stage) {
+        MOEA_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp, tmp, ws.key64[0], ws.key64[1],
+                                                      ws.sel_vals[0], ws.sel_vals[1], n_cap, 0, 64,
+                                                      stream));
+        std::swap(ws.key64[0], ws.key64[1]);
+        std::swap(ws.sel_vals[0], ws.sel_vals[1]);
+        if (stage == 3) break;
+        nich_heads<<<G, T, 0, stream>>>(ws.key64[0], n_cap, ws.head);
+        MOEA_CUDA_TRY(cub::DeviceScan::InclusiveScan(ws.cub_tmp, tmp, ws.head, ws.run_start,
+                                                     cub::Max(), n_cap, stream));
+        nich_keys23<<<G, T, 0, stream>>>(ws.key64[0], ws.run_start, sizes, ws.rho, H, seed,
+                                         ws.offset_dev, stage + 1);
+    }
+    nich_select<<<G, T, 0, stream>>>(ws.sel_vals[0], nds_gidx, sizes, selected, ws.offset_dev);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+int run_flag_compaction(Workspace& ws, int n, int* out, cudaStream_t stream)
+{
+    return run_compaction(FlagClass{ws.flags}, n, ws.chunk_counts, 0, out, nullptr, stream);
+}
+
+int run_order_selection(Workspace& ws, const int* selected, int count, int n_mix,
+                        int* out_sorted, cudaStream_t stream)
+{
+    MOEA_CUDA_TRY(cudaMemsetAsync(ws.flags, 0, sizeof(int) * (size_t)n_mix, stream));
+    flags_set<<<ceil_div(count, 256), 256, 0, stream>>>(selected, count, ws.flags);
+    return run_compaction(FlagClass{ws.flags}, n_mix, ws.chunk_counts, 0, out_sorted, nullptr,
+                          stream);
+}
+
+// One NSGA-III environmental selection on the split population.
+int run_nsga3_select(Workspace& ws, const SplitPop& pop, int M, int N, const float* refs, int H,
+                     uint64_t seed, float* ideal_last, int* survivors, int* survivor_fronts,
+                     int assoc_mode, cudaStream_t stream, const SplitPop* sort_pop)
+{
+    const int n_mix = pop.n;
+    // the sort may see quantised violations (cv_quantization.cu), the rest the raw ones
+    MOEA_TRY(run_ndsort(ws, sort_pop ? *sort_pop : pop, M, N, ws.fronts, stream));
+    MOEA_TRY(run_extract(ws, ws.fronts, n_mix, ws.counters + 2, N, ws.nds_gidx, ws.sizes, stream));
+    // ideal point: running minimum over the offspring objectives (ideal_point.cu:97-165)
+    MOEA_TRY(run_ideal(pop.objs_b, pop.stride_b, M, n_mix - pop.n_a, ideal_last, ideal_last, stream));
+    stage_mark("select.extract_ideal", stream);
+    MOEA_TRY(run_normalize_split(ws, pop, ws.nds_gidx, ws.sizes, ideal_last, M, stream));
+    stage_mark("select.normalize", stream);
+    MOEA_TRY(run_associate(ws, ws.nds_objs, ws.n_max, ws.rcp_b, refs, M, ws.sizes + 3, n_mix, H,
+                           ws.assoc_idx, ws.assoc_dist, assoc_mode, stream));
+    stage_mark("select.associate", stream);
+    MOEA_TRY(run_niching(ws, seed, ws.nds_gidx, ws.assoc_dist, ws.assoc_idx, ws.sizes, H, N,
+                         ws.selected, stream));
+    stage_mark("select.niching", stream);
+    MOEA_TRY(run_order_selection(ws, ws.selected, N, n_mix, survivors, stream));
+    if (survivor_fronts) {
+        gather_fronts<<<ceil_div(N, 256), 256, 0, stream>>>(survivors, N, ws.fronts, survivor_fronts);
+        MOEA_CUDA_TRY(cudaGetLastError());
+    }
+    return MOEA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CV quantisation (cv_quantization.cu:11-95)
+// ---------------------------------------------------------------------------
+
+__global__ void cv_quant_kernel(const float* __restrict__ cv, float* __restrict__ out, int n,
+                                float eps, float clip, float inv_clip_log, float log_alpha,
+                                float inv_clip, int bins)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float raw = cv[i];
+    const float u = fminf(fmaxf(raw, 0.0f), clip);
+    const float x = (log_alpha > 0.0f) ? log1pf(log_alpha * u) * inv_clip_log : u * inv_clip;
+    int bin = 1 + __float2int_rd(x * __int2float_rn(bins));
+    bin = max(1, min(bins, bin));
+    const bool infeas = (eps == 0.0f) ? (raw != 0.0f) : (raw > eps);
+    out[i] = infeas ? __int2float_rn(bin) : 0.0f;
+}
+
+int run_quantize_cv(const float* cv, float* out, int n, float eps, float clip, float log_alpha,
+                    int bins, cudaStream_t stream)
+{
+    if (n <= 0) return MOEA_OK;
+    const float inv_clip = 1.0f / clip;
+    const float inv_clip_log = (log_alpha > 0.0f) ? 1.0f / log1pf(log_alpha * clip) : 0.0f;
+    cv_quant_kernel<<<ceil_div(n, 256), 256, 0, stream>>>(cv, out, n, eps, clip, inv_clip_log,
+                                                          log_alpha, inv_clip, bins);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+}  // namespace moea

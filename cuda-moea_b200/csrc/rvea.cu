@@ -1,0 +1,493 @@
+// RVEA environmental selection and direction adaptation for sm_100a.
+//
+// Reference (paths relative to python/csrc/native/src/):
+//   translation   selection/rvea/kernels/objective_translation.cu:15-167
+//   partition     selection/rvea/kernels/reference_partition.cu:48-439
+//   APD, gamma    selection/rvea/kernels/angle_penalized_distance.cu:45-417
+//   elitism       selection/rvea/kernels/elitism_selection.cu:68-419
+//   update        selection/rvea/kernels/rvea_population_update.cu:185-293
+//   adaptation    reference/rvea_reference_adaptation.cu:20-317
+//   front 0       selection/rvea/kernels/front_zero.cu:200-293
+// The reference reads the winner count back to the host every generation
+// (elitism_selection.cu:256-257); here the count stays on the device and the
+// truncation, the active count and the sentinel rows are decided there.
+#include <cub/cub.cuh>
+
+#include <math_constants.h>
+
+#include "internal.cuh"
+
+namespace moea {
+
+int run_problem(int kind, const float* x, int N, int D, int M, float* objs, float* cv,
+                cudaStream_t s);
+
+namespace {
+
+constexpr float kMetricMax = 1e30f;
+constexpr float kSentinel = 1e15f;
+
+__global__ void __launch_bounds__(512) zmin_kernel(SplitPop pop, float* __restrict__ zmin)
+{
+    const int m = blockIdx.x;
+    float v = CUDART_INF_F;
+    for (int i = threadIdx.x; i < pop.n; i += blockDim.x) v = fminf(v, pop.obj(m, i));
+    __shared__ float sh[16];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_down_sync(0xFFFFFFFFu, v, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float r = CUDART_INF_F;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fminf(r, sh[w]);
+        zmin[m] = r;
+    }
+}
+
+__global__ void translate_kernel(SplitPop pop, int M, const float* __restrict__ zmin,
+                                 float* __restrict__ t, int t_stride)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pop.n) return;
+    for (int m = 0; m < M; ++m) t[(size_t)m * t_stride + i] = fmaxf(pop.obj(m, i) - zmin[m], 1e-32f);
+}
+
+template <int M>
+__global__ void __launch_bounds__(256)
+partition_kernel(const float* __restrict__ t, int t_stride, int n, const float* __restrict__ refs,
+                 int K, const int* __restrict__ d_active, int n_active_host, int n_parent,
+                 float* __restrict__ theta, int* __restrict__ idx)
+{
+    constexpr int kPartTile = (M <= 8) ? 1024 : 512;
+    __shared__ float s_ref[M][kPartTile];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    float x[M];
+    float sqr = 0.f;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        const float v = valid ? t[(size_t)m * t_stride + i] : 0.f;
+        x[m] = v;
+        sqr = fmaf(v, v, sqr);
+    }
+    const float inv_norm = rsqrtf(sqr + 1e-12f);
+    float best = -CUDART_INF_F;
+    int bj = -1;
+    for (int j0 = 0; j0 < K; j0 += kPartTile) {
+        const int cnt = min(kPartTile, K - j0);
+        __syncthreads();
+        for (int u = threadIdx.x; u < cnt; u += blockDim.x)
+#pragma unroll
+            for (int m = 0; m < M; ++m) s_ref[m][u] = refs[(size_t)m * K + j0 + u];
+        __syncthreads();
+        if (!valid) continue;
+        for (int u = 0; u < cnt; ++u) {
+            float dot = 0.f;
+#pragma unroll
+            for (int m = 0; m < M; ++m) dot = fmaf(x[m], s_ref[m][u], dot);
+            const float c = dot * inv_norm;
+            if (c > best) { best = c; bj = j0 + u; }
+        }
+    }
+    if (!valid) return;
+    theta[i] = (best > -CUDART_INF_F) ? acosf(fminf(fmaxf(best, 0.f), 1.f)) : CUDART_INF_F;
+    const int n_active = d_active ? *d_active : n_active_host;
+    idx[i] = (i >= n_active && i < n_parent) ? K : bj;
+}
+
+template <int M>
+__global__ void gamma_kernel(const float* __restrict__ refs, int K, float* __restrict__ gamma)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= K) return;
+    if (K == 1) { gamma[j] = CUDART_PI_F; return; }
+    float q[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) q[m] = refs[(size_t)m * K + j];
+    float mx = -CUDART_INF_F;
+    for (int k = 0; k < K; ++k) {
+        if (k == j) continue;
+        float dot = 0.f;
+#pragma unroll
+        for (int m = 0; m < M; ++m) dot = fmaf(q[m], __ldg(refs + (size_t)m * K + k), dot);
+        mx = fmaxf(mx, dot);
+    }
+    gamma[j] = (mx > -CUDART_INF_F) ? acosf(fminf(fmaxf(mx, 0.f), 1.f)) : CUDART_PI_F;
+}
+
+template <int M>
+__global__ void apd_kernel(const float* __restrict__ t, int t_stride, int n,
+                           const float* __restrict__ theta, const float* __restrict__ gamma,
+                           const int* __restrict__ idx, int K, const float* __restrict__ ps_table,
+                           const int* __restrict__ d_gen, float ps_host, float* __restrict__ apd)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float penalty_scale = ps_table ? ps_table[*d_gen] : ps_host;
+    float norm_sq = 0.f;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        const float v = t[(size_t)m * t_stride + i];
+        norm_sq = fmaf(v, v, norm_sq);
+    }
+    const float norm = sqrtf(norm_sq);
+    if (norm > 1e-12f) {
+        const int r = idx[i];
+        if (r < 0 || r >= K) { apd[i] = kMetricMax; return; }
+        const float theta_safe = fminf(fmaxf(theta[i], 0.f), CUDART_PI_F);
+        const float gamma_safe = fmaxf(gamma[r], 1e-6f);
+        const float a = (1.f + penalty_scale * theta_safe / gamma_safe) * norm;
+        apd[i] = (!isfinite(a) || a < 0.f) ? kMetricMax : a;
+    } else {
+        apd[i] = 0.f;
+    }
+}
+
+__device__ __forceinline__ uint32_t metric_bits(float cv, float apd, uint32_t& flag)
+{
+    const bool feas = cv <= 1e-8f;
+    float m = feas ? apd : cv;
+    if (!(isfinite(m) && m >= 0.f)) m = kMetricMax;
+    flag = feas ? 0u : 1u;
+    return __float_as_uint(m) & 0x7FFFFFFFu;
+}
+
+__global__ void elite_keys(const int* __restrict__ idx, SplitPop pop, const float* __restrict__ apd,
+                           uint64_t* __restrict__ key, int* __restrict__ val)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pop.n) return;
+    uint32_t flag;
+    const uint32_t mb = metric_bits(pop.cvv(i), apd[i], flag);
+    key[i] = ((uint64_t)(uint32_t)idx[i] << 32) | ((uint64_t)flag << 31) | mb;
+    val[i] = i;
+}
+
+__global__ void elite_heads(const uint64_t* __restrict__ key, int n, int* __restrict__ head)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    head[t] = (t == 0 || (uint32_t)(key[t] >> 32) != (uint32_t)(key[t - 1] >> 32)) ? t : 0;
+}
+
+__global__ void elite_winners(const uint64_t* __restrict__ key, const int* __restrict__ val,
+                              const int* __restrict__ run_start, int n, int K,
+                              int* __restrict__ win_flag, int* __restrict__ win_count)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    bool w = false;
+    if (t < n) {
+        const int ref = (int)(uint32_t)(key[t] >> 32);
+        w = (t == run_start[t]) && ref >= 0 && ref < K;
+        win_flag[val[t]] = w ? 1 : 0;
+    }
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, w);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(win_count, __popc(m));
+}
+
+__global__ void elite_trunc_keys(const int* __restrict__ win_flag, SplitPop pop,
+                                 const float* __restrict__ apd, uint64_t* __restrict__ key,
+                                 int* __restrict__ val)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pop.n) return;
+    if (win_flag[i]) {
+        uint32_t flag;
+        const uint32_t mb = metric_bits(pop.cvv(i), apd[i], flag);
+        key[i] = ((uint64_t)flag << 63) | ((uint64_t)mb << 32) | (uint32_t)i;
+    } else {
+        key[i] = ~0ull;
+    }
+    val[i] = i;
+}
+
+// selected = first N of the first sort when there is no winner, else the
+// first min(W, N) winners in truncation order; active = that count.
+__global__ void elite_select(const int* __restrict__ first_vals, const int* __restrict__ trunc_vals,
+                             const int* __restrict__ win_count, int N, int* __restrict__ selected,
+                             int* __restrict__ active, int* __restrict__ flags)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int W = *win_count;
+    const int a = (W > 0) ? min(W, N) : N;
+    if (i == 0) *active = a;
+    if (i < a) {
+        const int s = (W > 0) ? trunc_vals[i] : first_vals[i];
+        selected[i] = s;
+        flags[s] = 1;
+    }
+}
+
+// Next population: active rows gathered, the rest sentinel rows.
+__global__ void rvea_update(SplitPop pop, const float* __restrict__ vars_a,
+                            const float* __restrict__ vars_b, const int* __restrict__ survivors,
+                            const int* __restrict__ d_active, int N, int D, int M,
+                            float* __restrict__ vars, float* __restrict__ objs,
+                            float* __restrict__ cv)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int active = *d_active;
+    if (e < (long long)N * D) {
+        const int r = (int)(e / D), d = (int)(e % D);
+        float v;
+        if (r < active) {
+            const int s = survivors[r];
+            v = (s < pop.n_a) ? vars_a[(size_t)s * D + d] : vars_b[(size_t)(s - pop.n_a) * D + d];
+        } else {
+            v = CUDART_NAN_F;
+        }
+        vars[e] = v;
+    }
+    if (e < N) {
+        const int r = (int)e;
+        if (r < active) {
+            const int s = survivors[r];
+            for (int m = 0; m < M; ++m) objs[(size_t)m * N + r] = pop.obj(m, s);
+            cv[r] = pop.cvv(s);
+        } else {
+            for (int m = 0; m < M; ++m) objs[(size_t)m * N + r] = kSentinel;
+            cv[r] = kSentinel;
+        }
+    }
+}
+
+__global__ void zrange_kernel(const float* __restrict__ objs, int stride, const int* __restrict__ d_n,
+                              int n_host, float* __restrict__ range)
+{
+    const int m = blockIdx.x;
+    const int n = d_n ? *d_n : n_host;
+    float lo = CUDART_INF_F, hi = -CUDART_INF_F;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float v = objs[(size_t)m * stride + i];
+        lo = fminf(lo, v);
+        hi = fmaxf(hi, v);
+    }
+    __shared__ float sl[32], sh[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fminf(lo, __shfl_down_sync(0xFFFFFFFFu, lo, o));
+        hi = fmaxf(hi, __shfl_down_sync(0xFFFFFFFFu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) { sl[threadIdx.x >> 5] = lo; sh[threadIdx.x >> 5] = hi; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { lo = fminf(lo, sl[w]); hi = fmaxf(hi, sh[w]); }
+        float r = hi - lo;
+        if (!isfinite(r) || r < 1e-12f) r = 1e-12f;
+        range[m] = r;
+    }
+}
+
+template <int M>
+__global__ void adapt_kernel(const float* __restrict__ v0, const float* __restrict__ range, int K,
+                             float* __restrict__ v)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= K) return;
+    float base[M], sc[M], bs = 0.f, ss = 0.f;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        float b = v0[(size_t)m * K + j];
+        if (!isfinite(b)) b = 0.f;
+        base[m] = b;
+        bs = fmaf(b, b, bs);
+        float s = b * range[m];
+        if (!isfinite(s)) s = 0.f;
+        sc[m] = s;
+        ss = fmaf(s, s, ss);
+    }
+    const bool us = isfinite(ss) && (ss > 1e-12f);
+    const bool ub = isfinite(bs) && (bs > 1e-12f);
+    const float is = us ? rsqrtf(ss) : 0.f;
+    const float ib = ub ? rsqrtf(bs) : 0.f;
+#pragma unroll
+    for (int m = 0; m < M; ++m)
+        v[(size_t)m * K + j] = us ? sc[m] * is : (ub ? base[m] * ib : (m == 0 ? 1.f : 0.f));
+}
+
+#define MOEA_DISPATCH_M(M, CALL)                                                      \
+    switch (M) {                                                                      \
+    case 1: { constexpr int MM = 1; CALL; } break;                                   \
+    case 2: { constexpr int MM = 2; CALL; } break;                                   \
+    case 3: { constexpr int MM = 3; CALL; } break;                                   \
+    case 4: { constexpr int MM = 4; CALL; } break;                                   \
+    case 5: { constexpr int MM = 5; CALL; } break;                                   \
+    case 6: { constexpr int MM = 6; CALL; } break;                                   \
+    case 7: { constexpr int MM = 7; CALL; } break;                                   \
+    case 8: { constexpr int MM = 8; CALL; } break;                                   \
+    case 9: { constexpr int MM = 9; CALL; } break;                                   \
+    case 10: { constexpr int MM = 10; CALL; } break;                                 \
+    case 11: { constexpr int MM = 11; CALL; } break;                                 \
+    case 12: { constexpr int MM = 12; CALL; } break;                                 \
+    case 13: { constexpr int MM = 13; CALL; } break;                                 \
+    case 14: { constexpr int MM = 14; CALL; } break;                                 \
+    case 15: { constexpr int MM = 15; CALL; } break;                                 \
+    case 16: { constexpr int MM = 16; CALL; } break;                                 \
+    default: return set_error(MOEA_ERR_UNSUPPORTED, "objectives=%d", (M));           \
+    }
+
+}  // namespace
+
+int run_rvea_translate(const SplitPop& pop, int M, float* t, int t_stride, float* zmin,
+                       cudaStream_t s)
+{
+    zmin_kernel<<<M, 512, 0, s>>>(pop, zmin);
+    translate_kernel<<<ceil_div(pop.n, 256), 256, 0, s>>>(pop, M, zmin, t, t_stride);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+int run_rvea_partition(const float* t, int t_stride, int n, const float* refs, int M, int K,
+                       const int* d_active, int n_active, int n_parent, float* theta, int* idx,
+                       cudaStream_t s)
+{
+    MOEA_DISPATCH_M(M, (partition_kernel<MM><<<ceil_div(n, 256), 256, 0, s>>>(
+                           t, t_stride, n, refs, K, d_active, n_active, n_parent, theta, idx)));
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+int run_rvea_gamma(const float* refs, int M, int K, float* gamma, cudaStream_t s)
+{
+    MOEA_DISPATCH_M(M, (gamma_kernel<MM><<<ceil_div(K, 128), 128, 0, s>>>(refs, K, gamma)));
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+int run_rvea_apd(const float* t, int t_stride, int n, const float* theta, const float* gamma,
+                 const int* idx, int M, int K, const float* ps_table, const int* d_gen,
+                 float ps_host, float* apd, cudaStream_t s)
+{
+    MOEA_DISPATCH_M(M, (apd_kernel<MM><<<ceil_div(n, 256), 256, 0, s>>>(
+                           t, t_stride, n, theta, gamma, idx, K, ps_table, d_gen, ps_host, apd)));
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+float rvea_penalty_scale(int M, int gen, int max_gen, float alpha)
+{
+    const float iter_total = std::fmax(static_cast<float>(max_gen), 1.0f);
+    const float progress = std::fmin(std::fmax(static_cast<float>(gen) / iter_total, 0.0f), 1.0f);
+    return static_cast<float>(M) * std::pow(progress, alpha);
+}
+
+// Elitism on the split population; writes the ascending survivor set into
+// survivors (first *d_active entries) and the active count to d_active.
+int run_rvea_elitism(Workspace& ws, const int* idx, const SplitPop& pop, const float* apd, int N,
+                     int K, int* survivors, int* d_active, cudaStream_t s)
+{
+    const int n = pop.n;
+    const int T = 256, G = ceil_div(n, T);
+    size_t tmp = ws.cub_bytes;
+    int* win_count = ws.counters + 7;
+    MOEA_CUDA_TRY(cudaMemsetAsync(win_count, 0, sizeof(int), s));
+    elite_keys<<<G, T, 0, s>>>(idx, pop, apd, ws.key64[0], ws.sel_vals[0]);
+    MOEA_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp, tmp, ws.key64[0], ws.key64[1],
+                                                  ws.sel_vals[0], ws.rank, n, 0, 64, s));
+    elite_heads<<<G, T, 0, s>>>(ws.key64[1], n, ws.head);
+    MOEA_CUDA_TRY(cub::DeviceScan::InclusiveScan(ws.cub_tmp, tmp, ws.head, ws.run_start, cub::Max(),
+                                                 n, s));
+    elite_winners<<<G, T, 0, s>>>(ws.key64[1], ws.rank, ws.run_start, n, K, ws.blocker, win_count);
+    elite_trunc_keys<<<G, T, 0, s>>>(ws.blocker, pop, apd, ws.key64[0], ws.sel_vals[0]);
+    MOEA_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp, tmp, ws.key64[0], ws.key64[1],
+                                                  ws.sel_vals[0], ws.sel_vals[1], n, 0, 64, s));
+    MOEA_CUDA_TRY(cudaMemsetAsync(ws.flags, 0, sizeof(int) * (size_t)n, s));
+    elite_select<<<ceil_div(N, T), T, 0, s>>>(ws.rank, ws.sel_vals[1], win_count, N, ws.selected,
+                                             d_active, ws.flags);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    // ascending order of the selected set: compaction of the flags
+    return run_flag_compaction(ws, n, survivors, s);
+}
+
+int run_rvea_update(const SplitPop& pop, const float* vars_a, const float* vars_b,
+                    const int* survivors, const int* d_active, int N, int D, int M, float* vars,
+                    float* objs, float* cv, cudaStream_t s)
+{
+    const long long count = (long long)N * D > N ? (long long)N * D : N;
+    rvea_update<<<(int)((count + 255) / 256), 256, 0, s>>>(pop, vars_a, vars_b, survivors, d_active,
+                                                           N, D, M, vars, objs, cv);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+int run_rvea_adapt(const float* v0, const float* objs, int stride, const int* d_active,
+                   int n_active, int M, int K, float* range_tmp, float* v, cudaStream_t s)
+{
+    zrange_kernel<<<M, 512, 0, s>>>(objs, stride, d_active, n_active, range_tmp);
+    MOEA_DISPATCH_M(M, (adapt_kernel<MM><<<ceil_div(K, 256), 256, 0, s>>>(v0, range_tmp, K, v)));
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+}  // namespace moea
+
+using namespace moea;
+
+extern "C" {
+
+moea_status moea_rvea_translate(moea_workspace* w, const float* d_objs, int M, int n, float* d_out,
+                                float* d_zmin, void* stream)
+{
+    if (!d_objs || !d_out || !d_zmin || n < 1 || M < 1 || M > kMaxObjectives)
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "rvea_translate: bad arguments");
+    (void)w;
+    return run_rvea_translate(merged_view(d_objs, d_objs, n), M, d_out, n, d_zmin, (cudaStream_t)stream);
+}
+
+moea_status moea_rvea_partition(moea_workspace* w, const float* d_t, const float* d_refs, int M,
+                                int n, int K, int n_active, int n_parent, float* d_theta,
+                                int* d_idx, void* stream)
+{
+    (void)w;
+    if (!d_t || !d_refs || !d_theta || !d_idx || n < 1 || K < 1)
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "rvea_partition: bad arguments");
+    return run_rvea_partition(d_t, n, n, d_refs, M, K, nullptr, n_active, n_parent, d_theta, d_idx,
+                              (cudaStream_t)stream);
+}
+
+moea_status moea_rvea_gamma(moea_workspace* w, const float* d_refs, int M, int K, float* d_gamma,
+                            void* stream)
+{
+    (void)w;
+    if (!d_refs || !d_gamma || K < 1) return set_error(MOEA_ERR_INVALID_ARGUMENT, "rvea_gamma: bad arguments");
+    return run_rvea_gamma(d_refs, M, K, d_gamma, (cudaStream_t)stream);
+}
+
+moea_status moea_rvea_apd(moea_workspace* w, const float* d_t, const float* d_theta,
+                          const float* d_gamma, const int* d_idx, int M, int n, int K, int gen,
+                          int max_gen, float alpha, float* d_apd, void* stream)
+{
+    (void)w;
+    if (!d_t || !d_theta || !d_gamma || !d_idx || !d_apd || n < 1 || K < 1)
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "rvea_apd: bad arguments");
+    return run_rvea_apd(d_t, n, n, d_theta, d_gamma, d_idx, M, K, nullptr, nullptr,
+                        rvea_penalty_scale(M, gen, max_gen, alpha), d_apd, (cudaStream_t)stream);
+}
+
+moea_status moea_rvea_elitism(moea_workspace* w, const int* d_idx, const float* d_cv,
+                              const float* d_apd, int N, int n_mix, int K, int* d_selected,
+                              int* h_active, void* stream)
+{
+    if (!w || !d_idx || !d_cv || !d_apd || !d_selected || !h_active || N < 1 || n_mix < 1 ||
+        n_mix > w->ws.n_max)
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "rvea_elitism: bad arguments");
+    Workspace& ws = w->ws;
+    const cudaStream_t s = (cudaStream_t)stream;
+    SplitPop pop{d_cv, d_cv, d_cv, d_cv, n_mix, n_mix, n_mix, n_mix};
+    int* d_active = ws.counters + 8;
+    MOEA_TRY(run_rvea_elitism(ws, d_idx, pop, d_apd, N, K, d_selected, d_active, s));
+    MOEA_CUDA_TRY(cudaMemcpyAsync(h_active, d_active, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MOEA_CUDA_TRY(cudaStreamSynchronize(s));
+    return MOEA_OK;
+}
+
+moea_status moea_rvea_adapt(moea_workspace* w, const float* d_v0, const float* d_objs, int M, int K,
+                            int n_active, int n_stride, float* d_v, void* stream)
+{
+    if (!w || !d_v0 || !d_objs || !d_v || K < 1 || n_active < 1 || n_stride < n_active)
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "rvea_adapt: bad arguments");
+    return run_rvea_adapt(d_v0, d_objs, n_stride, nullptr, n_active, M, K, w->ws.ideal_tmp, d_v,
+                          (cudaStream_t)stream);
+}
+
+}  // extern "C"

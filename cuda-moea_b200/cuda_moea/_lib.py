@@ -1,0 +1,147 @@
+"""ctypes binding of libmoea_b200.so (declarations in include/moea_b200.h).
+
+The library is the product: this module only loads it and declares the entry
+points.  There is no CPU fallback -- if the shared object is missing or a call
+fails, an exception is raised.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+_LIB_NAME = "libmoea_b200.so"
+_lib = None
+
+c_int, c_float, c_double = ctypes.c_int, ctypes.c_float, ctypes.c_double
+c_u64, c_u32, c_i64 = ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int64
+c_size_t, vp = ctypes.c_size_t, ctypes.c_void_p
+fp = ctypes.POINTER(ctypes.c_float)
+ip = ctypes.POINTER(ctypes.c_int)
+
+EVALUATE_FN = ctypes.CFUNCTYPE(c_int, vp, vp, vp, vp, c_int, c_int, c_int, c_int, c_int, vp)
+MATING_FN = ctypes.CFUNCTYPE(c_int, vp, vp, vp, vp, vp, c_int, vp, c_int, c_int, c_int, c_int, vp)
+
+MOEA_OK = 0
+ERROR_NAMES = {1: "invalid argument", 2: "CUDA error", 3: "unsupported", 4: "invalid state",
+               5: "device timeout", 6: "out of memory", 7: "callback failed"}
+
+
+class MoeaError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERROR_NAMES.get(code, 'error')} ({code}): {message}")
+        self.code = code
+
+
+class AlgorithmConfig(ctypes.Structure):
+    """moea_algorithm_config (include/moea_b200.h)."""
+    _fields_ = [
+        ("algorithm", c_int), ("population_size", c_int), ("max_generations", c_int),
+        ("device", c_int), ("seed", c_u64), ("stream", vp),
+        ("problem_kind", c_int), ("dimension", c_int), ("objectives", c_int),
+        ("constraint_activation_ratio", c_float), ("h_lower", fp), ("h_upper", fp),
+        ("evaluate", EVALUATE_FN), ("evaluate_user", vp),
+        ("mating", c_int), ("mate", MATING_FN), ("mate_user", vp),
+        ("sbx_eta_initial", c_float), ("sbx_eta_final", c_float),
+        ("sbx_probability", c_float), ("sbx_copy_probability", c_float),
+        ("mutation", c_int), ("pm_eta_initial", c_float), ("pm_eta_final", c_float),
+        ("pm_probability", c_float),
+        ("directions", c_int), ("partitions", c_int), ("adapt_frequency", c_float),
+        ("h_user_directions", fp), ("user_direction_count", c_int),
+        ("normalize_user_directions", c_int),
+        ("sparse_ratio", c_float), ("cv_bins", c_int), ("cv_clip_upper", c_float),
+        ("cv_log_alpha", c_float), ("feasibility_epsilon", c_float),
+        ("association_mode", c_int), ("rvea_alpha", c_float),
+        ("h_initial_population", fp), ("use_graphs", c_int),
+    ]
+
+
+class PopulationViewC(ctypes.Structure):
+    """moea_population_view (include/moea_b200.h)."""
+    _fields_ = [
+        ("d_variables", vp), ("d_objectives", vp), ("d_constraints", vp), ("d_auxiliary", vp),
+        ("auxiliary_count", c_int), ("size", c_int), ("dimension", c_int), ("objectives", c_int),
+        ("active_count", c_int), ("generation", c_int), ("initialized", c_int),
+        ("finished", c_int), ("device", c_int), ("total_ms", c_double),
+        ("kernels_per_generation", c_int), ("graph_active", c_int),
+    ]
+
+
+def library_path() -> Path:
+    override = os.environ.get("MOEA_B200_LIBRARY")
+    if override:
+        return Path(override)
+    return Path(__file__).resolve().parent / _LIB_NAME
+
+
+# (name, restype, argtypes)
+_SIGNATURES = [
+    ("moea_abi_version", c_int, []),
+    ("moea_last_error", ctypes.c_char_p, []),
+    ("moea_workspace_create", c_int, [c_int, c_int, c_int, c_int, ctypes.POINTER(vp)]),
+    ("moea_workspace_destroy", None, [vp]),
+    ("moea_workspace_bytes", c_size_t, [vp]),
+    ("moea_ndsort", c_int, [vp, vp, vp, c_int, c_int, c_int, vp, ip, vp]),
+    ("moea_nds_extract", c_int, [vp, vp, c_int, vp, c_int, vp, vp, vp]),
+    ("moea_ideal_point", c_int, [vp, vp, c_int, c_int, vp, vp]),
+    ("moea_normalize", c_int, [vp, vp, vp, c_int, c_int, vp, vp, vp]),
+    ("moea_associate", c_int, [vp, vp, vp, c_int, c_int, c_int, vp, vp, c_int, vp]),
+    ("moea_niching", c_int, [vp, c_u64, ctypes.POINTER(c_u64), vp, vp, vp, vp, c_int, c_int, vp, vp]),
+    ("moea_nsga3_select", c_int, [vp, vp, vp, c_int, c_int, vp, c_int, c_u64, ctypes.POINTER(c_u64),
+                                  vp, vp, vp, vp, c_int, vp]),
+    ("moea_quantize_cv", c_int, [vp, vp, c_int, c_float, c_float, c_float, c_int, vp]),
+    ("moea_rvea_translate", c_int, [vp, vp, c_int, c_int, vp, vp, vp]),
+    ("moea_rvea_partition", c_int, [vp, vp, vp, c_int, c_int, c_int, c_int, c_int, vp, vp, vp]),
+    ("moea_rvea_gamma", c_int, [vp, vp, c_int, c_int, vp, vp]),
+    ("moea_rvea_apd", c_int, [vp, vp, vp, vp, vp, c_int, c_int, c_int, c_int, c_int, c_float, vp, vp]),
+    ("moea_rvea_elitism", c_int, [vp, vp, vp, vp, c_int, c_int, c_int, vp, ip, vp]),
+    ("moea_rvea_adapt", c_int, [vp, vp, vp, c_int, c_int, c_int, c_int, vp, vp]),
+    ("moea_tournament", c_int, [vp, vp, vp, c_int, vp, vp]),
+    ("moea_sbx", c_int, [vp, vp, vp, vp, vp, vp, vp, c_float, c_float, c_float, c_int, c_int, vp]),
+    ("moea_pm", c_int, [vp, vp, vp, c_float, c_float, c_int, c_int, vp]),
+    ("moea_reproduce", c_int, [vp, vp, vp, c_int, vp, vp, vp, c_int, c_int, c_int, c_int, c_float,
+                               c_float, c_float, c_int, c_float, c_float, c_u64, c_u32, vp]),
+    ("moea_rng_blocks", c_int, [c_u64, c_u32, c_u32, c_i64, vp, vp]),
+    ("moea_problem_evaluate", c_int, [c_int, vp, c_int, c_int, c_int, vp, vp, vp]),
+    ("moea_reference_directions", c_int, [c_int, c_int, c_int, fp, c_size_t, ip]),
+    ("moea_algorithm_config_defaults", None, [ctypes.POINTER(AlgorithmConfig), c_int]),
+    ("moea_algorithm_create", c_int, [ctypes.POINTER(AlgorithmConfig), ctypes.POINTER(vp)]),
+    ("moea_algorithm_destroy", None, [vp]),
+    ("moea_algorithm_initialize", c_int, [vp]),
+    ("moea_algorithm_step", c_int, [vp]),
+    ("moea_algorithm_run", c_int, [vp, ctypes.POINTER(c_double)]),
+    ("moea_algorithm_reset", c_int, [vp]),
+    ("moea_algorithm_synchronize", c_int, [vp]),
+    ("moea_algorithm_finalize", c_int, [vp]),
+    ("moea_algorithm_view", c_int, [vp, ctypes.POINTER(PopulationViewC)]),
+    ("moea_algorithm_directions", c_int, [vp, ctypes.POINTER(vp), ip]),
+    ("moea_algorithm_profile_step", c_int, [vp, ctypes.c_char_p, c_size_t, fp, c_int, ip]),
+    ("moea_algorithm_device_status", c_int, [vp, ip]),
+]
+
+SYMBOLS = [s[0] for s in _SIGNATURES]
+
+
+def lib():
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        path = library_path()
+        if not path.exists():
+            raise ImportError(f"{path} is missing: build it with `python cuda-moea_b200/build.py` "
+                              "(the B200 path has no CPU fallback)")
+        L = ctypes.CDLL(str(path))
+        for name, res, args in _SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        if L.moea_abi_version() != 1:
+            raise ImportError("libmoea_b200 ABI mismatch")
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != MOEA_OK:
+        msg = lib().moea_last_error()
+        raise MoeaError(status, msg.decode() if msg else "")

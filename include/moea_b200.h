@@ -1,0 +1,318 @@
+/*
+ * moea_b200 -- C ABI of the B200 implementation of the CUDA-MOEA generation
+ * hot path (NSGA-III / RVEA environmental selection, SBX, polynomial mutation,
+ * tournament/random mating and DTLZ evaluation).
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Pointers named d_* are CUDA device
+ *     pointers, h_* are host pointers.  `stream` is a cudaStream_t passed as
+ *     void* (NULL = legacy default stream).  All device work is stream-ordered.
+ *   - Layouts follow the reference: variables (N,D) row-major, objectives (M,N)
+ *     objective-major, constraint violation (N,), bounds interleaved
+ *     [lb0,ub0,lb1,ub1,...], reference directions (M,H) objective-major.
+ *   - Every function returns a moea_status; the message of the last failure on
+ *     the calling thread is available from moea_last_error().  Nothing in this
+ *     library calls exit() (the reference's CUDA_CHECK does,
+ *     nat/include/cuda_moea/core/cuda/cuda_utils.cuh:16-22).
+ *
+ * Reference paths below are relative to python/csrc/native/ of CUDA-MOEA.
+ */
+#ifndef MOEA_B200_H
+#define MOEA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MOEA_ABI_VERSION 1
+
+typedef int moea_status;
+enum {
+    MOEA_OK = 0,
+    MOEA_ERR_INVALID_ARGUMENT = 1, /* reference: std::invalid_argument */
+    MOEA_ERR_CUDA = 2,             /* CUDA runtime error */
+    MOEA_ERR_UNSUPPORTED = 3,      /* configuration outside what the kernels support */
+    MOEA_ERR_STATE = 4,            /* reference: std::logic_error */
+    MOEA_ERR_DEVICE_TIMEOUT = 5,   /* a bounded device-side wait gave up */
+    MOEA_ERR_OUT_OF_MEMORY = 6,
+    MOEA_ERR_CALLBACK = 7          /* a user callback reported failure */
+};
+
+/* Version of this ABI (MOEA_ABI_VERSION). */
+int moea_abi_version(void);
+/* Message of the last failure on the calling thread ("" if none). */
+const char* moea_last_error(void);
+
+/* ========================================================================
+ * Workspace for the stage-level entry points.  Owns the device scratch a
+ * stage needs (dominance rows, sort buffers, partial reductions).  Replaces
+ * the per-generation pool allocations of the reference
+ * (nat/src/selection/nsga3/kernels/dynamic_workspace.cu:3-125).
+ * ====================================================================== */
+typedef struct moea_workspace moea_workspace;
+
+/* max_points: largest merged population (2N); max_objectives <= 16;
+ * max_directions: largest reference-direction count. */
+moea_status moea_workspace_create(int device, int max_points, int max_objectives,
+                                  int max_directions, moea_workspace** out);
+void moea_workspace_destroy(moea_workspace* ws);
+/* Bytes of device memory held by the workspace. */
+size_t moea_workspace_bytes(const moea_workspace* ws);
+
+/* ========================================================================
+ * Stage-level entry points (one hot-path stage each).
+ * ====================================================================== */
+
+/* Constraint-dominance non-dominated sort of n points with the reference stop
+ * rule: fronts are peeled until >= target points are assigned; later points
+ * get -1.  d_fronts (n) receives front indices; *h_max_front the index of the
+ * last (partially selected) front.  Synchronises the stream before returning.
+ * Replaces run_ndsort / run_ndsort_init
+ * (nat/src/selection/nsga3/kernels/non_dominated_sort.cu:1337, :1407). */
+moea_status moea_ndsort(moea_workspace* ws, const float* d_cv, const float* d_objs,
+                        int M, int n, int target, int* d_fronts, int* h_max_front,
+                        void* stream);
+
+/* Prior/last-front sizes and the [prior; last] ascending-index compaction.
+ * d_sizes receives {N_prior, N_last, N_rem, N_nds}; d_nds_gidx (n_mix).
+ * max_front is read from d_max_front.  Replaces get_nds_mask_size +
+ * extract_ndsfit_mskidx (non_dominated_sort.cu:1636, :1720). */
+moea_status moea_nds_extract(moea_workspace* ws, const int* d_fronts, int n_mix,
+                             const int* d_max_front, int N, int* d_nds_gidx,
+                             int* d_sizes, void* stream);
+
+/* Per-objective minimum (fminf semantics) of d_objs (M,n) into d_ideal (M).
+ * Replaces get_idpts (nat/src/selection/nsga3/kernels/ideal_point.cu:97). */
+moea_status moea_ideal_point(moea_workspace* ws, const float* d_objs, int M, int n,
+                             float* d_ideal, void* stream);
+
+/* Hyperplane normalisation of d_objs (M,n) in place: translate by d_ideal,
+ * ASF extreme points, FP64 intercept solve with the reference's degeneracy
+ * fallback, sanitise, scale.  d_rcp_b (M) receives the reciprocal intercepts,
+ * d_extreme (M) the extreme-point indices (may be NULL).  Replaces
+ * execute_normalization (nat/src/selection/nsga3/kernels/normalization.cu:1593). */
+moea_status moea_normalize(moea_workspace* ws, float* d_objs, const float* d_ideal, int M,
+                           int n, float* d_rcp_b, int* d_extreme, void* stream);
+
+/* Association of normalised points d_x (M,n) to unit directions d_refs (M,H):
+ * perpendicular distance with the reference's FP32 formula, ties to the
+ * smaller direction index.  mode 0 = plain SIMT kernel, 1 = tensor-core
+ * candidate search with FP32 re-score (same results).  Replaces
+ * execute_association (nat/src/selection/nsga3/kernels/association.cu:586). */
+moea_status moea_associate(moea_workspace* ws, const float* d_x, const float* d_refs, int M,
+                           int n, int H, int* d_idx, float* d_dist, int mode, void* stream);
+
+/* NSGA-III niche selection.  d_sizes as produced by moea_nds_extract; the
+ * tie-break draws use SplitMix64(offset + i, seed) like the reference and
+ * *h_offset is advanced by 2*N_last.  d_selected (N) receives mixed indices
+ * [prior; chosen]. Replaces execute_niching
+ * (nat/src/selection/nsga3/kernels/niching.cu:250). */
+moea_status moea_niching(moea_workspace* ws, uint64_t seed, uint64_t* h_offset,
+                         const int* d_nds_gidx, const float* d_dist, const int* d_idx,
+                         const int* d_sizes, int H, int N, int* d_selected, void* stream);
+
+/* One complete NSGA-III environmental selection over the merged population
+ * (parents are mixed indices [0,N), offspring [N,2N)).  d_ideal_last (M) is
+ * the running ideal point (updated).  Outputs: d_survivors (N, ascending mixed
+ * indices), d_survivor_fronts (N), d_sizes (4).  *h_offset as for
+ * moea_niching.  Replaces NSGA3EnvironmentSelector::select
+ * (nat/src/selection/nsga3/nsga3_environment_selector.cu:289-538). */
+moea_status moea_nsga3_select(moea_workspace* ws, const float* d_mix_cv,
+                              const float* d_mix_objs, int M, int N, const float* d_refs,
+                              int H, uint64_t seed, uint64_t* h_offset, float* d_ideal_last,
+                              int* d_survivors, int* d_survivor_fronts, int* d_sizes,
+                              int assoc_mode, void* stream);
+
+/* Optional CV quantisation (nat/src/selection/nsga3/kernels/cv_quantization.cu:65). */
+moea_status moea_quantize_cv(const float* d_cv, float* d_out, int n, float eps_feas,
+                             float clip_upper, float log_alpha, int bins, void* stream);
+
+/* ---- RVEA ---- */
+/* z_min translation (nat/src/selection/rvea/kernels/objective_translation.cu:125). */
+moea_status moea_rvea_translate(moea_workspace* ws, const float* d_objs, int M, int n,
+                                float* d_out, float* d_zmin, void* stream);
+/* Max-cosine partition with dead parent slots [n_active, n_parent) marked K
+ * (nat/src/selection/rvea/kernels/reference_partition.cu:407). */
+moea_status moea_rvea_partition(moea_workspace* ws, const float* d_t, const float* d_refs,
+                                int M, int n, int K, int n_active, int n_parent,
+                                float* d_theta, int* d_idx, void* stream);
+/* gamma per direction (angle_penalized_distance.cu:387). */
+moea_status moea_rvea_gamma(moea_workspace* ws, const float* d_refs, int M, int K,
+                            float* d_gamma, void* stream);
+/* APD with penalty M*progress^alpha, progress = gen/max_gen clamped
+ * (angle_penalized_distance.cu:159). */
+moea_status moea_rvea_apd(moea_workspace* ws, const float* d_t, const float* d_theta,
+                          const float* d_gamma, const int* d_idx, int M, int n, int K,
+                          int gen, int max_gen, float alpha, float* d_apd, void* stream);
+/* Elitism: per-direction winner, truncation to N; d_selected (N) receives the
+ * survivor set sorted ascending, *h_active the active count
+ * (nat/src/selection/rvea/kernels/elitism_selection.cu:194). */
+moea_status moea_rvea_elitism(moea_workspace* ws, const int* d_idx, const float* d_cv,
+                              const float* d_apd, int N, int n_mix, int K, int* d_selected,
+                              int* h_active, void* stream);
+/* Direction adaptation V = normalize(V0 * (zmax - zmin)) over the first
+ * n_active columns (nat/src/reference/rvea_reference_adaptation.cu:279). */
+moea_status moea_rvea_adapt(moea_workspace* ws, const float* d_v0, const float* d_objs,
+                            int M, int K, int n_active, int n_stride, float* d_v,
+                            void* stream);
+
+/* ---- reproduction ---- */
+/* Tournament winners from explicit candidate pairs d_cand (n,2)
+ * (nat/src/reproduction/mating_selection.cu:11-35, :74). */
+moea_status moea_tournament(const int* d_cand, const int* d_rank, const float* d_cv, int n,
+                            int* d_winners, void* stream);
+/* SBX from explicit draws: d_u (pairs*D,2), d_sign (pairs*D), d_copy (pairs*D)
+ * (nat/src/reproduction/sbx_crossover.cu:20-70, :123). */
+moea_status moea_sbx(const float* d_parents, const int* d_pidx, const float* d_bounds,
+                     const float* d_u, const int* d_sign, const float* d_copy, float* d_off,
+                     float eta, float prob, float copy_prob, int n_off, int D, void* stream);
+/* Polynomial mutation in place from explicit draws d_u (n*D,2)
+ * (nat/src/reproduction/polynomial_mutation.cu:20-60, :95). */
+moea_status moea_pm(float* d_off, const float* d_bounds, const float* d_u, float eta,
+                    float prob, int n, int D, void* stream);
+/* Fused tournament (or random, mating=0) + SBX + PM with in-register Philox
+ * draws for (seed, generation).  d_rank may be NULL for random mating.
+ * d_parent_idx (n_off) receives the chosen parents (may be NULL). */
+moea_status moea_reproduce(const float* d_parents, const float* d_parent_cv,
+                           const int* d_rank, int active, const float* d_bounds,
+                           float* d_off, int* d_parent_idx, int n_parents, int n_off, int D,
+                           int mating, float sbx_eta, float sbx_prob, float sbx_copy_prob,
+                           int mutate, float pm_eta, float pm_prob, uint64_t seed,
+                           uint32_t generation, void* stream);
+/* The raw product draws of moea_reproduce, for checking: d_out (count,4). */
+moea_status moea_rng_blocks(uint64_t seed, uint32_t generation, uint32_t tag, int64_t count,
+                            uint32_t* d_out, void* stream);
+
+/* ---- problems ---- */
+/* Built-in problems (nat/src/problem/dtlz/dtlz_kernels.cu:28-1176): kind
+ * 1..7 DTLZ1-7, 8 ConvexDTLZ2, 9 C1-DTLZ1, 10 C1-DTLZ3, 11 C2-DTLZ2,
+ * 12 C2-ConvexDTLZ2, 13 C3-DTLZ1, 14 C3-DTLZ4, 15 CSDP.  d_objs (M,N),
+ * d_cv (N) (zeros for unconstrained kinds). */
+moea_status moea_problem_evaluate(int kind, const float* d_x, int N, int D, int M,
+                                  float* d_objs, float* d_cv, void* stream);
+
+/* ---- reference directions ---- */
+/* Das-Dennis directions (nat/src/reference/nsga3_reference_generator.cu:153,
+ * :184; rvea_reference_generator.cu:182).  mode 0 = NSGA-III auto layers for
+ * n points, 1 = NSGA-III single layer with n partitions, 2 = RVEA auto
+ * (clamped to >= 1e-6).  *h_count receives the count; h_out (M,count) is
+ * written when non-NULL and capacity (floats) suffices. */
+moea_status moea_reference_directions(int mode, int n, int M, float* h_out, size_t capacity,
+                                      int* h_count);
+
+/* ========================================================================
+ * Algorithm (the NSGA3 / RVEA entry points, Algorithm / AlgorithmBuilder).
+ * Replaces EvolutionaryAlgorithm (nat/src/algorithm/algorithm.cu:104-432)
+ * built by AlgorithmFactory::create (nat/src/factory/algorithm_factory.cu:66).
+ * ====================================================================== */
+typedef struct moea_algorithm moea_algorithm;
+
+enum { MOEA_NSGA3 = 0, MOEA_RVEA = 1 };
+enum { MOEA_MATING_RANDOM = 0, MOEA_MATING_TOURNAMENT = 1, MOEA_MATING_CALLBACK = 2 };
+enum { MOEA_DIRS_DAS_DENNIS = 0, MOEA_DIRS_ADAPTIVE = 1, MOEA_DIRS_USER = 2 };
+
+/* Problem evaluated by the caller (a PythonProblem or a native plugin): writes
+ * objectives (M,N) and constraint violation (N) for d_vars (N,D) on stream.
+ * Returns 0 on success.  generation is -1 for the initial population. */
+typedef int (*moea_evaluate_fn)(void* user, const float* d_vars, float* d_objs, float* d_cv,
+                                int N, int D, int M, int generation, int max_generations,
+                                void* stream);
+/* Mating selection by the caller: writes N parent indices (int32) for the
+ * current parents.  d_rank may be NULL. */
+typedef int (*moea_mating_fn)(void* user, const float* d_vars, const float* d_objs,
+                              const float* d_cv, const int* d_rank, int active, int* d_out,
+                              int N, int D, int M, int generation, void* stream);
+
+typedef struct moea_algorithm_config {
+    int algorithm;            /* MOEA_NSGA3 / MOEA_RVEA */
+    int population_size;
+    int max_generations;
+    int device;
+    uint64_t seed;            /* CudaConfig.seed, default 2887 */
+    void* stream;             /* stream to run on; NULL = an internal stream */
+    /* problem */
+    int problem_kind;         /* 1..15 built-in, 0 = callback */
+    int dimension;
+    int objectives;
+    float constraint_activation_ratio;
+    const float* h_lower;     /* (D) bounds, used for callback problems; NULL = [0,1] */
+    const float* h_upper;
+    moea_evaluate_fn evaluate;
+    void* evaluate_user;
+    /* mating */
+    int mating;               /* MOEA_MATING_* */
+    moea_mating_fn mate;
+    void* mate_user;
+    /* SBX */
+    float sbx_eta_initial, sbx_eta_final, sbx_probability, sbx_copy_probability;
+    /* polynomial mutation (mutation = 0 -> NoMutation) */
+    int mutation;
+    float pm_eta_initial, pm_eta_final, pm_probability;
+    /* reference directions */
+    int directions;           /* MOEA_DIRS_* */
+    int partitions;           /* Das-Dennis partitions (0 = from population size) */
+    float adapt_frequency;    /* AdaptiveRVEADirections.frequency */
+    const float* h_user_directions; /* (M,count) objective-major */
+    int user_direction_count;
+    int normalize_user_directions;
+    /* NSGA-III selector */
+    float sparse_ratio;       /* validated for compatibility; the bitmask path needs no pair buffer */
+    int cv_bins;
+    float cv_clip_upper, cv_log_alpha, feasibility_epsilon;
+    int association_mode;     /* 0 plain, 1 tensor-core candidate search */
+    /* RVEA selector */
+    float rvea_alpha;
+    /* initial population (N,D) row-major on the host, or NULL */
+    const float* h_initial_population;
+    int use_graphs;           /* capture one generation into a CUDA graph when possible */
+} moea_algorithm_config;
+
+/* Fills cfg with the reference defaults (nat/src/factory/algorithm_factory.cu:25-118). */
+void moea_algorithm_config_defaults(moea_algorithm_config* cfg, int algorithm);
+
+moea_status moea_algorithm_create(const moea_algorithm_config* cfg, moea_algorithm** out);
+void moea_algorithm_destroy(moea_algorithm* alg);
+moea_status moea_algorithm_initialize(moea_algorithm* alg);
+moea_status moea_algorithm_step(moea_algorithm* alg);
+/* Runs the remaining generations; *h_total_ms receives the device time of
+ * the loop (CUDA events, like run_device, algorithm.cu:313-329). */
+moea_status moea_algorithm_run(moea_algorithm* alg, double* h_total_ms);
+moea_status moea_algorithm_reset(moea_algorithm* alg);
+moea_status moea_algorithm_synchronize(moea_algorithm* alg);
+/* Runs finalize (front-0 indices for RVEA) before results are read. */
+moea_status moea_algorithm_finalize(moea_algorithm* alg);
+
+typedef struct moea_population_view {
+    float* d_variables;       /* (N,D) */
+    float* d_objectives;      /* (M,N) */
+    float* d_constraints;     /* (N) */
+    const int* d_auxiliary;   /* result indices (fronts for NSGA-III, front-0 for RVEA) */
+    int auxiliary_count;
+    int size, dimension, objectives;
+    int active_count;
+    int generation;
+    int initialized, finished;
+    int device;
+    double total_ms;
+    int kernels_per_generation; /* kernel nodes of the captured generation graph (0 if not captured) */
+    int graph_active;           /* 1 when generations replay a CUDA graph */
+} moea_population_view;
+
+moea_status moea_algorithm_view(moea_algorithm* alg, moea_population_view* out);
+/* Reference directions in use: d_values (M,count). */
+moea_status moea_algorithm_directions(moea_algorithm* alg, const float** d_values, int* count);
+/* Runs one generation with direct launches and CUDA events between its
+ * stages: h_ms[i] is the device time of stage i, h_names the '\n'-separated
+ * stage names (both up to cap / names_cap). */
+moea_status moea_algorithm_profile_step(moea_algorithm* alg, char* h_names, size_t names_cap,
+                                        float* h_ms, int cap, int* h_count);
+/* Device status of the last generation (0 ok); also returned as a status by step. */
+moea_status moea_algorithm_device_status(moea_algorithm* alg, int* h_status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

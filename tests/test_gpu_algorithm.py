@@ -1,0 +1,175 @@
+"""End-to-end runs of NSGA3 / RVEA through the Python API on the GPU: API
+behaviour of the reference (shapes, CUDA tensors, reset, streams), a
+generation-by-generation trajectory check of NSGA-III against the oracle's
+selection, graph replay against direct launches, and solution quality (IGD on
+the analytic DTLZ2 front)."""
+import numpy as np
+import pytest
+import torch
+
+import cuda_moea as cm
+
+pytestmark = pytest.mark.gpu
+
+
+class Sphere(cm.PythonProblem):
+    def __init__(self):
+        super().__init__(4, 2)
+
+    def evaluate(self, variables, context):
+        return torch.stack((variables.square().sum(1), (variables - 1).square().sum(1)), 1)
+
+
+class BiSphere(cm.PythonProblem):
+    """Two shifted spheres with a radius constraint (the reference's BiSphere plugin)."""
+
+    def __init__(self, dimension, offset=1.5, radius=2.0):
+        super().__init__(dimension, 2, -5.0, 5.0, constraints=1)
+        self.offset, self.radius = offset, radius
+
+    def evaluate(self, x, context):
+        f = torch.stack((x.square().sum(1), (x - self.offset).square().sum(1)), 1)
+        return f, (f[:, 0] - self.radius ** 2).clamp_min(0)
+
+
+def igd_dtlz2(objs: torch.Tensor) -> float:
+    ref = torch.from_numpy(__import__("oracle.oracle", fromlist=["x"]).reference_directions(1, 30, 3).T.copy())
+    ref = ref.to(objs.device, torch.float64)  # unit directions lie on the DTLZ2 front
+    d = torch.cdist(ref, objs.to(torch.float64))
+    return float(d.min(1).values.mean())
+
+
+def test_cuda_smoke_python_problem():
+    algorithm = cm.NSGA3(population_size=32, max_generations=2, problem=Sphere(),
+                         enable_warmup=False, print_progress=False)
+    result = algorithm.run()
+    assert tuple(result.variables.shape) == (32, 4)
+    assert tuple(result.objectives.shape) == (32, 2)
+    assert result.variables.is_cuda
+    x = result.variables
+    torch.testing.assert_close(result.objectives,
+                               torch.stack((x.square().sum(1), (x - 1).square().sum(1)), 1))
+
+
+@pytest.mark.parametrize("algorithm", [cm.NSGA3, cm.RVEA])
+@pytest.mark.parametrize("dimension", [7, 129])
+def test_python_problem_streams_reset_lifetime(algorithm, dimension):
+    p = BiSphere(dimension)
+    with torch.cuda.stream(torch.cuda.Stream()):
+        algo = algorithm(problem=p, population_size=32, max_generations=2, enable_warmup=False,
+                         print_progress=False)
+        algo.initialize()
+        for action in (lambda: None, algo.step, algo.reset):
+            action()
+            pop = algo.population
+            valid = torch.isfinite(pop.variables).all(1)
+            assert valid.any()
+            x = pop.variables[valid]
+            f = torch.stack((x.square().sum(1), (x - 1.5).square().sum(1)), 1)
+            torch.testing.assert_close(pop.objectives[valid], f, rtol=2e-5, atol=2e-4)
+            torch.testing.assert_close(pop.constraints[valid], (f[:, 0] - 4).clamp_min(0),
+                                       rtol=2e-5, atol=2e-4)
+        result = algo.run(copy=False)
+        del algo, p
+        assert result.active_count > 0
+        assert torch.isfinite(result.objectives[:result.active_count]).all()
+
+
+def test_nsga3_trajectory_matches_oracle_selection(oracle):
+    """Each generation: offspring from the fused reproduction kernel (same
+    Philox streams as the algorithm), objectives from the problem kernel, then
+    the oracle's NSGA-III selection must reproduce the algorithm's next
+    parents exactly (survivor set, fronts, objectives, niching RNG offset)."""
+    from cuda_moea import stages
+    N, D, M, T, seed = 200, 7, 3, 6, 77
+    algo = cm.NSGA3(population_size=N, max_generations=T, problem=cm.DTLZ1(D, M), seed=seed,
+                    print_progress=False, use_graphs=False)
+    algo.initialize()
+    refs = oracle.reference_directions(0, N, M)
+    pop = algo.population
+    par_x = pop.variables.clone()
+    par_f = pop.objectives.t().contiguous().cpu().numpy()
+    par_cv = pop.constraints.cpu().numpy().copy()
+    ideal = par_f.min(1).astype(np.float32)
+    fronts0, _ = oracle.ndsort(par_cv, par_f, N)
+    rank = torch.from_numpy(fronts0).cuda()
+    bounds = torch.tile(torch.tensor([0.0, 1.0]), (D,)).cuda()
+    dseed = oracle.derive_seed(seed)
+    offset = 0
+    for g in range(T):
+        off_x, _ = stages.reproduce(par_x, torch.from_numpy(par_cv).cuda(), rank, N, bounds, N,
+                                    seed=dseed, generation=g)
+        off_f, off_cv = stages.problem_evaluate(1, off_x, M)
+        mix_f = np.concatenate([par_f, off_f.cpu().numpy()], 1)
+        mix_cv = np.concatenate([par_cv, off_cv.cpu().numpy()])
+        want = oracle.nsga3_select(mix_cv, mix_f, refs, dseed, offset, ideal)
+        offset, ideal = want["offset"], want["ideal"]
+        algo.step()
+        pop = algo.population
+        surv = want["survivors"]
+        mix_x = torch.cat([par_x, off_x]).cpu().numpy()
+        np.testing.assert_array_equal(pop.variables.cpu().numpy(), mix_x[surv])
+        np.testing.assert_array_equal(pop.objectives.t().cpu().numpy(), mix_f[:, surv])
+        par_x = pop.variables.clone()
+        par_f = pop.objectives.t().contiguous().cpu().numpy()
+        par_cv = pop.constraints.cpu().numpy().copy()
+        rank = torch.from_numpy(want["fronts"]).cuda()
+
+
+@pytest.mark.parametrize("kind", ["NSGA3", "RVEA"])
+def test_graph_replay_equals_direct_launches(kind):
+    runs = []
+    for graphs in (True, False):
+        a = cm.Algorithm(kind, population_size=256, max_generations=8, problem=cm.DTLZ2(12, 3),
+                         seed=5, print_progress=False, use_graphs=graphs)
+        r = a.run()
+        runs.append((r.variables.cpu(), r.objectives.cpu(), r.active_count))
+    torch.testing.assert_close(runs[0][0], runs[1][0], rtol=0, atol=0, equal_nan=True)
+    torch.testing.assert_close(runs[0][1], runs[1][1], rtol=0, atol=0, equal_nan=True)
+    assert runs[0][2] == runs[1][2]
+
+
+def test_nsga3_dtlz2_quality():
+    algo = cm.NSGA3(population_size=92, max_generations=100, problem=cm.DTLZ2(12, 3), seed=2887,
+                    print_progress=False)
+    r = algo.run()
+    assert r.total_ms > 0
+    assert igd_dtlz2(r.objectives) < 0.08
+    # NSGA-III keeps the survivor fronts as result indices
+    assert r.auxiliary_indices.shape == (92,) and int(r.auxiliary_indices.min()) >= 0
+
+
+def test_rvea_dtlz2_quality_and_front_zero():
+    algo = cm.RVEA(population_size=92, max_generations=100, problem=cm.DTLZ2(12, 3), seed=2887,
+                   print_progress=False)
+    r = algo.run()
+    act = r.active_count
+    assert 0 < act <= 92
+    assert igd_dtlz2(r.objectives[:act]) < 0.1
+    aux = r.auxiliary_indices.cpu().numpy()
+    assert len(aux) > 0 and aux.max() < act
+
+
+def test_constrained_and_quantized_and_user_directions():
+    algo = cm.NSGA3(population_size=200, max_generations=20, problem=cm.C1DTLZ1(12, 3),
+                    environment_selector=cm.NSGA3EnvironmentSelector(cv_bins=16, cv_clip_upper=10.0),
+                    print_progress=False)
+    r = algo.run()
+    assert torch.isfinite(r.objectives).all()
+    algo = cm.NSGA3(population_size=100, max_generations=5, problem=cm.DTLZ2(12, 3),
+                    reference_directions=cm.UserDefinedDirections(torch.eye(3) + 0.1),
+                    print_progress=False)
+    r = algo.run()
+    assert tuple(r.objectives.shape) == (100, 3)
+    # RVEA with fixed two-layer directions (gamma computed for any provider)
+    algo = cm.RVEA(population_size=64, max_generations=5, problem=cm.DTLZ2(17, 8),
+                   reference_directions=cm.DasDennisDirections(3), print_progress=False)
+    assert algo.run().active_count > 0
+
+
+def test_errors_raise():
+    with pytest.raises(Exception):
+        cm.NSGA3(population_size=33, max_generations=2, print_progress=False).run()
+    with pytest.raises(Exception):
+        cm.RVEA(population_size=32, max_generations=2, mating=cm.TournamentMating(),
+                print_progress=False).run()
