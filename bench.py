@@ -179,6 +179,8 @@ def main() -> None:
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    # one non-default stream for the algorithm, the timing events and the copies
+    torch.cuda.set_stream(torch.cuda.Stream(local))
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))

@@ -246,7 +246,7 @@ struct moea_algorithm {
         std::vector<float> host;
         int count = 0;
         if (cfg.directions == MOEA_DIRS_USER) {
-            if (!cfg.h_user_directions || cfg.user_direction_count < 1)
+            if (user_dirs.empty() || cfg.user_direction_count < 1)
                 return set_error(MOEA_ERR_INVALID_ARGUMENT, "User directions must have shape (objective_count, count)");
             count = cfg.user_direction_count;
             host = user_dirs;
@@ -718,6 +718,7 @@ moea_status moea_algorithm_view(moea_algorithm* a, moea_population_view* v)
     v->total_ms = a->total_ms;
     v->kernels_per_generation = a->graph_kernels;
     v->graph_active = (a->graph[0] || a->graph[1]) ? 1 : 0;
+    v->last_max_front = -1;
     if (!a->initialized) return MOEA_OK;
     v->d_variables = a->vars[a->P];
     v->d_objectives = a->objs[a->P];
@@ -730,6 +731,17 @@ moea_status moea_algorithm_view(moea_algorithm* a, moea_population_view* v)
         v->auxiliary_count = a->frontzero_count;
     }
     v->active_count = a->active_count_sync();
+    return MOEA_OK;
+}
+
+moea_status moea_algorithm_selection_stats(moea_algorithm* a, int* h_max_front, int* h_sizes)
+{
+    if (!a || !h_max_front || !h_sizes) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL argument");
+    *h_max_front = -1;
+    if (!a->initialized || !a->nsga3()) return MOEA_OK;
+    MOEA_CUDA_TRY(cudaMemcpyAsync(h_max_front, a->ws.counters + 2, sizeof(int), cudaMemcpyDeviceToHost, a->stream));
+    MOEA_CUDA_TRY(cudaMemcpyAsync(h_sizes, a->ws.sizes, 4 * sizeof(int), cudaMemcpyDeviceToHost, a->stream));
+    MOEA_CUDA_TRY(cudaStreamSynchronize(a->stream));
     return MOEA_OK;
 }
 

@@ -134,6 +134,84 @@ int normalize_user_directions(std::vector<float>& v, int M, int count)
     return MOEA_OK;
 }
 
+// Spatial groups of directions for the pruned association: recursive median
+// splits along the coordinate of largest spread until a group has at most
+// `group` members; per group the unit mean direction and a cone around it
+// that contains every member (cos and sin of its half angle, rounded outwards).
+// Outputs: order (H) direction indices grouped, table (ngroups * (M + 4))
+// floats: center[M], cos_rho, sin_rho, start (int bits), count (int bits).
+int build_direction_groups(const float* refs, int M, int H, int group, std::vector<int>& order,
+                           std::vector<float>& table)
+{
+    order.resize(H);
+    for (int j = 0; j < H; ++j) order[j] = j;
+    std::vector<std::pair<int, int>> stack{{0, H}}, leaves;
+    while (!stack.empty()) {
+        auto [lo, hi] = stack.back();
+        stack.pop_back();
+        if (hi - lo <= group) {
+            leaves.push_back({lo, hi});
+            continue;
+        }
+        int axis = 0;
+        float best = -1.0f;
+        for (int m = 0; m < M; ++m) {
+            float mn = INFINITY, mx = -INFINITY;
+            for (int i = lo; i < hi; ++i) {
+                const float v = refs[(size_t)m * H + order[i]];
+                mn = std::min(mn, v);
+                mx = std::max(mx, v);
+            }
+            if (mx - mn > best) { best = mx - mn; axis = m; }
+        }
+        const int mid = lo + (hi - lo) / 2;
+        std::nth_element(order.begin() + lo, order.begin() + mid, order.begin() + hi, [&](int a, int b) {
+            const float va = refs[(size_t)axis * H + a], vb = refs[(size_t)axis * H + b];
+            return va < vb || (va == vb && a < b);
+        });
+        stack.push_back({mid, hi});
+        stack.push_back({lo, mid});
+    }
+    std::sort(leaves.begin(), leaves.end());
+    const int stride = M + 4;
+    table.assign(leaves.size() * (size_t)stride, 0.0f);
+    for (size_t g = 0; g < leaves.size(); ++g) {
+        const int lo = leaves[g].first, hi = leaves[g].second;
+        std::vector<double> c(M, 0.0);
+        for (int i = lo; i < hi; ++i)
+            for (int m = 0; m < M; ++m) c[m] += refs[(size_t)m * H + order[i]];
+        double norm = 0.0;
+        for (int m = 0; m < M; ++m) norm += c[m] * c[m];
+        norm = std::sqrt(norm);
+        double cmin = 1.0;
+        if (norm > 0.0) {
+            for (int m = 0; m < M; ++m) c[m] /= norm;
+            for (int i = lo; i < hi; ++i) {
+                double dot = 0.0, rr = 0.0;
+                for (int m = 0; m < M; ++m) {
+                    const double r = refs[(size_t)m * H + order[i]];
+                    dot += c[m] * r;
+                    rr += r * r;
+                }
+                cmin = std::min(cmin, dot / std::sqrt(rr > 0.0 ? rr : 1.0));
+            }
+            cmin -= 1e-6;  // outward rounding of the cone
+        } else {
+            cmin = -1.0;   // degenerate group: no pruning
+        }
+        if (cmin < -1.0) cmin = -1.0;
+        const double smax = std::min(1.0, std::sqrt(std::max(0.0, 1.0 - cmin * cmin)) + 1e-6);
+        float* t = &table[g * (size_t)stride];
+        for (int m = 0; m < M; ++m) t[m] = (float)c[m];
+        t[M] = std::nextafter((float)cmin, -2.0f);
+        t[M + 1] = std::nextafter((float)smax, 2.0f);
+        std::memcpy(&t[M + 2], &lo, sizeof(int));
+        const int cnt = hi - lo;
+        std::memcpy(&t[M + 3], &cnt, sizeof(int));
+    }
+    return (int)leaves.size();
+}
+
 }  // namespace moea
 
 extern "C" moea_status moea_reference_directions(int mode, int n, int M, float* h_out,

@@ -37,7 +37,7 @@ namespace {
 constexpr int kQB = 128;      // sorted positions (dominatees) per tile CTA
 constexpr int kPW = 32;       // dominator words per tile CTA (1024 positions)
 constexpr int kTileThreads = 256;
-constexpr int kPeelThreads = 512;
+constexpr int kPeelThreads = 1024;
 constexpr uint32_t kInfeasibleBit = 0x80000000u;
 
 // ---------------------------------------------------------------------------
@@ -177,10 +177,14 @@ __device__ __forceinline__ void tile_word_loop(const float4* __restrict__ sq, co
     }
 }
 
+// Writes the dominator rows of kQB consecutive sorted positions for kPW words
+// of dominator positions, and raises blocker[q] to the highest dominator
+// position seen, so that after the kernel blocker[q] == -1 exactly for the
+// points that nothing dominates (front 0).
 template <int M>
 __global__ void __launch_bounds__(kTileThreads)
 nds_tiles(const float* __restrict__ sf, int sf_stride, const int* __restrict__ qinfo, int n, int W,
-          uint32_t* __restrict__ rows)
+          uint32_t* __restrict__ rows, int* __restrict__ blocker)
 {
     constexpr int V = QRec<M>::kVec;
     const int b = blockIdx.y;
@@ -234,7 +238,11 @@ nds_tiles(const float* __restrict__ sf, int sf_stride, const int* __restrict__ q
     for (int r = warp; r < kQB; r += kTileThreads / 32) {
         const int pos = q0 + r;
         if (pos >= n) break;
-        if (lane < wcount) rows[(size_t)pos * W + w0 + lane] = so[r][lane];
+        const uint32_t word = (lane < wcount) ? so[r][lane] : 0u;
+        if (lane < wcount) rows[(size_t)pos * W + w0 + lane] = word;
+        const unsigned nz = __ballot_sync(0xFFFFFFFFu, word != 0u);
+        if (nz && lane == 31 - __clz(nz))
+            atomicMax(blocker + pos, (w0 + lane) * 32 + (31 - __clz(word)));
     }
 }
 
@@ -311,37 +319,59 @@ nds_peel(const uint32_t* __restrict__ rows, int W, int n, int target, const int*
         for (int g = gwarp; g < ngroups; g += twarps) {
             const int q = g * 32 + lane;
             const bool alive = q < n && ((U[q >> 5] >> (q & 31)) & 1u);
-            bool need = false;
+            // blocker[q] is an unassigned dominator of q, or -1 when nothing dominates q
+            bool is_free = false, need = false;
             int start_w = -1;
             if (alive) {
                 const int b = blocker[q];
-                if (b < 0 || !((U[b >> 5] >> (b & 31)) & 1u)) {
-                    need = true;
-                    if (b >= 0) {
-                        start_w = b >> 5;
+                if (b < 0) {
+                    is_free = true;
+                } else if (!((U[b >> 5] >> (b & 31)) & 1u)) {
+                    // blocker assigned: probe its word and the one below; bits
+                    // above it were already free of unassigned dominators
+                    const uint32_t* row = rows + (size_t)q * W;
+                    int w = b >> 5;
+                    uint32_t bits = __ldg(row + w) & U[w];
+                    if (!bits && w > 0) {
+                        --w;
+                        bits = __ldg(row + w) & U[w];
+                    }
+                    if (bits) {
+                        blocker[q] = w * 32 + (31 - __clz(bits));
+                    } else if (w == 0) {
+                        is_free = true;
                     } else {
-                        const int d = qinfo[q] & 0x7FFFFFFF;
-                        start_w = ((d + 31) >> 5) - 1;
+                        need = true;
+                        start_w = w - 1;
                     }
                 }
             }
+            // rows not resolved by the probe: the whole warp scans each of
+            // them downwards, 8 coalesced words per lane in flight
             unsigned needm = __ballot_sync(0xFFFFFFFFu, need);
-            bool is_free = false;
             while (needm) {
                 const int L = __ffs(needm) - 1;
                 needm &= needm - 1;
                 const int qL = g * 32 + L;
+                const uint32_t* row = rows + (size_t)qL * W;
                 const int sw = __shfl_sync(0xFFFFFFFFu, start_w, L);
                 int found = -1;
-                for (int w0 = sw; w0 >= 0; w0 -= 32) {
-                    const int w = w0 - lane;
-                    const uint32_t bits = (w >= 0) ? (__ldg(rows + (size_t)qL * W + w) & U[w]) : 0u;
-                    const unsigned nz = __ballot_sync(0xFFFFFFFFu, bits != 0u);
-                    if (nz) {
-                        const int src = __ffs(nz) - 1;
-                        const uint32_t bb = __shfl_sync(0xFFFFFFFFu, bits, src);
-                        found = (w0 - src) * 32 + (31 - __clz(bb));
-                        break;
+                for (int w0 = sw; w0 >= 0 && found < 0; w0 -= 256) {
+                    uint32_t acc[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const int w = w0 - lane - 32 * i;
+                        acc[i] = (w >= 0) ? (__ldg(row + w) & U[w]) : 0u;
+                    }
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const unsigned nz = __ballot_sync(0xFFFFFFFFu, acc[i] != 0u);
+                        if (nz) {
+                            const int src = __ffs(nz) - 1;
+                            const uint32_t bb = __shfl_sync(0xFFFFFFFFu, acc[i], src);
+                            found = (w0 - src - 32 * i) * 32 + (31 - __clz(bb));
+                            break;
+                        }
                     }
                 }
                 if (lane == L) {
@@ -404,7 +434,7 @@ void launch_tiles(const Workspace& ws, int n, cudaStream_t stream)
     const int maxw = ceil_div(n, 32);
     dim3 grid(ceil_div(maxw, kPW), nqb);
     nds_tiles<M><<<grid, kTileThreads, 0, stream>>>(ws.sorted_f, ws.n_max, ws.qinfo, n,
-                                                     ws.words, ws.rows);
+                                                     ws.words, ws.rows, ws.blocker);
 }
 
 }  // namespace

@@ -64,6 +64,7 @@ class PopulationViewC(ctypes.Structure):
         ("active_count", c_int), ("generation", c_int), ("initialized", c_int),
         ("finished", c_int), ("device", c_int), ("total_ms", c_double),
         ("kernels_per_generation", c_int), ("graph_active", c_int),
+        ("last_max_front", c_int), ("last_sizes", c_int * 4),
     ]
 
 
@@ -116,6 +117,7 @@ _SIGNATURES = [
     ("moea_algorithm_view", c_int, [vp, ctypes.POINTER(PopulationViewC)]),
     ("moea_algorithm_directions", c_int, [vp, ctypes.POINTER(vp), ip]),
     ("moea_algorithm_profile_step", c_int, [vp, ctypes.c_char_p, c_size_t, fp, c_int, ip]),
+    ("moea_algorithm_selection_stats", c_int, [vp, ip, ip]),
     ("moea_algorithm_device_status", c_int, [vp, ip]),
 ]
 

@@ -185,9 +185,15 @@ class Algorithm:
         cfg.device = self._device
         cfg.seed = int(self._cuda.seed)
         # run on the caller's current torch stream, so tensor views of the
-        # population are ordered with the algorithm's kernels
+        # population are ordered with the algorithm's kernels; the legacy
+        # default stream cannot be captured into a graph, so a dedicated
+        # stream (self.stream) is used instead of it
         with torch.cuda.device(self._device):
-            cfg.stream = torch.cuda.current_stream(self._device).cuda_stream
+            cur = torch.cuda.current_stream(self._device)
+            if cur.cuda_stream == 0:
+                cur = torch.cuda.Stream(self._device)
+            self.stream = cur
+            cfg.stream = cur.cuda_stream
         cfg.use_graphs = 1 if self._use_graphs else 0
         D, M = self._problem_info
         cfg.dimension, cfg.objectives = D, M
@@ -392,6 +398,13 @@ class Algorithm:
         self._call(lib().moea_algorithm_profile_step, h, names, 4096, ms, 64, ctypes.byref(cnt))
         labels = names.value.decode().split("\n")
         return [(labels[i], float(ms[i])) for i in range(cnt.value)]
+
+    def selection_stats(self) -> dict:
+        """NSGA-III: last front index and sizes of the latest selection."""
+        mf = ctypes.c_int(-1)
+        sz = (ctypes.c_int * 4)()
+        self._call(lib().moea_algorithm_selection_stats, self._ensure_native(), ctypes.byref(mf), sz)
+        return {"max_front": mf.value, "N_prior": sz[0], "N_last": sz[1], "N_rem": sz[2], "N_nds": sz[3]}
 
     @property
     def graph_info(self) -> tuple[bool, int]:

@@ -299,7 +299,13 @@ typedef struct moea_population_view {
     double total_ms;
     int kernels_per_generation; /* kernel nodes of the captured generation graph (0 if not captured) */
     int graph_active;           /* 1 when generations replay a CUDA graph */
+    int last_max_front;         /* reserved (-1); see moea_algorithm_selection_stats */
+    int last_sizes[4];
 } moea_population_view;
+
+/* NSGA-III: index of the last front and {N_prior, N_last, N_rem, N_nds} of the
+ * latest selection (synchronises the algorithm's stream). */
+moea_status moea_algorithm_selection_stats(moea_algorithm* alg, int* h_max_front, int* h_sizes);
 
 moea_status moea_algorithm_view(moea_algorithm* alg, moea_population_view* out);
 /* Reference directions in use: d_values (M,count). */
