@@ -77,7 +77,11 @@ def test_rvea_golden(g, oracle):
     np.testing.assert_array_equal(t, g["rvea_t"])
     th, idx = oracle.rvea_partition(g["rvea_t"], g["rvea_refs"], 130, 150)
     assert (idx != g["rvea_idx"]).sum() <= 1
-    np.testing.assert_allclose(th, g["rvea_theta"], rtol=3e-6, atol=3e-6)
+    # theta = acosf(cos) with the device's rsqrtf/acosf against the host's
+    # 1/sqrtf and acosf: a few ulps apart in cos, which acos amplifies by
+    # 1/sin(theta) near theta = 0, so the check is on the cosines
+    np.testing.assert_allclose(np.cos(th.astype(np.float64)), np.cos(g["rvea_theta"].astype(np.float64)),
+                               rtol=0, atol=2e-6)
     np.testing.assert_allclose(oracle.rvea_gamma(g["rvea_refs"]), g["rvea_gamma"], rtol=3e-6, atol=3e-7)
     apd = oracle.rvea_apd(g["rvea_t"], g["rvea_theta"], g["rvea_gamma"], g["rvea_idx"], 10, 100, 2.0)
     np.testing.assert_array_equal(apd, g["rvea_apd"])
