@@ -270,6 +270,12 @@ struct moea_algorithm {
         return MOEA_OK;
     }
 
+    // Adapted directions change on the device, so they are always scanned.
+    int assoc_mode() const
+    {
+        return cfg.directions == MOEA_DIRS_ADAPTIVE ? MOEA_ASSOC_SCAN : cfg.association_mode;
+    }
+
     int validate()
     {
         if (cfg.population_size <= 0 || cfg.max_generations <= 0)
@@ -305,6 +311,9 @@ struct moea_algorithm {
         if (cfg.mutation && (cfg.pm_eta_initial <= 0.0f || cfg.pm_eta_final <= 0.0f ||
                              cfg.pm_probability < 0.0f || cfg.pm_probability > 1.0f))
             return set_error(MOEA_ERR_INVALID_ARGUMENT, "Invalid polynomial-mutation configuration");
+        if (cfg.association_mode != MOEA_ASSOC_TREE && cfg.association_mode != MOEA_ASSOC_SCAN)
+            return set_error(MOEA_ERR_INVALID_ARGUMENT, "association_mode must be %d or %d", MOEA_ASSOC_TREE,
+                             MOEA_ASSOC_SCAN);
         if (cfg.mating == MOEA_MATING_CALLBACK && !cfg.mate)
             return set_error(MOEA_ERR_INVALID_ARGUMENT, "callback mating without a function");
         // only the NSGA-III selector provides ranks (mating_selection.cu:80-86)
@@ -378,6 +387,8 @@ struct moea_algorithm {
         MOEA_TRY(directions_init());
         MOEA_TRY(workspace_init(ws, cfg.device, 2 * N, M, H));
         ws_ready = true;
+        if (nsga3() && assoc_mode() == MOEA_ASSOC_TREE)
+            MOEA_TRY(prepare_direction_tree(ws, refs, nullptr, M, H, stream));
         if (!init_pop.empty()) {
             for (int r = 0; r < N; ++r)
                 for (int d = 0; d < D; ++d) {
@@ -458,7 +469,7 @@ struct moea_algorithm {
                 sort_pop.cv_b = cv_sort[1];
             }
             MOEA_TRY(run_nsga3_select(ws, pop, M, N, refs, H, seed, ideal_last, survivors, nullptr,
-                                      cfg.association_mode, stream, &sort_pop));
+                                      assoc_mode(), stream, &sort_pop));
             gather_next<<<ceil_div((long long)N * D > N ? (long long)N * D : N, 256), 256, 0, stream>>>(
                 vars[P], vars[O], pop, survivors, ws.fronts, N, D, M, vars[X], objs[X], cv[X], rank[X]);
             MOEA_CUDA_TRY(cudaGetLastError());

@@ -72,7 +72,8 @@ void free_all(Workspace& ws)
                     ws.nds_gidx, ws.sizes, ws.chunk_counts, ws.nds_objs, ws.norm_part,
                     ws.norm_part_idx, ws.rcp_b, ws.extreme, ws.ideal_tmp, ws.assoc_best,
                     ws.assoc_idx, ws.assoc_dist, ws.rho, ws.sel_vals[0], ws.sel_vals[1],
-                    ws.rank, ws.selected, ws.flags, ws.offset_dev, ws.cub_tmp};
+                    ws.rank, ws.selected, ws.flags, ws.offset_dev, ws.cub_tmp, ws.tree_dirs,
+                    ws.tree_order, ws.tree_center, ws.dir_delta};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     ws = Workspace{};
@@ -117,6 +118,7 @@ int workspace_init(Workspace& ws, int device, int n_max, int m_max, int h_max)
     A(ws.sel_vals[0], n); A(ws.sel_vals[1], n);
     A(ws.rank, n); A(ws.selected, n); A(ws.flags, n);
     A(ws.offset_dev, 1);
+    A(ws.dir_delta, 1);
 #undef A
     if (st == MOEA_OK) {
         ws.cub_bytes = cub_temp_bytes_needed(n_max);
@@ -247,6 +249,7 @@ moea_status moea_associate(moea_workspace* w, const float* d_x, const float* d_r
         return set_error(MOEA_ERR_INVALID_ARGUMENT, "associate: bad arguments");
     if (n == 0) return MOEA_OK;
     Workspace& ws = w->ws;
+    if (mode == MOEA_ASSOC_TREE) MOEA_TRY(prepare_direction_tree(ws, d_refs, nullptr, M, H, S(stream)));
     int hs[4] = {0, n, 0, n};
     MOEA_CUDA_TRY(cudaMemcpyAsync(ws.sizes + 4, &hs[3], sizeof(int), cudaMemcpyHostToDevice, S(stream)));
     return run_associate(ws, d_x, n, nullptr, d_refs, M, ws.sizes + 4, n, H, d_idx, d_dist, mode,
@@ -281,6 +284,7 @@ moea_status moea_nsga3_select(moea_workspace* w, const float* d_mix_cv, const fl
     if (!d_mix_cv || !d_mix_objs || !d_refs || !h_offset || !d_ideal_last || !d_survivors ||
         N < 1 || 2 * N > ws.n_max || M < 1 || M > ws.m_max || H < 1 || H > ws.h_max)
         return set_error(MOEA_ERR_INVALID_ARGUMENT, "nsga3_select: bad arguments");
+    if (assoc_mode == MOEA_ASSOC_TREE) MOEA_TRY(prepare_direction_tree(ws, d_refs, nullptr, M, H, S(stream)));
     unsigned long long off = *h_offset;
     MOEA_CUDA_TRY(cudaMemcpyAsync(ws.offset_dev, &off, sizeof(off), cudaMemcpyHostToDevice, S(stream)));
     SplitPop pop{d_mix_objs, d_mix_objs + N, d_mix_cv, d_mix_cv + N, 2 * N, 2 * N, N, 2 * N};

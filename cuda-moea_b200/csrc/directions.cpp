@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "moea_b200.h"
+#include "dirtree.h"
 
 namespace moea {
 
@@ -134,82 +135,124 @@ int normalize_user_directions(std::vector<float>& v, int M, int count)
     return MOEA_OK;
 }
 
-// Spatial groups of directions for the pruned association: recursive median
-// splits along the coordinate of largest spread until a group has at most
-// `group` members; per group the unit mean direction and a cone around it
-// that contains every member (cos and sin of its half angle, rounded outwards).
-// Outputs: order (H) direction indices grouped, table (ngroups * (M + 4))
-// floats: center[M], cos_rho, sin_rho, start (int bits), count (int bits).
-int build_direction_groups(const float* refs, int M, int H, int group, std::vector<int>& order,
-                           std::vector<float>& table)
+// Cone tree over the directions for the pruned association search.
+//
+// Directions are reordered so that every node covers a contiguous range of
+// the new order.  A node with more than kTreeLeaf directions gets up to 32
+// children by five levels of median splits along the coordinate of largest
+// spread; a node with at most kTreeLeaf directions is a leaf.  Nodes are
+// numbered breadth first, so the children of a node are contiguous.  Each
+// node stores the unit mean of its members' unit vectors and a cone around it
+// that contains every member (cos and sin of the half angle, rounded
+// outwards).  delta = max | |r|^2 - 1 | over the directions.
+namespace {
+
+constexpr int kTreeLeaf = 32;
+
+int median_split(const float* refs, int M, int H, std::vector<int>& order, int lo, int hi)
 {
-    order.resize(H);
-    for (int j = 0; j < H; ++j) order[j] = j;
-    std::vector<std::pair<int, int>> stack{{0, H}}, leaves;
-    while (!stack.empty()) {
-        auto [lo, hi] = stack.back();
-        stack.pop_back();
-        if (hi - lo <= group) {
-            leaves.push_back({lo, hi});
+    int axis = 0;
+    float best = -1.0f;
+    for (int m = 0; m < M; ++m) {
+        float mn = INFINITY, mx = -INFINITY;
+        for (int i = lo; i < hi; ++i) {
+            const float v = refs[(size_t)m * H + order[i]];
+            mn = std::min(mn, v);
+            mx = std::max(mx, v);
+        }
+        if (mx - mn > best) { best = mx - mn; axis = m; }
+    }
+    const int mid = lo + (hi - lo) / 2;
+    std::nth_element(order.begin() + lo, order.begin() + mid, order.begin() + hi, [&](int a, int b) {
+        const float va = refs[(size_t)axis * H + a], vb = refs[(size_t)axis * H + b];
+        return va < vb || (va == vb && a < b);
+    });
+    return mid;
+}
+
+void expand(const float* refs, int M, int H, std::vector<int>& order, int lo, int hi, int levels,
+            std::vector<std::pair<int, int>>& out)
+{
+    if (hi - lo <= kTreeLeaf || levels == 0) {
+        out.push_back({lo, hi});
+        return;
+    }
+    const int mid = median_split(refs, M, H, order, lo, hi);
+    expand(refs, M, H, order, lo, mid, levels - 1, out);
+    expand(refs, M, H, order, mid, hi, levels - 1, out);
+}
+
+}  // namespace
+
+int build_direction_tree(const float* refs, int M, int H, DirectionTreeHost& t)
+{
+    t = DirectionTreeHost{};
+    t.M = M;
+    t.H = H;
+    t.order.resize(H);
+    for (int j = 0; j < H; ++j) t.order[j] = j;
+    double delta = 0.0;
+    std::vector<double> unit((size_t)M * H);
+    for (int j = 0; j < H; ++j) {
+        double rr = 0.0;
+        for (int m = 0; m < M; ++m) rr += (double)refs[(size_t)m * H + j] * refs[(size_t)m * H + j];
+        if (!std::isfinite(rr)) delta = INFINITY;
+        else delta = std::max(delta, std::fabs(rr - 1.0));
+        const double inv = rr > 0.0 ? 1.0 / std::sqrt(rr) : 0.0;
+        for (int m = 0; m < M; ++m) unit[(size_t)m * H + j] = refs[(size_t)m * H + j] * inv;
+    }
+    t.delta = (float)std::min(delta, 1e30);
+    std::vector<std::pair<int, int>> ranges{{0, H}};
+    std::vector<int> depth{0};
+    for (size_t k = 0; k < ranges.size(); ++k) {
+        const int lo = ranges[k].first, hi = ranges[k].second;
+        t.max_depth = std::max(t.max_depth, depth[k] + 1);
+        if (hi - lo <= kTreeLeaf) {
+            t.link.push_back(lo);
+            t.link.push_back(-(hi - lo));
             continue;
         }
-        int axis = 0;
-        float best = -1.0f;
-        for (int m = 0; m < M; ++m) {
-            float mn = INFINITY, mx = -INFINITY;
-            for (int i = lo; i < hi; ++i) {
-                const float v = refs[(size_t)m * H + order[i]];
-                mn = std::min(mn, v);
-                mx = std::max(mx, v);
-            }
-            if (mx - mn > best) { best = mx - mn; axis = m; }
+        std::vector<std::pair<int, int>> kids;
+        expand(refs, M, H, t.order, lo, hi, 5, kids);
+        t.link.push_back((int)ranges.size());
+        t.link.push_back((int)kids.size());
+        for (auto& c : kids) {
+            ranges.push_back(c);
+            depth.push_back(depth[k] + 1);
         }
-        const int mid = lo + (hi - lo) / 2;
-        std::nth_element(order.begin() + lo, order.begin() + mid, order.begin() + hi, [&](int a, int b) {
-            const float va = refs[(size_t)axis * H + a], vb = refs[(size_t)axis * H + b];
-            return va < vb || (va == vb && a < b);
-        });
-        stack.push_back({mid, hi});
-        stack.push_back({lo, mid});
     }
-    std::sort(leaves.begin(), leaves.end());
-    const int stride = M + 4;
-    table.assign(leaves.size() * (size_t)stride, 0.0f);
-    for (size_t g = 0; g < leaves.size(); ++g) {
-        const int lo = leaves[g].first, hi = leaves[g].second;
-        std::vector<double> c(M, 0.0);
+    const int nodes = (int)ranges.size();
+    t.nodes = nodes;
+    t.center.assign((size_t)M * nodes, 0.0f);
+    t.cos_r.assign(nodes, -1.0f);
+    t.sin_r.assign(nodes, 1.0f);
+    std::vector<double> c(M);
+    for (int k = 0; k < nodes; ++k) {
+        const int lo = ranges[k].first, hi = ranges[k].second;
+        std::fill(c.begin(), c.end(), 0.0);
         for (int i = lo; i < hi; ++i)
-            for (int m = 0; m < M; ++m) c[m] += refs[(size_t)m * H + order[i]];
+            for (int m = 0; m < M; ++m) c[m] += unit[(size_t)m * H + t.order[i]];
         double norm = 0.0;
         for (int m = 0; m < M; ++m) norm += c[m] * c[m];
         norm = std::sqrt(norm);
+        if (!(norm > 1e-12)) continue;  // no cone: the node is never pruned
+        for (int m = 0; m < M; ++m) c[m] /= norm;
         double cmin = 1.0;
-        if (norm > 0.0) {
-            for (int m = 0; m < M; ++m) c[m] /= norm;
-            for (int i = lo; i < hi; ++i) {
-                double dot = 0.0, rr = 0.0;
-                for (int m = 0; m < M; ++m) {
-                    const double r = refs[(size_t)m * H + order[i]];
-                    dot += c[m] * r;
-                    rr += r * r;
-                }
-                cmin = std::min(cmin, dot / std::sqrt(rr > 0.0 ? rr : 1.0));
-            }
-            cmin -= 1e-6;  // outward rounding of the cone
-        } else {
-            cmin = -1.0;   // degenerate group: no pruning
+        for (int i = lo; i < hi; ++i) {
+            double dot = 0.0;
+            for (int m = 0; m < M; ++m) dot += c[m] * unit[(size_t)m * H + t.order[i]];
+            cmin = std::min(cmin, dot);
         }
-        if (cmin < -1.0) cmin = -1.0;
+        cmin = std::max(-1.0, cmin - 1e-6);
         const double smax = std::min(1.0, std::sqrt(std::max(0.0, 1.0 - cmin * cmin)) + 1e-6);
-        float* t = &table[g * (size_t)stride];
-        for (int m = 0; m < M; ++m) t[m] = (float)c[m];
-        t[M] = std::nextafter((float)cmin, -2.0f);
-        t[M + 1] = std::nextafter((float)smax, 2.0f);
-        std::memcpy(&t[M + 2], &lo, sizeof(int));
-        const int cnt = hi - lo;
-        std::memcpy(&t[M + 3], &cnt, sizeof(int));
+        for (int m = 0; m < M; ++m) t.center[(size_t)m * nodes + k] = (float)c[m];
+        t.cos_r[k] = std::nextafter((float)cmin, -2.0f);
+        t.sin_r[k] = std::min(1.0f, std::nextafter((float)smax, 2.0f));
     }
-    return (int)leaves.size();
+    t.dirs.resize((size_t)M * H);
+    for (int m = 0; m < M; ++m)
+        for (int i = 0; i < H; ++i) t.dirs[(size_t)m * H + i] = refs[(size_t)m * H + t.order[i]];
+    return MOEA_OK;
 }
 
 }  // namespace moea

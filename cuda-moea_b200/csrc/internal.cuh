@@ -98,6 +98,21 @@ struct Workspace {
     int* flags = nullptr;           // (n_max) survivor flags
     unsigned long long* offset_dev = nullptr;  // niching counter offset
 
+    // --- cone tree of the directions for the pruned association ---
+    // Device copy of a DirectionTreeHost; valid for the directions at
+    // tree_src (M = tree_M, H = tree_H) until prepared again.
+    const float* tree_src = nullptr;
+    int tree_M = 0, tree_H = 0, tree_nodes = 0, tree_depth = 0;
+    float tree_delta = 0.0f;
+    size_t tree_cap_dirs = 0, tree_cap_nodes = 0;   // allocated capacities
+    float* tree_dirs = nullptr;     // (M, H) directions in tree order
+    int* tree_order = nullptr;      // (H) tree position -> direction index
+    float* tree_center = nullptr;   // (M, nodes)
+    float* tree_cos = nullptr;      // (nodes)
+    float* tree_sin = nullptr;      // (nodes)
+    int2* tree_link = nullptr;      // (nodes)
+    float* dir_delta = nullptr;     // (1) max | |r|^2 - 1 | of the last scanned directions
+
     // --- CUB temporary storage ---
     void* cub_tmp = nullptr;
     size_t cub_bytes = 0;
@@ -118,9 +133,17 @@ int run_extract(Workspace& ws, const int* fronts, int n, const int* d_max_front,
 int run_normalize_split(Workspace& ws, const SplitPop& pop, const int* nds_gidx,
                         const int* sizes, const float* ideal, int M, cudaStream_t stream);
 
+// mode MOEA_ASSOC_TREE needs prepare_direction_tree for these refs first.
 int run_associate(Workspace& ws, const float* x, int x_stride, const float* scale,
                   const float* refs, int M, const int* d_n, int n_cap, int H, int* idx,
                   float* dist, int mode, cudaStream_t stream);
+
+// Builds the cone tree of the directions on the host and uploads it into the
+// workspace, tagged with the device pointer d_refs.  h_refs may be null, in
+// which case the directions are read back from d_refs (synchronising stream).
+int prepare_direction_tree(Workspace& ws, const float* d_refs, const float* h_refs, int M, int H,
+                           cudaStream_t stream);
+bool direction_tree_ready(const Workspace& ws, const float* d_refs, int M, int H);
 
 int run_niching(Workspace& ws, uint64_t seed, const int* nds_gidx, const float* dist,
                 const int* idx, const int* sizes, int H, int N, int* selected,

@@ -18,8 +18,9 @@
 //       feasible q:    p dominates q  <=>  p < dup[q] and f_m(p) <= f_m(q), m >= 1
 //     which is the reference relation (non_dominated_sort.cu:190-239) with one
 //     integer and M-1 float comparisons per pair on the lower triangle only.
-//  3. A tile kernel evaluates that test with warp ballots and stores, for every
-//     q, the bit row of its dominators (sorted positions, 32 per word).
+//  3. A tile kernel evaluates that test, one dominatee per lane against
+//     dominator objectives broadcast from shared memory, and stores for every
+//     q the bit row of its dominators (sorted positions, 32 per word).
 //  4. One cooperative persistent kernel peels the fronts: q joins front k when
 //     no still-unassigned point is left in its row.  Each point remembers one
 //     unassigned dominator ("blocker"); while that blocker is unassigned the
@@ -35,7 +36,6 @@ namespace moea {
 namespace {
 
 constexpr int kQB = 128;      // sorted positions (dominatees) per tile CTA
-constexpr int kPW = 32;       // dominator words per tile CTA (1024 positions)
 constexpr int kTileThreads = 256;
 constexpr int kPeelThreads = 1024;
 constexpr uint32_t kInfeasibleBit = 0x80000000u;
@@ -139,102 +139,104 @@ __global__ void nds_finalize_rows(int n, const uint64_t* __restrict__ key0,
 // 2. dominance rows
 // ---------------------------------------------------------------------------
 
-// Number of float4 slots of a q record: objectives 1..M-1 then the dup word.
+// Dominator words per tile CTA (32 positions each), so that the staged
+// dominator objectives stay within 16 KB of shared memory.
 template <int M>
-struct QRec {
-    static constexpr int kWords = M;                  // (M-1) floats + 1 dup word
-    static constexpr int kVec = (kWords + 3) / 4;
+struct TileCfg {
+    static constexpr int kPW = (M <= 4) ? 32 : ((M <= 8) ? 16 : 8);
+    static constexpr int kMF = (M > 1) ? M - 1 : 1;   // staged objectives 1..M-1
 };
 
-template <int M, bool kAnyInfeasible>
-__device__ __forceinline__ void tile_word_loop(const float4* __restrict__ sq, const float (&pf)[M > 1 ? M - 1 : 1],
-                                               int p, int lane, uint32_t* __restrict__ out_col,
-                                               int out_stride)
-{
-    constexpr int V = QRec<M>::kVec;
-    for (int qi = 0; qi < kQB; qi += 32) {
-#pragma unroll 8
-        for (int t = 0; t < 32; ++t) {
-            const float4* rec = sq + (qi + t) * V;
-            float w[V * 4];
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                const float4 r = rec[v];
-                w[4 * v + 0] = r.x; w[4 * v + 1] = r.y; w[4 * v + 2] = r.z; w[4 * v + 3] = r.w;
-            }
-            const uint32_t dinfo = __float_as_uint(w[M - 1]);
-            bool d;
-            if (kAnyInfeasible && (dinfo & kInfeasibleBit)) {
-                d = p < (int)(dinfo & ~kInfeasibleBit);
-            } else {
-                d = p < (int)dinfo;
-#pragma unroll
-                for (int m = 0; m < M - 1; ++m) d &= pf[m] <= w[m];
-            }
-            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, d);
-            if (lane == 0) out_col[(qi + t) * out_stride] = bal;
-        }
-    }
-}
-
-// Writes the dominator rows of kQB consecutive sorted positions for kPW words
-// of dominator positions, and raises blocker[q] to the highest dominator
-// position seen, so that after the kernel blocker[q] == -1 exactly for the
-// points that nothing dominates (front 0).
+// One CTA covers kQB dominatees q (one per lane of warps 0-3, again of warps
+// 4-7) against kPW words of dominator positions p (the first half of the
+// words for warps 0-3, the second half for warps 4-7).  The p objectives are
+// staged in shared memory and read as warp-wide broadcasts, four positions
+// per 16-byte load; each lane keeps its q's objectives in registers and
+// builds the 32-bit word of its row directly, so one warp instruction
+// evaluates one comparison for 32 pairs.  Words are transposed through shared
+// memory and written as coalesced row segments.  The epilogue raises
+// blocker[q] to the highest dominator position seen, so that after the kernel
+// blocker[q] == -1 exactly for the points that nothing dominates (front 0).
 template <int M>
 __global__ void __launch_bounds__(kTileThreads)
 nds_tiles(const float* __restrict__ sf, int sf_stride, const int* __restrict__ qinfo, int n, int W,
           uint32_t* __restrict__ rows, int* __restrict__ blocker)
 {
-    constexpr int V = QRec<M>::kVec;
-    const int b = blockIdx.y;
-    const int q0 = b * kQB;
+    constexpr int PW = TileCfg<M>::kPW;
+    constexpr int MF = TileCfg<M>::kMF;
+    constexpr int P = PW * 32;
+    const int q0 = blockIdx.y * kQB;
     if (q0 >= n) return;
     const int qend = min(q0 + kQB, n);
     // dominators of the block lie at positions < qend - 1
     const int nwords = (qend - 1 + 31) >> 5;
-    const int w0 = blockIdx.x * kPW;
+    const int w0 = blockIdx.x * PW;
     if (w0 >= nwords) return;
+    const int wcount = min(PW, nwords - w0);
 
-    __shared__ float4 sq[kQB * V];
-    __shared__ uint32_t so[kQB][kPW + 1];
-    __shared__ int s_any_inf;
-    if (threadIdx.x == 0) s_any_inf = 0;
-    __syncthreads();
-    for (int t = threadIdx.x; t < kQB; t += blockDim.x) {
-        const int pos = q0 + t;
-        float w[V * 4];
+    __shared__ __align__(16) float s_p[MF][P];
+    __shared__ uint32_t so[kQB][PW + 1];
+    const int p0 = w0 * 32;
+    if (M > 1) {
+        for (int t = threadIdx.x; t < wcount * 32; t += kTileThreads) {
+            const int p = p0 + t;
 #pragma unroll
-        for (int i = 0; i < V * 4; ++i) w[i] = 0.0f;
-        uint32_t dinfo = 0u;
-        if (pos < n) {
-#pragma unroll
-            for (int m = 0; m < M - 1; ++m) w[m] = sf[(size_t)m * sf_stride + pos];
-            dinfo = (uint32_t)qinfo[pos];
+            for (int m = 0; m < MF; ++m) s_p[m][t] = (p < n) ? sf[(size_t)m * sf_stride + p] : 0.0f;
         }
-        w[M - 1] = __uint_as_float(dinfo);
-        if (dinfo & kInfeasibleBit) s_any_inf = 1;
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ql = (warp & 3) * 32 + lane;
+    const int q = q0 + ql;
+    float qf[MF];
+    int dup = 0;
+    bool inf = false;
 #pragma unroll
-        for (int v = 0; v < V; ++v) sq[t * V + v] = make_float4(w[4 * v], w[4 * v + 1], w[4 * v + 2], w[4 * v + 3]);
+    for (int m = 0; m < MF; ++m) qf[m] = 0.0f;
+    if (q < n) {
+        if (M > 1) {
+#pragma unroll
+            for (int m = 0; m < MF; ++m) qf[m] = sf[(size_t)m * sf_stride + q];
+        }
+        const uint32_t info = (uint32_t)qinfo[q];
+        inf = (info & kInfeasibleBit) != 0u;
+        dup = (int)(info & ~kInfeasibleBit);
     }
     __syncthreads();
 
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const bool any_inf = s_any_inf != 0;
-    for (int wl = warp; wl < kPW; wl += kTileThreads / 32) {
-        const int w = w0 + wl;
-        if (w >= nwords) break;
-        const int p = w * 32 + lane;
-        float pf[M > 1 ? M - 1 : 1];
+    constexpr int kHalf = PW / 2;
+    const int wb = (warp >> 2) * kHalf;
+    for (int wl = wb; wl < wb + kHalf; ++wl) {
+        uint32_t bits = 0u;
+        if (wl < wcount) {
+            // positions p < dup[q] of this word
+            const int rem = dup - (w0 + wl) * 32;
+            const uint32_t mask = rem >= 32 ? 0xFFFFFFFFu : (rem <= 0 ? 0u : ((1u << rem) - 1u));
+            const bool need = mask != 0u && !inf;
+            if (M > 1 && __any_sync(0xFFFFFFFFu, need)) {
+                uint32_t cmp = 0u;
+                constexpr int kUnroll = (MF > 7) ? 2 : 8;
+#pragma unroll kUnroll
+                for (int j = 0; j < 32; j += 4) {
+                    bool d0 = true, d1 = true, d2 = true, d3 = true;
 #pragma unroll
-        for (int m = 0; m < M - 1; ++m) pf[m] = (p < n) ? sf[(size_t)m * sf_stride + p] : __int_as_float(0x7FC00000);
-        if (any_inf)
-            tile_word_loop<M, true>(sq, pf, p, lane, &so[0][wl], kPW + 1);
-        else
-            tile_word_loop<M, false>(sq, pf, p, lane, &so[0][wl], kPW + 1);
+                    for (int m = 0; m < MF; ++m) {
+                        const float4 v = *reinterpret_cast<const float4*>(&s_p[m][wl * 32 + j]);
+                        d0 &= v.x <= qf[m];
+                        d1 &= v.y <= qf[m];
+                        d2 &= v.z <= qf[m];
+                        d3 &= v.w <= qf[m];
+                    }
+                    cmp |= ((uint32_t)d0 << j) | ((uint32_t)d1 << (j + 1)) | ((uint32_t)d2 << (j + 2)) |
+                           ((uint32_t)d3 << (j + 3));
+                }
+                bits = inf ? mask : (mask & cmp);
+            } else {
+                bits = (inf || M == 1) ? mask : 0u;
+            }
+        }
+        so[ql][wl] = bits;
     }
     __syncthreads();
-    const int wcount = min(kPW, nwords - w0);
     for (int r = warp; r < kQB; r += kTileThreads / 32) {
         const int pos = q0 + r;
         if (pos >= n) break;
@@ -432,7 +434,7 @@ void launch_tiles(const Workspace& ws, int n, cudaStream_t stream)
 {
     const int nqb = ceil_div(n, kQB);
     const int maxw = ceil_div(n, 32);
-    dim3 grid(ceil_div(maxw, kPW), nqb);
+    dim3 grid(ceil_div(maxw, TileCfg<M>::kPW), nqb);
     nds_tiles<M><<<grid, kTileThreads, 0, stream>>>(ws.sorted_f, ws.n_max, ws.qinfo, n,
                                                      ws.words, ws.rows, ws.blocker);
 }

@@ -12,8 +12,10 @@
 #include <cub/cub.cuh>
 
 #include <cmath>
+#include <vector>
 
 #include "internal.cuh"
+#include "dirtree.h"
 
 namespace moea {
 namespace {
@@ -401,11 +403,48 @@ struct DirTile {
     static constexpr int kLen = (M <= 4) ? kAssocTile : 512;  // directions per smem tile
 };
 
+// Margin of the dot^2 candidate filter for a point with |x|^2 = xx.  For
+// directions with | |r|^2 - 1 | <= delta, d2 = xx - dot^2 (2 - |r|^2) differs
+// from xx - dot^2 by at most xx (1 + delta) delta, hence the 2.5 delta term.
+// Directions far from unit length (delta > 1e-3) and non-finite points get an
+// infinite margin: every direction is re-scored.
+__device__ __forceinline__ float assoc_margin(int M, float xx, float delta)
+{
+    const float kEps = 5.9604645e-08f;  // 2^-24
+    float margin = xx * ((16.0f * M + 64.0f) * kEps + 2.5f * delta) + 1e-35f;
+    if (!isfinite(xx) || !(delta <= 1e-3f)) margin = INFINITY;
+    return margin;
+}
+
+// delta = max_j | |r_j|^2 - 1 | in FP64, rounded up to FP32 (one block).
+__global__ void dir_delta_kernel(const float* __restrict__ refs, int M, int H, float* __restrict__ out)
+{
+    __shared__ double s_max[32];
+    double d = 0.0;
+    for (int j = threadIdx.x; j < H; j += blockDim.x) {
+        double rr = 0.0;
+        for (int m = 0; m < M; ++m) {
+            const double v = refs[(size_t)m * H + j];
+            rr += v * v;
+        }
+        const double e = fabs(rr - 1.0);
+        d = (e == e) ? fmax(d, e) : INFINITY;
+    }
+    for (int o = 16; o; o >>= 1) d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
+    if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = d;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        d = threadIdx.x < (blockDim.x >> 5) ? s_max[threadIdx.x] : 0.0;
+        for (int o = 16; o; o >>= 1) d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
+        if (threadIdx.x == 0) out[0] = __double2float_ru(fmin(d, 1e30));
+    }
+}
+
 template <int M>
 __global__ void __launch_bounds__(kAssocThreads)
 assoc_plain(const float* __restrict__ x, int x_stride, const float* __restrict__ scale,
             const float* __restrict__ refs, int H, const int* __restrict__ d_n, int split_len,
-            unsigned long long* __restrict__ best_out)
+            const float* __restrict__ d_delta, unsigned long long* __restrict__ best_out)
 {
     constexpr int TL = DirTile<M>::kLen;
     __shared__ __align__(16) float s_dir[TL * ((M <= 4) ? 4 : M)];
@@ -424,9 +463,7 @@ assoc_plain(const float* __restrict__ x, int x_stride, const float* __restrict__
         xr[m] = v;
         xx = fmaf(v, v, xx);
     }
-    const float kEps = 5.9604645e-08f;  // 2^-24
-    float margin = xx * ((16.0f * M + 64.0f) * kEps) + 1e-35f;
-    if (!isfinite(xx)) margin = INFINITY;
+    const float margin = assoc_margin(M, xx, *d_delta);
     // coarse pre-pass over a strided subset to start with a tight threshold
     float maxd = -INFINITY;
     for (int j = j_begin; j < j_end; j += 61) {
@@ -520,7 +557,8 @@ __global__ void assoc_finish(const unsigned long long* __restrict__ best, const 
 
 template <int M>
 void launch_assoc(const float* x, int x_stride, const float* scale, const float* refs, int H,
-                  const int* d_n, int n_cap, unsigned long long* best, int sms, cudaStream_t stream)
+                  const int* d_n, int n_cap, const float* d_delta, unsigned long long* best, int sms,
+                  cudaStream_t stream)
 {
     const int pb = ceil_div(n_cap, kAssocThreads);
     int splits = ceil_div(8LL * sms, pb);
@@ -529,7 +567,187 @@ void launch_assoc(const float* x, int x_stride, const float* scale, const float*
     if (splits < 1) splits = 1;
     const int split_len = ceil_div(H, splits);
     assoc_plain<M><<<dim3(pb, splits), kAssocThreads, 0, stream>>>(x, x_stride, scale, refs, H, d_n,
-                                                                   split_len, best);
+                                                                   split_len, d_delta, best);
+}
+
+// ---- cone-tree search ------------------------------------------------------
+//
+// One warp per point.  The directions sit in the leaves of a 32-ary cone tree
+// (at most 32 per leaf, children of a node contiguous).  The warp keeps the
+// same running state as the scan kernel -- the largest dot^2 seen (maxd), the
+// threshold thr = maxd - margin, and the best packed (d2 bits, index) -- and
+// visits children best first (largest projection on the cone axis).  A
+// subtree is skipped when a bound on the FP32 dot^2 of every member lies
+// below thr: such members are never candidates in the scan kernel either,
+// and skipping them cannot change maxd.  Ties are resolved by the packed
+// minimum on the original index, so the result equals the reference argmin.
+//
+// Bound for a cone with axis c and half angle rho: the angle between x and a
+// member lies in [theta - rho, theta + rho] (theta = angle(x, c)), so
+// |cos| <= max(|cos(max(0, theta - rho))|, |cos(min(pi, theta + rho))|).
+// cos(theta) is estimated as (c . x) / |x| with error below dc = (4M + 16)
+// 2^-24; sin(theta) is bounded above from the estimate's interval; the FP32
+// dot of a member is within (M + 1) 2^-24 |x| |r| of the exact one (covered
+// by the 2 dc slack) and |r|^2 <= 1 + delta.
+
+constexpr int kTreeWarps = 8;
+constexpr int kTreeMaxDepth = 8;
+
+struct TreeArgs {
+    const float* dirs;    // (M, H) in tree order
+    const int* order;     // tree position -> direction index
+    const float* center;  // (M, nodes)
+    const float* cos_r;
+    const float* sin_r;
+    const int2* link;
+    int H, nodes;
+    float delta;
+};
+
+template <int M>
+__global__ void __launch_bounds__(kTreeWarps * 32)
+assoc_tree(const float* __restrict__ x, int x_stride, const float* __restrict__ scale, TreeArgs t,
+           const int* __restrict__ d_n, int* __restrict__ idx_out, float* __restrict__ dist_out)
+{
+    __shared__ float s_bound[kTreeWarps][kTreeMaxDepth][32];
+    __shared__ float s_proj[kTreeWarps][kTreeMaxDepth][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * kTreeWarps + warp;
+    if (i >= *d_n) return;
+    float xr[M];
+    float xx = 0.0f;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        float v = x[(size_t)m * x_stride + i];
+        if (scale) v = v * scale[m];
+        xr[m] = v;
+        xx = fmaf(v, v, xx);
+    }
+    const float kEps = 5.9604645e-08f;  // 2^-24
+    const float margin = assoc_margin(M, xx, t.delta);
+    const bool prune = margin < INFINITY && xx > 0.0f;
+    const float rnorm = prune ? 1.0f / sqrtf(xx) : 0.0f;
+    const float dc = (4.0f * M + 16.0f) * kEps;
+    const float dd_scale = (1.0f + t.delta) * (1.0f + 9.5367432e-07f);  // (1 + delta)(1 + 2^-20)
+    float maxd = -INFINITY, thr = -INFINITY;
+    unsigned long long best = ~0ull;
+
+    // bounds of children first..first+count-1 (one per lane) at stack level `level`
+    auto test = [&](int first, int count, int level) -> unsigned {
+        float bound = INFINITY, proj = 0.0f;
+        if (lane < count && prune) {
+            const int k = first + lane;
+            float p = 0.0f;
+#pragma unroll
+            for (int m = 0; m < M; ++m) p = fmaf(__ldg(t.center + (size_t)m * t.nodes + k), xr[m], p);
+            const float ce = p * rnorm;
+            proj = ce;
+            const float cr = __ldg(t.cos_r + k);
+            if (cr > 0.0f) {
+                const float sr = __ldg(t.sin_r + k);
+                const float hi = fminf(1.0f, ce + dc), lo = fmaxf(-1.0f, ce - dc);
+                const float mc = (lo <= 0.0f && hi >= 0.0f) ? 0.0f : fminf(lo * lo, hi * hi);
+                const float sh = fminf(1.0f, sqrtf(fmaxf(0.0f, 1.0f - mc) + 4.0f * kEps));
+                const float a = (hi >= cr) ? 1.0f : fmaf(hi, cr, sh * sr);
+                const float b = (lo <= -cr) ? -1.0f : fmaf(lo, cr, -(sh * sr));
+                const float cm = fminf(1.0f, fmaxf(fabsf(a), fabsf(b))) + 2.0f * dc;
+                bound = xx * (cm * cm * dd_scale);
+            }
+        }
+        s_bound[warp][level][lane] = bound;
+        s_proj[warp][level][lane] = proj;
+        __syncwarp();
+        return __ballot_sync(0xffffffffu, lane < count && bound >= thr);
+    };
+
+    // exact FP32 evaluation of the directions of one leaf (one per lane)
+    auto visit = [&](int start, int count) {
+        const bool v = lane < count;
+        float r[M];
+        float dot = 0.0f;
+        if (v) {
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                r[m] = __ldg(t.dirs + (size_t)m * t.H + start + lane);
+                dot = fmaf(xr[m], r[m], dot);
+            }
+        }
+        const float dd = dot * dot;
+        float g = v ? dd : -INFINITY;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) g = fmaxf(g, __shfl_xor_sync(0xffffffffu, g, o));
+        if (g > maxd) {
+            maxd = g;
+            const float nt = maxd - margin;
+            thr = (nt == nt) ? nt : -INFINITY;
+        }
+        if (v && dd >= thr) {
+            float d2 = 0.0f;
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                const float res = fmaf(-dot, r[m], xr[m]);
+                d2 = fmaf(res, res, d2);
+            }
+            if (d2 < INFINITY) {
+                const unsigned long long packed = ((unsigned long long)__float_as_uint(d2) << 32) |
+                                                  (unsigned)__ldg(t.order + start + lane);
+                best = packed < best ? packed : best;
+            }
+        }
+    };
+
+    const int2 root = __ldg(t.link);
+    if (root.y <= 0) {
+        visit(root.x, -root.y);
+    } else {
+        int first_s[kTreeMaxDepth];
+        unsigned mask_s[kTreeMaxDepth];
+        int sp = 0;
+        first_s[0] = root.x;
+        mask_s[0] = test(root.x, root.y, 0);
+        while (sp >= 0) {
+            const bool mine = (mask_s[sp] >> lane) & 1u;
+            const unsigned m = __ballot_sync(0xffffffffu, mine && s_bound[warp][sp][lane] >= thr);
+            if (!m) {
+                --sp;
+                continue;
+            }
+            float pv = ((m >> lane) & 1u) ? s_proj[warp][sp][lane] : -INFINITY;
+            int pl = lane;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                const float ov = __shfl_xor_sync(0xffffffffu, pv, o);
+                const int ol = __shfl_xor_sync(0xffffffffu, pl, o);
+                if (ov > pv || (ov == pv && ol < pl)) {
+                    pv = ov;
+                    pl = ol;
+                }
+            }
+            mask_s[sp] = m & ~(1u << pl);
+            const int2 ln = __ldg(t.link + first_s[sp] + pl);
+            if (ln.y <= 0) {
+                visit(ln.x, -ln.y);
+            } else {
+                ++sp;  // the host guarantees depth <= kTreeMaxDepth
+                first_s[sp] = ln.x;
+                mask_s[sp] = test(ln.x, ln.y, sp);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long ob = __shfl_xor_sync(0xffffffffu, best, o);
+        best = ob < best ? ob : best;
+    }
+    if (lane == 0) {
+        if (best == ~0ull) {
+            idx_out[i] = -1;
+            dist_out[i] = INFINITY;
+        } else {
+            idx_out[i] = (int)(unsigned)(best & 0xFFFFFFFFull);
+            dist_out[i] = sqrtf(__uint_as_float((unsigned)(best >> 32)));
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -677,17 +895,102 @@ int run_normalize_inplace(Workspace& ws, float* objs, const float* ideal, int M,
     return MOEA_OK;
 }
 
+bool direction_tree_ready(const Workspace& ws, const float* d_refs, int M, int H)
+{
+    return ws.tree_src == d_refs && d_refs && ws.tree_M == M && ws.tree_H == H && ws.tree_nodes > 0;
+}
+
+int prepare_direction_tree(Workspace& ws, const float* d_refs, const float* h_refs, int M, int H,
+                           cudaStream_t stream)
+{
+    if (!d_refs || M < 1 || M > kMaxObjectives || H < 1)
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "direction tree: bad arguments");
+    std::vector<float> host;
+    if (!h_refs) {
+        host.resize((size_t)M * H);
+        MOEA_CUDA_TRY(cudaMemcpyAsync(host.data(), d_refs, sizeof(float) * host.size(),
+                                      cudaMemcpyDeviceToHost, stream));
+        MOEA_CUDA_TRY(cudaStreamSynchronize(stream));
+        h_refs = host.data();
+    }
+    DirectionTreeHost t;
+    MOEA_TRY(build_direction_tree(h_refs, M, H, t));
+    ws.tree_src = nullptr;
+    const size_t nd = (size_t)M * H, nn = (size_t)t.nodes;
+    if (nd > ws.tree_cap_dirs) {
+        cudaFree(ws.tree_dirs);
+        cudaFree(ws.tree_order);
+        ws.tree_dirs = nullptr;
+        ws.tree_order = nullptr;
+        ws.tree_cap_dirs = 0;
+        MOEA_CUDA_TRY(cudaMalloc((void**)&ws.tree_dirs, sizeof(float) * nd));
+        MOEA_CUDA_TRY(cudaMalloc((void**)&ws.tree_order, sizeof(int) * nd));
+        ws.tree_cap_dirs = nd;
+    }
+    // one allocation for the nodes: center (M*nodes), cos (nodes), sin (nodes),
+    // then link (nodes int2) at an even float offset
+    const size_t link_off = ((size_t)(M + 2) * nn + 1) & ~(size_t)1;
+    const size_t node_words = link_off + 2 * nn;
+    if (node_words > ws.tree_cap_nodes) {
+        cudaFree(ws.tree_center);
+        ws.tree_center = nullptr;
+        ws.tree_cap_nodes = 0;
+        MOEA_CUDA_TRY(cudaMalloc((void**)&ws.tree_center, sizeof(float) * node_words));
+        ws.tree_cap_nodes = node_words;
+    }
+    ws.tree_cos = ws.tree_center + (size_t)M * nn;
+    ws.tree_sin = ws.tree_cos + nn;
+    ws.tree_link = reinterpret_cast<int2*>(ws.tree_center + link_off);
+    MOEA_CUDA_TRY(cudaMemcpyAsync(ws.tree_dirs, t.dirs.data(), sizeof(float) * nd, cudaMemcpyHostToDevice, stream));
+    MOEA_CUDA_TRY(cudaMemcpyAsync(ws.tree_order, t.order.data(), sizeof(int) * H, cudaMemcpyHostToDevice, stream));
+    MOEA_CUDA_TRY(cudaMemcpyAsync(ws.tree_center, t.center.data(), sizeof(float) * M * nn, cudaMemcpyHostToDevice, stream));
+    MOEA_CUDA_TRY(cudaMemcpyAsync(ws.tree_cos, t.cos_r.data(), sizeof(float) * nn, cudaMemcpyHostToDevice, stream));
+    MOEA_CUDA_TRY(cudaMemcpyAsync(ws.tree_sin, t.sin_r.data(), sizeof(float) * nn, cudaMemcpyHostToDevice, stream));
+    MOEA_CUDA_TRY(cudaMemcpyAsync(ws.tree_link, t.link.data(), sizeof(int) * 2 * nn, cudaMemcpyHostToDevice, stream));
+    MOEA_CUDA_TRY(cudaStreamSynchronize(stream));
+    ws.tree_src = d_refs;
+    ws.tree_M = M;
+    ws.tree_H = H;
+    ws.tree_nodes = t.nodes;
+    ws.tree_depth = t.max_depth;
+    ws.tree_delta = t.delta;
+    return MOEA_OK;
+}
+
 int run_associate(Workspace& ws, const float* x, int x_stride, const float* scale,
                   const float* refs, int M, const int* d_n, int n_cap, int H, int* idx,
                   float* dist, int mode, cudaStream_t stream)
 {
-    (void)mode;
     if (n_cap <= 0) return MOEA_OK;
     if (H <= 0) return set_error(MOEA_ERR_INVALID_ARGUMENT, "associate: no directions");
+    if (mode != MOEA_ASSOC_TREE && mode != MOEA_ASSOC_SCAN)
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "associate: mode %d", mode);
+    if (mode == MOEA_ASSOC_TREE) {
+        if (!direction_tree_ready(ws, refs, M, H))
+            return set_error(MOEA_ERR_STATE, "associate: no cone tree prepared for these directions");
+        if (ws.tree_depth <= kTreeMaxDepth) {
+            const TreeArgs t{ws.tree_dirs, ws.tree_order, ws.tree_center, ws.tree_cos, ws.tree_sin,
+                             ws.tree_link, H, ws.tree_nodes, ws.tree_delta};
+            const int blocks = ceil_div(n_cap, kTreeWarps);
+            switch (M) {
+#define MOEA_TREE_CASE(K) case K: assoc_tree<K><<<blocks, kTreeWarps * 32, 0, stream>>>(x, x_stride, scale, t, d_n, idx, dist); break;
+            MOEA_TREE_CASE(1) MOEA_TREE_CASE(2) MOEA_TREE_CASE(3) MOEA_TREE_CASE(4)
+            MOEA_TREE_CASE(5) MOEA_TREE_CASE(6) MOEA_TREE_CASE(7) MOEA_TREE_CASE(8)
+            MOEA_TREE_CASE(9) MOEA_TREE_CASE(10) MOEA_TREE_CASE(11) MOEA_TREE_CASE(12)
+            MOEA_TREE_CASE(13) MOEA_TREE_CASE(14) MOEA_TREE_CASE(15) MOEA_TREE_CASE(16)
+#undef MOEA_TREE_CASE
+            default: return set_error(MOEA_ERR_UNSUPPORTED, "associate: M=%d", M);
+            }
+            MOEA_CUDA_TRY(cudaGetLastError());
+            return MOEA_OK;
+        }
+        // a tree deeper than the kernel's stack: visit every direction instead
+    }
+    dir_delta_kernel<<<1, 1024, 0, stream>>>(refs, M, H, ws.dir_delta);
     assoc_reset<<<ceil_div(n_cap, 256), 256, 0, stream>>>(ws.assoc_best, n_cap);
     const int sms = sm_count(ws.device);
     switch (M) {
-#define MOEA_ASSOC_CASE(K) case K: launch_assoc<K>(x, x_stride, scale, refs, H, d_n, n_cap, ws.assoc_best, sms, stream); break;
+#define MOEA_ASSOC_CASE(K) case K: launch_assoc<K>(x, x_stride, scale, refs, H, d_n, n_cap, ws.dir_delta, ws.assoc_best, sms, stream); break;
     MOEA_ASSOC_CASE(1) MOEA_ASSOC_CASE(2) MOEA_ASSOC_CASE(3) MOEA_ASSOC_CASE(4)
     MOEA_ASSOC_CASE(5) MOEA_ASSOC_CASE(6) MOEA_ASSOC_CASE(7) MOEA_ASSOC_CASE(8)
     MOEA_ASSOC_CASE(9) MOEA_ASSOC_CASE(10) MOEA_ASSOC_CASE(11) MOEA_ASSOC_CASE(12)

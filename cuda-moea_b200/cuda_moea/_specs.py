@@ -81,7 +81,7 @@ class NSGA3EnvironmentSelector(_Spec):
     cv_clip_upper: float = 0.0
     cv_log_alpha: float = 0.0
     feasibility_epsilon: float = 0.0
-    # B200 extension: 0 = SIMT association, 1 = tensor-core candidate search
+    # B200 extension: 0 = cone-tree association search, 1 = full scan (same results)
     association_mode: int = 0
 
 

@@ -88,7 +88,11 @@ def normalize(ws: Workspace, objs: torch.Tensor, ideal: torch.Tensor):
     return f, rcp, ext
 
 
-def associate(ws: Workspace, x: torch.Tensor, refs: torch.Tensor, mode: int = 0):
+ASSOC_TREE = 0  # cone-tree search (default)
+ASSOC_SCAN = 1  # every direction visited
+
+
+def associate(ws: Workspace, x: torch.Tensor, refs: torch.Tensor, mode: int = ASSOC_TREE):
     M, n = x.shape
     idx = torch.empty(n, dtype=torch.int32, device=x.device)
     dist = torch.empty(n, dtype=torch.float32, device=x.device)

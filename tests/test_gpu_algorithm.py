@@ -129,6 +129,24 @@ def test_graph_replay_equals_direct_launches(kind):
     assert runs[0][2] == runs[1][2]
 
 
+@pytest.mark.parametrize("problem,dirs", [("DTLZ1", None), ("DTLZ2", "user_unnormalised")])
+def test_association_modes_give_identical_runs(problem, dirs):
+    runs = []
+    for mode in (0, 1):
+        kw = {}
+        if dirs == "user_unnormalised":
+            d = torch.rand(150, 3, generator=torch.Generator().manual_seed(3)) * 2 + 0.05
+            kw["reference_directions"] = cm.UserDefinedDirections(d, normalize=False)
+        prob = cm.DTLZ1(7, 3) if problem == "DTLZ1" else cm.DTLZ2(12, 3)
+        a = cm.NSGA3(population_size=1000, max_generations=12, problem=prob, seed=11,
+                     environment_selector=cm.NSGA3EnvironmentSelector(association_mode=mode),
+                     print_progress=False, **kw)
+        r = a.run()
+        runs.append((r.variables.cpu(), r.objectives.cpu()))
+    torch.testing.assert_close(runs[0][0], runs[1][0], rtol=0, atol=0)
+    torch.testing.assert_close(runs[0][1], runs[1][1], rtol=0, atol=0)
+
+
 def test_nsga3_dtlz2_quality():
     algo = cm.NSGA3(population_size=92, max_generations=100, problem=cm.DTLZ2(12, 3), seed=2887,
                     print_progress=False)

@@ -125,9 +125,10 @@ def test_extract_ideal_normalize_associate(st, ws, oracle):
     np.testing.assert_array_equal(dist_g.cpu().numpy(), dist_w)
 
 
+@pytest.mark.parametrize("mode", [0, 1])
 @pytest.mark.parametrize("M,n,H_mode", [(3, 3000, (1, 254)), (3, 500, (1, 12)), (5, 2000, (0, 3000)),
                                         (8, 1500, (0, 900)), (10, 1200, (0, 2000)), (2, 4096, (1, 999))])
-def test_association_bit_exact(st, ws, oracle, M, n, H_mode):
+def test_association_bit_exact(st, ws, oracle, M, n, H_mode, mode):
     rng = np.random.default_rng(M + n)
     refs = oracle.reference_directions(H_mode[0], H_mode[1], M)
     x = rng.random((M, n)).astype(np.float32) * rng.random(n).astype(np.float32) * 3
@@ -135,9 +136,73 @@ def test_association_bit_exact(st, ws, oracle, M, n, H_mode):
     x[:, 10:14] = 0.0                       # at the ideal point: every distance is 0
     x[0, 14] = np.inf                       # non-finite point: no association
     idx_w, dist_w = oracle.associate(x, refs)
-    idx_g, dist_g = st.associate(ws, _t(x), _t(refs))
+    idx_g, dist_g = st.associate(ws, _t(x), _t(refs), mode)
     np.testing.assert_array_equal(idx_g.cpu().numpy(), idx_w)
     np.testing.assert_array_equal(dist_g.cpu().numpy(), dist_w)
+
+
+def _dirs(rng, kind, M, H):
+    if kind == "random_unit":
+        r = np.abs(rng.standard_normal((M, H))).astype(np.float32)
+        return (r / np.sqrt((r.astype(np.float64) ** 2).sum(0))).astype(np.float32)
+    if kind == "signed_unit":      # directions in every orthant, points too
+        r = rng.standard_normal((M, H)).astype(np.float32)
+        return (r / np.sqrt((r.astype(np.float64) ** 2).sum(0))).astype(np.float32)
+    if kind == "non_unit":         # user directions left unnormalised: full re-score
+        return (rng.random((M, H)) * 3 + 0.01).astype(np.float32)
+    if kind == "duplicates":       # repeated directions: ties go to the smaller index
+        base = rng.random((M, H // 4)).astype(np.float32) + 0.05
+        base = (base / np.sqrt((base.astype(np.float64) ** 2).sum(0))).astype(np.float32)
+        return np.ascontiguousarray(np.tile(base, 4)[:, rng.permutation(H)])
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("M,H,n,kind", [(3, 4000, 3000, "random_unit"), (3, 2000, 2000, "signed_unit"),
+                                        (4, 1500, 2000, "non_unit"), (3, 2048, 3000, "duplicates"),
+                                        (1, 7, 100, "random_unit"), (2, 31, 500, "signed_unit"),
+                                        (16, 600, 800, "random_unit"), (6, 5000, 1500, "duplicates")])
+def test_association_tree_adversarial(st, ws, oracle, M, H, n, kind):
+    """The cone-tree search against the full scan and the oracle on direction
+    sets the Das-Dennis tests do not reach."""
+    rng = np.random.default_rng(M * 1000 + H)
+    refs = _dirs(rng, kind, M, H)
+    if kind == "signed_unit":
+        x = rng.standard_normal((M, n)).astype(np.float32)
+    else:
+        x = (rng.random((M, n)) * rng.random(n) * 2).astype(np.float32)
+    k = min(16, H)
+    x[:, :k] = refs[:, :k] * 1.5
+    x[:, 16:20] = 0.0
+    x[:, 20] = 1e-30
+    x[:, 21] = 3e18
+    x[1 % M, 22] = np.nan
+    idx_w, dist_w = oracle.associate(x, refs)
+    for mode in (0, 1):
+        idx_g, dist_g = st.associate(ws, _t(x), _t(refs), mode)
+        np.testing.assert_array_equal(idx_g.cpu().numpy(), idx_w, err_msg=f"mode {mode}")
+        np.testing.assert_array_equal(dist_g.cpu().numpy(), dist_w, err_msg=f"mode {mode}")
+
+
+def test_association_tree_full_size(st, oracle):
+    """M=3 with the 32640 Das-Dennis directions of 254 partitions (the bench
+    workload's direction set), 16384 points: tree search == full scan, and a
+    sample against the oracle."""
+    rng = np.random.default_rng(32640)
+    refs = oracle.reference_directions(1, 254, 3)
+    n = 16384
+    x = (rng.random((3, n)) ** 2 * rng.random(n) * 4).astype(np.float32)
+    w = st.Workspace(max_points=n, max_objectives=3, max_directions=refs.shape[1])
+    try:
+        a_i, a_d = st.associate(w, _t(x), _t(refs), 0)
+        b_i, b_d = st.associate(w, _t(x), _t(refs), 1)
+    finally:
+        w.close()
+    np.testing.assert_array_equal(a_i.cpu().numpy(), b_i.cpu().numpy())
+    np.testing.assert_array_equal(a_d.cpu().numpy(), b_d.cpu().numpy())
+    sample = rng.choice(n, 512, replace=False)
+    idx_w, dist_w = oracle.associate(np.ascontiguousarray(x[:, sample]), refs)
+    np.testing.assert_array_equal(a_i.cpu().numpy()[sample], idx_w)
+    np.testing.assert_array_equal(a_d.cpu().numpy()[sample], dist_w)
 
 
 def test_niching_bit_exact(st, ws, oracle):
@@ -158,7 +223,8 @@ def test_niching_bit_exact(st, ws, oracle):
 @pytest.mark.parametrize("seed,M,N,kind", [(0, 3, 92, "dtlz1"), (1, 3, 1024, "dtlz1"),
                                            (2, 3, 2048, "uniform"), (3, 5, 600, "ties"),
                                            (4, 8, 512, "uniform"), (5, 3, 4096, "correlated")])
-def test_nsga3_select_bit_exact(st, ws, oracle, seed, M, N, kind):
+@pytest.mark.parametrize("assoc_mode", [0, 1])
+def test_nsga3_select_bit_exact(st, ws, oracle, seed, M, N, kind, assoc_mode):
     rng = np.random.default_rng(seed)
     objs = _population(rng, M, 2 * N, kind)
     cv = _cv(rng, 2 * N, "mixed" if seed % 2 else "feasible")
@@ -166,7 +232,7 @@ def test_nsga3_select_bit_exact(st, ws, oracle, seed, M, N, kind):
     ideal = np.full(M, np.inf, np.float32)
     ideal = np.minimum(ideal, objs[:, :N].min(1))
     want = oracle.nsga3_select(cv, objs, refs, 12345, 9, ideal)
-    got = st.nsga3_select(ws, _t(cv), _t(objs), _t(refs), 12345, 9, _t(ideal))
+    got = st.nsga3_select(ws, _t(cv), _t(objs), _t(refs), 12345, 9, _t(ideal), assoc_mode)
     np.testing.assert_array_equal(got["sizes"].cpu().numpy(), want["sizes"])
     np.testing.assert_array_equal(got["survivors"].cpu().numpy(), want["survivors"])
     np.testing.assert_array_equal(got["fronts"].cpu().numpy(), want["fronts"])
