@@ -1004,6 +1004,31 @@ int run_associate(Workspace& ws, const float* x, int x_stride, const float* scal
     return MOEA_OK;
 }
 
+// The full-scan association with caller-provided scratch instead of a
+// workspace: best (n_cap packed minima), delta (1 float), d_n (device count).
+// Used by the allocation-free entry point (noalloc.cu).
+int run_associate_scan_scratch(const float* x, const float* refs, int M, const int* d_n, int n_cap,
+                               int H, int* idx, float* dist, unsigned long long* best, float* delta,
+                               int device, cudaStream_t stream)
+{
+    dir_delta_kernel<<<1, 1024, 0, stream>>>(refs, M, H, delta);
+    assoc_reset<<<ceil_div(n_cap, 256), 256, 0, stream>>>(best, n_cap);
+    const int sms = sm_count(device);
+    switch (M) {
+#define MOEA_SCRATCH_CASE(K) case K: launch_assoc<K>(x, n_cap, nullptr, refs, H, d_n, n_cap, delta, best, sms, stream); break;
+    MOEA_SCRATCH_CASE(1) MOEA_SCRATCH_CASE(2) MOEA_SCRATCH_CASE(3) MOEA_SCRATCH_CASE(4)
+    MOEA_SCRATCH_CASE(5) MOEA_SCRATCH_CASE(6) MOEA_SCRATCH_CASE(7) MOEA_SCRATCH_CASE(8)
+    MOEA_SCRATCH_CASE(9) MOEA_SCRATCH_CASE(10) MOEA_SCRATCH_CASE(11) MOEA_SCRATCH_CASE(12)
+    MOEA_SCRATCH_CASE(13) MOEA_SCRATCH_CASE(14) MOEA_SCRATCH_CASE(15) MOEA_SCRATCH_CASE(16)
+#undef MOEA_SCRATCH_CASE
+    default: return set_error(MOEA_ERR_UNSUPPORTED, "associate: M=%d", M);
+    }
+    MOEA_CUDA_TRY(cudaGetLastError());
+    assoc_finish<<<ceil_div(n_cap, 256), 256, 0, stream>>>(best, d_n, idx, dist);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
 int run_niching(Workspace& ws, uint64_t seed, const int* nds_gidx, const float* dist,
                 const int* idx, const int* sizes, int H, int N, int* selected,
                 cudaStream_t stream)

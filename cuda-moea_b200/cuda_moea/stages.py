@@ -101,6 +101,16 @@ def associate(ws: Workspace, x: torch.Tensor, refs: torch.Tensor, mode: int = AS
     return idx, dist
 
 
+def associate_static(x: torch.Tensor, refs: torch.Tensor):
+    """Full-scan association through the allocation-free entry point."""
+    M, n = x.shape
+    idx = torch.empty(n, dtype=torch.int32, device=x.device)
+    dist = torch.empty(n, dtype=torch.float32, device=x.device)
+    check(lib().moea_associate_static(_p(x), _p(refs), M, n, refs.shape[1], _p(idx), _p(dist),
+                                      _stream()))
+    return idx, dist
+
+
 def niching(ws: Workspace, seed: int, offset: int, nds_gidx, dist, idx, sizes, H: int, N: int):
     sel = torch.empty(N, dtype=torch.int32, device=dist.device)
     off = ctypes.c_uint64(offset)

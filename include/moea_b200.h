@@ -111,6 +111,19 @@ moea_status moea_normalize(moea_workspace* ws, float* d_objs, const float* d_ide
 moea_status moea_associate(moea_workspace* ws, const float* d_x, const float* d_refs, int M,
                            int n, int H, int* d_idx, float* d_dist, int mode, void* stream);
 
+/* Allocation-free variant of moea_associate in MOEA_ASSOC_SCAN mode: no
+ * workspace, no device allocation.  Scratch lives in static device arrays
+ * sized for at most 65536 points (larger n -> MOEA_ERR_INVALID_ARGUMENT).
+ * For callers that hold no workspace and may not allocate during a
+ * generation (strategies that receive only borrowed views).  Calls whose work
+ * overlaps on the device share the scratch and race; the first call on a
+ * device resolves the scratch addresses (not stream-ordered), so make it
+ * before any stream capture that includes this function.  No counterpart in
+ * the reference, whose association always draws scratch from its pool
+ * (nat/src/selection/nsga3/kernels/association.cu:586). */
+moea_status moea_associate_static(const float* d_x, const float* d_refs, int M, int n, int H,
+                                  int* d_idx, float* d_dist, void* stream);
+
 /* NSGA-III niche selection.  d_sizes as produced by moea_nds_extract; the
  * tie-break draws use SplitMix64(offset + i, seed) like the reference and
  * *h_offset is advanced by 2*N_last.  d_selected (N) receives mixed indices
