@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "internal.cuh"
@@ -494,18 +495,42 @@ struct moea_algorithm {
         return cfg.use_graphs && cfg.problem_kind != 0 && cfg.mating != MOEA_MATING_CALLBACK;
     }
 
-    int step()
+    // Work before a generation's body: the constraint activation switch
+    // refreshes parent violations and re-sorts them (problem_evaluator
+    // prepare_parent, dtlz_kernels.cu:1361-1394).
+    int pre_step()
     {
-        if (!initialized) MOEA_TRY(initialize());
-        if (generation >= T) return MOEA_OK;
-        MOEA_CUDA_TRY(cudaSetDevice(cfg.device));
-        // constraint activation switch: refresh parent violations and re-sort
-        // (problem_evaluator prepare_parent, dtlz_kernels.cu:1361-1394)
         if (constrained() && cfg.problem_kind != 0 && cv_switch_node(generation)) {
             MOEA_TRY(run_problem(cfg.problem_kind, vars[P], N, D, M, objs[P], cv[P], stream));
             last_prepared_target = generation;
             MOEA_TRY(prepare());
         }
+        return MOEA_OK;
+    }
+
+    // Work after a generation's body: RVEA direction adaptation
+    // (reference_directions.cu:132-162) and the slot rotation.
+    int post_step()
+    {
+        if (cfg.directions == MOEA_DIRS_ADAPTIVE) {
+            const int interval = std::max(1, (int)std::lround(cfg.adapt_frequency * T));
+            if ((generation + 1) % interval == 0) {
+                MOEA_TRY(run_rvea_adapt(refs0, objs[X], N, nsga3() ? nullptr : d_active, N, M, H, zmin,
+                                        refs, stream));
+                if (!nsga3()) MOEA_TRY(run_rvea_gamma(refs, M, H, gamma, stream));
+            }
+        }
+        std::swap(P, X);
+        ++generation;
+        return MOEA_OK;
+    }
+
+    int step()
+    {
+        if (!initialized) MOEA_TRY(initialize());
+        if (generation >= T) return MOEA_OK;
+        MOEA_CUDA_TRY(cudaSetDevice(cfg.device));
+        MOEA_TRY(pre_step());
         bool done = false;
         if (graphable() && !graph_failed) {
             const int parity = (P == 0) ? 0 : 1;
@@ -542,18 +567,7 @@ struct moea_algorithm {
             }
         }
         if (!done) MOEA_TRY(generation_body());
-        // RVEA direction adaptation (reference_directions.cu:132-162)
-        if (cfg.directions == MOEA_DIRS_ADAPTIVE) {
-            const int interval = std::max(1, (int)std::lround(cfg.adapt_frequency * T));
-            if ((generation + 1) % interval == 0) {
-                MOEA_TRY(run_rvea_adapt(refs0, objs[X], N, nsga3() ? nullptr : d_active, N, M, H, zmin,
-                                        refs, stream));
-                if (!nsga3()) MOEA_TRY(run_rvea_gamma(refs, M, H, gamma, stream));
-            }
-        }
-        std::swap(P, X);
-        ++generation;
-        return MOEA_OK;
+        return post_step();
     }
 
     int active_count_sync()
@@ -809,6 +823,220 @@ moea_status moea_algorithm_device_status(moea_algorithm* a, int* h_status)
     if (!a->initialized) return MOEA_OK;
     MOEA_CUDA_TRY(cudaMemcpy(h_status, a->ws.counters + 6, sizeof(int), cudaMemcpyDeviceToHost));
     return MOEA_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched instances: many independent algorithms advance one generation per
+// CUDA graph launch.  Each instance keeps its own buffers, workspace and
+// generation body (so its results are those of running it alone); the batch
+// captures all bodies into one graph as parallel branches forked from and
+// joined into the batch stream.  Work outside the bodies (initialisation, the
+// constraint-activation switch, direction adaptation, views) runs on the
+// batch stream, so it is ordered with the graph launches.  Instances peel
+// their fronts with one ordinary CTA instead of a cooperative grid, so that
+// branches may run side by side.
+// ---------------------------------------------------------------------------
+
+struct moea_batch {
+    std::vector<moea_algorithm*> inst;
+    std::vector<cudaStream_t> branch;
+    std::vector<cudaEvent_t> join;
+    cudaEvent_t fork = nullptr;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    int T = 0;
+    int generation = 0;
+    cudaGraphExec_t graph[2] = {};
+    int graph_kernels = 0;
+
+    ~moea_batch()
+    {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& g : graph)
+            if (g) cudaGraphExecDestroy(g);
+        for (moea_algorithm* a : inst) delete a;
+        for (cudaStream_t s : branch) cudaStreamDestroy(s);
+        for (cudaEvent_t e : join) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+
+    int capture(cudaGraphExec_t* out)
+    {
+        MOEA_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        int st = MOEA_OK;
+        cudaError_t ce = cudaEventRecord(fork, stream);
+        for (size_t i = 0; i < inst.size() && st == MOEA_OK && ce == cudaSuccess; ++i) {
+            moea_algorithm* a = inst[i];
+            ce = cudaStreamWaitEvent(branch[i], fork, 0);
+            if (ce != cudaSuccess) break;
+            a->stream = branch[i];
+            st = a->generation_body();
+            a->stream = stream;
+            if (st == MOEA_OK) ce = cudaEventRecord(join[i], branch[i]);
+            if (st == MOEA_OK && ce == cudaSuccess) ce = cudaStreamWaitEvent(stream, join[i], 0);
+        }
+        cudaGraph_t g = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(stream, &g);
+        if (st == MOEA_OK && ce == cudaSuccess && ee == cudaSuccess) {
+            size_t count = 0;
+            if (cudaGraphGetNodes(g, nullptr, &count) == cudaSuccess && count > 0) {
+                std::vector<cudaGraphNode_t> nodes(count);
+                cudaGraphGetNodes(g, nodes.data(), &count);
+                int k = 0;
+                for (auto nd : nodes) {
+                    cudaGraphNodeType ty;
+                    if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++k;
+                }
+                graph_kernels = k;
+            }
+            ce = cudaGraphInstantiate(out, g, 0);
+        }
+        if (g) cudaGraphDestroy(g);
+        if (st != MOEA_OK) return st;
+        if (ce != cudaSuccess || ee != cudaSuccess) {
+            const cudaError_t e = ce != cudaSuccess ? ce : ee;
+            cudaGetLastError();
+            return set_error(MOEA_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(e));
+        }
+        return MOEA_OK;
+    }
+
+    int step()
+    {
+        if (generation >= T) return MOEA_OK;
+        MOEA_CUDA_TRY(cudaSetDevice(device));
+        for (moea_algorithm* a : inst) MOEA_TRY(a->pre_step());
+        const int parity = (inst[0]->P == 0) ? 0 : 1;
+        if (!graph[parity]) MOEA_TRY(capture(&graph[parity]));
+        MOEA_CUDA_TRY(cudaGraphLaunch(graph[parity], stream));
+        for (moea_algorithm* a : inst) MOEA_TRY(a->post_step());
+        ++generation;
+        return MOEA_OK;
+    }
+};
+
+extern "C" {
+
+moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void* stream, moea_batch** out)
+{
+    if (!cfgs || count < 1 || !out) return set_error(MOEA_ERR_INVALID_ARGUMENT, "batch: bad arguments");
+    *out = nullptr;
+    const int device = cfgs[0].device, T = cfgs[0].max_generations;
+    for (int i = 0; i < count; ++i) {
+        const moea_algorithm_config& c = cfgs[i];
+        if (c.device != device || c.max_generations != T)
+            return set_error(MOEA_ERR_INVALID_ARGUMENT,
+                             "batch: instance %d differs in device or max_generations from instance 0", i);
+        if (c.problem_kind == 0 || c.mating == MOEA_MATING_CALLBACK)
+            return set_error(MOEA_ERR_INVALID_ARGUMENT,
+                             "batch: instance %d uses a callback; batched instances need built-in problems "
+                             "and mating", i);
+    }
+    MOEA_CUDA_TRY(cudaSetDevice(device));
+    moea_batch* b = new (std::nothrow) moea_batch();
+    if (!b) return set_error(MOEA_ERR_OUT_OF_MEMORY, "host allocation failed");
+    b->device = device;
+    b->T = T;
+    int st = MOEA_OK;
+    cudaError_t ce = cudaSuccess;
+    if (stream) {
+        b->stream = (cudaStream_t)stream;
+    } else {
+        ce = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+        b->own_stream = ce == cudaSuccess;
+    }
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    for (int i = 0; i < count && st == MOEA_OK && ce == cudaSuccess; ++i) {
+        moea_algorithm_config c = cfgs[i];
+        c.stream = b->stream;
+        c.use_graphs = 0;
+        moea_algorithm* a = nullptr;
+        st = moea_algorithm_create(&c, &a);
+        if (st != MOEA_OK) break;
+        b->inst.push_back(a);
+        st = a->initialize();
+        if (st != MOEA_OK) {
+            const std::string msg = last_error();  // set_error rewrites the buffer it returns
+            st = set_error(st, "batch instance %d: %s", i, msg.c_str());
+            break;
+        }
+        a->ws.peel_single_cta = true;
+        cudaStream_t s = nullptr;
+        cudaEvent_t e = nullptr;
+        ce = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        if (ce == cudaSuccess) b->branch.push_back(s);
+        if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        if (ce == cudaSuccess) b->join.push_back(e);
+    }
+    if (st == MOEA_OK && ce != cudaSuccess) {
+        cudaGetLastError();
+        st = set_error(MOEA_ERR_CUDA, "batch: %s", cudaGetErrorString(ce));
+    }
+    if (st != MOEA_OK) {
+        delete b;
+        return st;
+    }
+    *out = b;
+    return MOEA_OK;
+}
+
+void moea_batch_destroy(moea_batch* b) { delete b; }
+
+moea_status moea_batch_step(moea_batch* b)
+{
+    if (!b) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL batch");
+    return b->step();
+}
+
+moea_status moea_batch_run(moea_batch* b, int generations, double* h_total_ms)
+{
+    if (!b) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL batch");
+    MOEA_CUDA_TRY(cudaSetDevice(b->device));
+    cudaEvent_t e0, e1;
+    MOEA_CUDA_TRY(cudaEventCreate(&e0));
+    MOEA_CUDA_TRY(cudaEventCreate(&e1));
+    MOEA_CUDA_TRY(cudaEventRecord(e0, b->stream));
+    int st = MOEA_OK;
+    for (int g = 0; (generations < 0 || g < generations) && b->generation < b->T && st == MOEA_OK; ++g)
+        st = b->step();
+    cudaEventRecord(e1, b->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != MOEA_OK) return st;
+    if (h_total_ms) *h_total_ms = ms;
+    for (moea_algorithm* a : b->inst) MOEA_TRY(workspace_check_status(a->ws, b->stream));
+    return MOEA_OK;
+}
+
+moea_status moea_batch_synchronize(moea_batch* b)
+{
+    if (!b) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL batch");
+    MOEA_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    for (moea_algorithm* a : b->inst) MOEA_TRY(workspace_check_status(a->ws, b->stream));
+    return MOEA_OK;
+}
+
+moea_status moea_batch_info(moea_batch* b, int* h_count, int* h_generation, int* h_graph_kernels)
+{
+    if (!b) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL batch");
+    if (h_count) *h_count = (int)b->inst.size();
+    if (h_generation) *h_generation = b->generation;
+    if (h_graph_kernels) *h_graph_kernels = b->graph_kernels;
+    return MOEA_OK;
+}
+
+moea_status moea_batch_view(moea_batch* b, int index, moea_population_view* out)
+{
+    if (!b || !out || index < 0 || index >= (int)b->inst.size())
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "batch_view: bad arguments");
+    return moea_algorithm_view(b->inst[index], out);
 }
 
 }  // extern "C"

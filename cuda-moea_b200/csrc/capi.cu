@@ -73,7 +73,7 @@ void free_all(Workspace& ws)
                     ws.norm_part_idx, ws.rcp_b, ws.extreme, ws.ideal_tmp, ws.assoc_best,
                     ws.assoc_idx, ws.assoc_dist, ws.rho, ws.sel_vals[0], ws.sel_vals[1],
                     ws.rank, ws.selected, ws.flags, ws.offset_dev, ws.cub_tmp, ws.tree_dirs,
-                    ws.tree_order, ws.tree_center, ws.dir_delta};
+                    ws.tree_order, ws.tree_center, ws.dir_delta, ws.chunk_keys, ws.chunk_bits};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     ws = Workspace{};
@@ -106,6 +106,8 @@ int workspace_init(Workspace& ws, int device, int n_max, int m_max, int h_max)
     A(ws.sorted_f, n * (size_t)(m_max > 1 ? m_max - 1 : 1));
     A(ws.qinfo, n); A(ws.head, n); A(ws.run_start, n);
     A(ws.blocker, n); A(ws.front_sorted, n); A(ws.front_list, n);
+    A(ws.chunk_keys, (size_t)(m_max > 1 ? m_max - 1 : 1) * ws.words * 32);
+    A(ws.chunk_bits, (size_t)(m_max > 1 ? m_max - 1 : 1) * ws.words * 33);
     A(ws.counters, 16);
     A(ws.fronts, n); A(ws.nds_gidx, n); A(ws.sizes, 8);
     A(ws.chunk_counts, 2 * (size_t)ceil_div(n_max, 1024) + 2);

@@ -68,6 +68,8 @@ struct Workspace {
     int* qinfo = nullptr;           // per sorted position: dup position | infeasible bit
     int* head = nullptr;            // run heads
     int* run_start = nullptr;       // scanned run heads
+    uint32_t* chunk_keys = nullptr; // [(m_max-1)][words*32] sorted objective keys per word
+    uint32_t* chunk_bits = nullptr; // [(m_max-1)][words*33] prefix position sets per word
     int* blocker = nullptr;         // per sorted position: last known unassigned dominator
     int* front_sorted = nullptr;    // per sorted position: front index or -1
     int* front_list = nullptr;      // members of each peeled front, front by front
@@ -76,6 +78,7 @@ struct Workspace {
                                     // [6] device status, [7..] spare
     int peel_grid = 0;              // co-resident CTAs of the peel kernel
     int peel_smem = 0;
+    bool peel_single_cta = false;   // peel with one ordinary CTA (instances of a batch)
 
     // --- NSGA-III stages ---
     int* fronts = nullptr;          // fronts of the merged population (point order)

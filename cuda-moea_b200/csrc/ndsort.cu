@@ -18,9 +18,12 @@
 //       feasible q:    p dominates q  <=>  p < dup[q] and f_m(p) <= f_m(q), m >= 1
 //     which is the reference relation (non_dominated_sort.cu:190-239) with one
 //     integer and M-1 float comparisons per pair on the lower triangle only.
-//  3. A tile kernel evaluates that test, one dominatee per lane against
-//     dominator objectives broadcast from shared memory, and stores for every
-//     q the bit row of its dominators (sorted positions, 32 per word).
+//  3. For every word of 32 sorted positions and every objective m >= 1 the
+//     positions are sorted by f_m once, with the prefix sets of that order.
+//     A tile kernel then evaluates the test for one dominatee per lane: the
+//     dominators of a word with f_m(p) <= f_m(q) are one prefix set, found
+//     by a binary search, and the row word is the AND of those sets with the
+//     dup mask.  It stores for every q the bit row of its dominators.
 //  4. One cooperative persistent kernel peels the fronts: q joins front k when
 //     no still-unassigned point is left in its row.  Each point remembers one
 //     unassigned dominator ("blocker"); while that blocker is unassigned the
@@ -139,32 +142,79 @@ __global__ void nds_finalize_rows(int n, const uint64_t* __restrict__ key0,
 // 2. dominance rows
 // ---------------------------------------------------------------------------
 
-// Dominator words per tile CTA (32 positions each), so that the staged
-// dominator objectives stay within 16 KB of shared memory.
+// Order key of an objective value for the dominance test; NaN maps above
+// every other key so that a NaN dominator never satisfies key(p) <= key(q).
+__device__ __forceinline__ uint32_t dom_key(float f)
+{
+    return isnan(f) ? 0xFFFFFFFFu : float_order_key(f);
+}
+
+// Per word of 32 sorted positions and per objective m >= 1: the 32 order
+// keys in ascending order (keys[m][32 w + k]) and the prefix sets
+// bits[m][33 w + k] = positions (bit j = position 32 w + j) of the k smallest
+// keys, k = 0..32.  For a value v, the positions of the word whose objective
+// is <= v are bits[m][33 w + c] with c = #{keys <= key(v)}: ties at the
+// boundary all lie inside the prefix, whatever their order.  Positions >= n
+// get the NaN key.  One warp per (word, objective): bitonic sort of
+// (key, lane) pairs, then an inclusive OR-scan of the lane bits.
+__global__ void nds_chunks(const float* __restrict__ sf, int sf_stride, int n, int W, int MF,
+                           uint32_t* __restrict__ ckeys, uint32_t* __restrict__ cbits)
+{
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (gw >= W * MF) return;
+    const int m = gw / W, w = gw - m * W;
+    const int p = w * 32 + lane;
+    const uint32_t key = (p < n) ? dom_key(sf[(size_t)m * sf_stride + p]) : 0xFFFFFFFFu;
+    unsigned long long kv = ((unsigned long long)key << 32) | (unsigned)lane;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const unsigned long long o = __shfl_xor_sync(0xFFFFFFFFu, kv, j);
+            const bool take_min = ((lane & j) == 0) == ((lane & k) == 0);
+            kv = take_min ? (o < kv ? o : kv) : (o > kv ? o : kv);
+        }
+    }
+    uint32_t pre = 1u << (unsigned)(kv & 31ull);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, pre, o);
+        if (lane >= o) pre |= t;
+    }
+    ckeys[(size_t)m * W * 32 + (size_t)w * 32 + lane] = (uint32_t)(kv >> 32);
+    uint32_t* b = cbits + (size_t)m * W * 33 + (size_t)w * 33;
+    b[lane + 1] = pre;
+    if (lane == 0) b[0] = 0u;
+}
+
+// Dominator words per tile CTA (32 positions each), sized so that the staged
+// word tables and the transposed output fit in 48 KB of shared memory.
 template <int M>
 struct TileCfg {
     static constexpr int kPW = (M <= 4) ? 32 : ((M <= 8) ? 16 : 8);
-    static constexpr int kMF = (M > 1) ? M - 1 : 1;   // staged objectives 1..M-1
+    static constexpr int kMF = (M > 1) ? M - 1 : 1;   // objectives 1..M-1
 };
 
 // One CTA covers kQB dominatees q (one per lane of warps 0-3, again of warps
 // 4-7) against kPW words of dominator positions p (the first half of the
-// words for warps 0-3, the second half for warps 4-7).  The p objectives are
-// staged in shared memory and read as warp-wide broadcasts, four positions
-// per 16-byte load; each lane keeps its q's objectives in registers and
-// builds the 32-bit word of its row directly, so one warp instruction
-// evaluates one comparison for 32 pairs.  Words are transposed through shared
-// memory and written as coalesced row segments.  The epilogue raises
-// blocker[q] to the highest dominator position seen, so that after the kernel
-// blocker[q] == -1 exactly for the points that nothing dominates (front 0).
+// words for warps 0-3, the second half for warps 4-7).  The word tables of
+// nds_chunks are staged in shared memory; for each word and objective a lane
+// finds the count of dominator keys <= its own key with a six-probe search
+// and ANDs the prefix set of that count into its row word, so a word of 32
+// pairs costs about 13 integer operations per objective instead of 32
+// comparisons.  Words are transposed through shared memory and written as
+// coalesced row segments.  The epilogue raises blocker[q] to the highest
+// dominator position seen, so that after the kernel blocker[q] == -1 exactly
+// for the points that nothing dominates (front 0).
 template <int M>
 __global__ void __launch_bounds__(kTileThreads)
-nds_tiles(const float* __restrict__ sf, int sf_stride, const int* __restrict__ qinfo, int n, int W,
-          uint32_t* __restrict__ rows, int* __restrict__ blocker)
+nds_tiles(const float* __restrict__ sf, int sf_stride, const int* __restrict__ qinfo,
+          const uint32_t* __restrict__ ckeys, const uint32_t* __restrict__ cbits, int n, int W,
+          int Wc, uint32_t* __restrict__ rows, int* __restrict__ blocker)
 {
     constexpr int PW = TileCfg<M>::kPW;
     constexpr int MF = TileCfg<M>::kMF;
-    constexpr int P = PW * 32;
     const int q0 = blockIdx.y * kQB;
     if (q0 >= n) return;
     const int qend = min(q0 + kQB, n);
@@ -174,28 +224,31 @@ nds_tiles(const float* __restrict__ sf, int sf_stride, const int* __restrict__ q
     if (w0 >= nwords) return;
     const int wcount = min(PW, nwords - w0);
 
-    __shared__ __align__(16) float s_p[MF][P];
+    __shared__ uint32_t s_key[MF][PW * 32];
+    __shared__ uint32_t s_bits[MF][PW * 33];
     __shared__ uint32_t so[kQB][PW + 1];
-    const int p0 = w0 * 32;
     if (M > 1) {
         for (int t = threadIdx.x; t < wcount * 32; t += kTileThreads) {
-            const int p = p0 + t;
 #pragma unroll
-            for (int m = 0; m < MF; ++m) s_p[m][t] = (p < n) ? sf[(size_t)m * sf_stride + p] : 0.0f;
+            for (int m = 0; m < MF; ++m) s_key[m][t] = ckeys[(size_t)m * Wc * 32 + (size_t)w0 * 32 + t];
+        }
+        for (int t = threadIdx.x; t < wcount * 33; t += kTileThreads) {
+#pragma unroll
+            for (int m = 0; m < MF; ++m) s_bits[m][t] = cbits[(size_t)m * Wc * 33 + (size_t)w0 * 33 + t];
         }
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ql = (warp & 3) * 32 + lane;
     const int q = q0 + ql;
-    float qf[MF];
+    uint32_t qk[MF];
     int dup = 0;
     bool inf = false;
 #pragma unroll
-    for (int m = 0; m < MF; ++m) qf[m] = 0.0f;
+    for (int m = 0; m < MF; ++m) qk[m] = 0u;
     if (q < n) {
         if (M > 1) {
 #pragma unroll
-            for (int m = 0; m < MF; ++m) qf[m] = sf[(size_t)m * sf_stride + q];
+            for (int m = 0; m < MF; ++m) qk[m] = dom_key(sf[(size_t)m * sf_stride + q]);
         }
         const uint32_t info = (uint32_t)qinfo[q];
         inf = (info & kInfeasibleBit) != 0u;
@@ -213,21 +266,19 @@ nds_tiles(const float* __restrict__ sf, int sf_stride, const int* __restrict__ q
             const uint32_t mask = rem >= 32 ? 0xFFFFFFFFu : (rem <= 0 ? 0u : ((1u << rem) - 1u));
             const bool need = mask != 0u && !inf;
             if (M > 1 && __any_sync(0xFFFFFFFFu, need)) {
-                uint32_t cmp = 0u;
-                constexpr int kUnroll = (MF > 7) ? 2 : 8;
-#pragma unroll kUnroll
-                for (int j = 0; j < 32; j += 4) {
-                    bool d0 = true, d1 = true, d2 = true, d3 = true;
+                uint32_t cmp = 0xFFFFFFFFu;
 #pragma unroll
-                    for (int m = 0; m < MF; ++m) {
-                        const float4 v = *reinterpret_cast<const float4*>(&s_p[m][wl * 32 + j]);
-                        d0 &= v.x <= qf[m];
-                        d1 &= v.y <= qf[m];
-                        d2 &= v.z <= qf[m];
-                        d3 &= v.w <= qf[m];
-                    }
-                    cmp |= ((uint32_t)d0 << j) | ((uint32_t)d1 << (j + 1)) | ((uint32_t)d2 << (j + 2)) |
-                           ((uint32_t)d3 << (j + 3));
+                for (int m = 0; m < MF; ++m) {
+                    const uint32_t* sk = &s_key[m][wl * 32];
+                    const uint32_t v = qk[m];
+                    int k = 0;
+                    k += (sk[k + 15] <= v) ? 16 : 0;
+                    k += (sk[k + 7] <= v) ? 8 : 0;
+                    k += (sk[k + 3] <= v) ? 4 : 0;
+                    k += (sk[k + 1] <= v) ? 2 : 0;
+                    k += (sk[k] <= v) ? 1 : 0;
+                    k += (sk[k] <= v) ? 1 : 0;   // reaches 32 only from k == 31
+                    cmp &= s_bits[m][wl * 33 + k];
                 }
                 bits = inf ? mask : (mask & cmp);
             } else {
@@ -268,6 +319,11 @@ __device__ bool grid_barrier(int* counters, unsigned nblocks)
 {
     __shared__ int s_ok;
     __syncthreads();
+    if (nblocks == 1) {  // single-CTA peel: a block barrier suffices
+        if (threadIdx.x == 0) counters[9] = atomicAdd(counters + 1, 0);
+        __syncthreads();
+        return true;
+    }
     if (threadIdx.x == 0) {
         volatile int* vgen = counters + 5;
         volatile int* vstatus = counters + 6;
@@ -434,9 +490,15 @@ void launch_tiles(const Workspace& ws, int n, cudaStream_t stream)
 {
     const int nqb = ceil_div(n, kQB);
     const int maxw = ceil_div(n, 32);
+    if (M > 1) {
+        const int warps = maxw * (M - 1);
+        nds_chunks<<<ceil_div(warps, 8), 256, 0, stream>>>(ws.sorted_f, ws.n_max, n, maxw, M - 1,
+                                                         ws.chunk_keys, ws.chunk_bits);
+    }
     dim3 grid(ceil_div(maxw, TileCfg<M>::kPW), nqb);
-    nds_tiles<M><<<grid, kTileThreads, 0, stream>>>(ws.sorted_f, ws.n_max, ws.qinfo, n,
-                                                     ws.words, ws.rows, ws.blocker);
+    nds_tiles<M><<<grid, kTileThreads, 0, stream>>>(ws.sorted_f, ws.n_max, ws.qinfo, ws.chunk_keys,
+                                                     ws.chunk_bits, n, ws.words, maxw, ws.rows,
+                                                     ws.blocker);
 }
 
 }  // namespace
@@ -523,7 +585,7 @@ int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_f
     const int wpb = kPeelThreads / 32;
     int grid = ceil_div(ceil_div(n, 32), wpb);
     if (grid > ws.peel_grid) grid = ws.peel_grid;
-    if (grid < 1) grid = 1;
+    if (grid < 1 || ws.peel_single_cta) grid = 1;
     const uint32_t* rows = ws.rows;
     int Wp = ws.words;
     int nn = n, tt = target;
@@ -545,7 +607,14 @@ int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_f
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    MOEA_CUDA_TRY(cudaLaunchKernelExC(&cfg, (const void*)nds_peel, args));
+    if (grid == 1) {
+        // one CTA needs no co-residency guarantee: an ordinary launch, which
+        // may run beside other work (batched instances)
+        nds_peel<<<1, kPeelThreads, cfg.dynamicSmemBytes, stream>>>(rows, Wp, nn, tt, qi, blk, fs, list,
+                                                                    ctr);
+    } else {
+        MOEA_CUDA_TRY(cudaLaunchKernelExC(&cfg, (const void*)nds_peel, args));
+    }
 
     nds_scatter_fronts<<<G, T, 0, stream>>>(n, perm, ws.front_sorted, fronts);
     MOEA_CUDA_TRY(cudaGetLastError());

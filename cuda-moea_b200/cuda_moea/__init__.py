@@ -8,6 +8,7 @@ include/moea_b200.h); ``cuda_moea.stages`` exposes the individual stages.
 import torch  # noqa: F401  -- CUDA tensors of the results
 
 from .algorithm import Algorithm, AlgorithmBuilder, NSGA3, Population, RVEA, Result
+from .batch import Batch
 from . import problem as _problem
 from .problem import *  # noqa: F401,F403
 from ._specs import (
@@ -21,7 +22,7 @@ from ._specs import (
 __version__ = "0.2.0+b200"
 
 __all__ = [
-    "Algorithm", "AlgorithmBuilder", "NSGA3", "RVEA", "Population", "Result",
+    "Algorithm", "AlgorithmBuilder", "NSGA3", "RVEA", "Population", "Result", "Batch",
     "CudaConfig", "SBX", "PolynomialMutation", "NoMutation",
     "RandomMating", "TournamentMating", "DasDennisDirections",
     "AdaptiveRVEADirections", "UserDefinedDirections",

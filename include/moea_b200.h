@@ -337,6 +337,27 @@ moea_status moea_algorithm_profile_step(moea_algorithm* alg, char* h_names, size
 /* Device status of the last generation (0 ok); also returned as a status by step. */
 moea_status moea_algorithm_device_status(moea_algorithm* alg, int* h_status);
 
+/* ========================================================================
+ * Batched instances (the batching form; no counterpart in the reference,
+ * whose algorithms run one at a time).  count independent algorithms with
+ * built-in problems and mating, one device and one max_generations, advance
+ * together: one CUDA graph launch per generation holds every instance's
+ * generation as a parallel branch.  Each instance's results equal those of
+ * running it alone with moea_algorithm_*.  cfgs[i].stream and use_graphs are
+ * ignored; stream (NULL = internal) orders all of the batch's work.
+ * ====================================================================== */
+typedef struct moea_batch moea_batch;
+moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void* stream,
+                              moea_batch** out);
+void moea_batch_destroy(moea_batch* b);
+moea_status moea_batch_step(moea_batch* b);
+/* generations < 0: run to max_generations.  *h_total_ms: device time. */
+moea_status moea_batch_run(moea_batch* b, int generations, double* h_total_ms);
+moea_status moea_batch_synchronize(moea_batch* b);
+moea_status moea_batch_info(moea_batch* b, int* h_count, int* h_generation, int* h_graph_kernels);
+/* Population view of instance `index` (same contract as moea_algorithm_view). */
+moea_status moea_batch_view(moea_batch* b, int index, moea_population_view* out);
+
 #ifdef __cplusplus
 }
 #endif

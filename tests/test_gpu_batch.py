@@ -1,0 +1,100 @@
+"""GPU: batched instances (cuda_moea.Batch) against the same instances run
+one at a time through the plain algorithm: variables, objectives, violations
+and front indices must be identical after every checked generation."""
+import numpy as np
+import pytest
+import torch
+
+import cuda_moea as cm
+
+pytestmark = pytest.mark.gpu
+
+KINDS = ["DTLZ1", "DTLZ2", "DTLZ3", "DTLZ4", "DTLZ5", "DTLZ6", "DTLZ7"]
+
+
+def _specs(count, seed, n_lo=92, n_hi=700):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        kind = KINDS[i % len(KINDS)]
+        M = int(rng.choice([3, 5, 8]))
+        N = int(rng.integers(n_lo // 2, n_hi // 2 + 1)) * 2
+        D = M + (19 if kind == "DTLZ7" else 9)
+        out.append((kind, M, N, D, 1000 + i))
+    return out
+
+
+def _make(spec, T):
+    kind, M, N, D, seed = spec
+    prob = getattr(cm, kind)(D, M)
+    return cm.NSGA3(population_size=N, max_generations=T, problem=prob, seed=seed, print_progress=False)
+
+
+def _same(a, b):
+    torch.testing.assert_close(a.variables.cpu(), b.variables.cpu(), rtol=0, atol=0, equal_nan=True)
+    torch.testing.assert_close(a.objectives.cpu(), b.objectives.cpu(), rtol=0, atol=0, equal_nan=True)
+    torch.testing.assert_close(a.constraints.cpu(), b.constraints.cpu(), rtol=0, atol=0, equal_nan=True)
+
+
+def test_batch_equals_instances_run_alone():
+    T = 6
+    specs = _specs(12, 7)
+    batch = cm.Batch([_make(s, T) for s in specs])
+    assert len(batch) == 12
+    batch.run(3)
+    mid = [batch.result(i) for i in range(len(specs))]
+    batch.run()
+    assert batch.generation == T
+    assert batch.graph_kernels > 0
+    for i, s in enumerate(specs):
+        alone = _make(s, T)
+        alone.initialize()
+        for _ in range(3):
+            alone.step()
+        r3 = alone.result()
+        _same(mid[i], r3)
+        np.testing.assert_array_equal(mid[i].auxiliary_indices.cpu().numpy(), r3.auxiliary_indices.cpu().numpy())
+        r = alone.run()
+        got = batch.result(i)
+        _same(got, r)
+        np.testing.assert_array_equal(got.auxiliary_indices.cpu().numpy(), r.auxiliary_indices.cpu().numpy())
+
+
+def test_batch_rvea_and_constrained_instances():
+    T = 5
+    algos = [cm.RVEA(population_size=120, max_generations=T, problem=cm.DTLZ2(12, 3), seed=3,
+                     print_progress=False),
+             cm.NSGA3(population_size=200, max_generations=T, problem=cm.C1DTLZ1(12, 3), seed=4,
+                      print_progress=False),
+             cm.NSGA3(population_size=92, max_generations=T, problem=cm.DTLZ4(14, 5), seed=5,
+                      print_progress=False)]
+    batch = cm.Batch(algos)
+    batch.run()
+    alone = [cm.RVEA(population_size=120, max_generations=T, problem=cm.DTLZ2(12, 3), seed=3,
+                     print_progress=False),
+             cm.NSGA3(population_size=200, max_generations=T, problem=cm.C1DTLZ1(12, 3), seed=4,
+                      print_progress=False),
+             cm.NSGA3(population_size=92, max_generations=T, problem=cm.DTLZ4(14, 5), seed=5,
+                      print_progress=False)]
+    for i, a in enumerate(alone):
+        r = a.run()
+        got = batch.result(i)
+        _same(got, r)
+        assert got.active_count == r.active_count
+
+
+def test_batch_rejects_callbacks_and_mismatched_generations():
+    from cuda_moea._lib import MoeaError
+
+    class Sphere(cm.PythonProblem):
+        def __init__(self):
+            super().__init__(4, 2)
+
+        def evaluate(self, x, context):
+            return torch.stack((x.square().sum(1), (x - 1).square().sum(1)), 1)
+
+    with pytest.raises((MoeaError, ValueError)):
+        cm.Batch([cm.NSGA3(population_size=32, max_generations=3, problem=Sphere(), print_progress=False)])
+    with pytest.raises(MoeaError):
+        cm.Batch([cm.NSGA3(population_size=32, max_generations=3, problem=cm.DTLZ2(12, 3), print_progress=False),
+                  cm.NSGA3(population_size=32, max_generations=4, problem=cm.DTLZ2(12, 3), print_progress=False)])
