@@ -155,6 +155,101 @@ def run_reference(args) -> None:
     }))
 
 
+def over_ranks(value: float, op: str, world: int, device) -> float:
+    """value combined over the ranks of the process group: "max" for device
+    times (the job's time is its slowest replica), "sum" for rates of
+    independent replicas.  A single process returns value unchanged."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def replica_seed(seed: int, rank: int) -> int:
+    """Seed of the replica on `rank` (independent replicas, one per GPU)."""
+    return seed + rank
+
+
+BATCH_WORKLOAD = ("batched NSGA-III: 256 independent instances, DTLZ1-7 uniform, M in {3,5,8}, "
+                  "N uniform even in 92..4096, D=M+9 (M+19 for DTLZ7), seeds 0..255, 200-generation runs")
+
+
+def batch_specs(count: int, seed: int = 0):
+    """The batched workload: (kind, M, N, D, seed) per instance."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        kind = int(rng.integers(1, 8))
+        M = int(rng.choice([3, 5, 8]))
+        N = int(rng.integers(46, 2049)) * 2
+        D = M + (19 if kind == 7 else 9)
+        out.append((kind, M, N, D, i))
+    return out
+
+
+def batched_measure(args, torch, cm):
+    """Instance-generations/s of the batch (one graph launch per generation)
+    against the same instances looped one after another through the plain
+    path on one stream; both advance the same generations, after which every
+    instance's front indices and objectives are compared."""
+    specs = batch_specs(args.batch_instances)
+    T = 200
+
+    def make(spec):
+        kind, M, N, D, seed = spec
+        return cm.NSGA3(population_size=N, max_generations=T, problem=getattr(cm, f"DTLZ{kind}")(D, M),
+                        seed=seed, print_progress=False)
+
+    warm, K = 2, args.batch_steps
+    batch = cm.Batch([make(s) for s in specs])
+    batch.run(warm)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(batch.stream)
+    for _ in range(K):
+        batch.step()
+    e1.record(batch.stream)
+    torch.cuda.synchronize()
+    batch_ms = e0.elapsed_time(e1)
+
+    shared = torch.cuda.Stream()
+    with torch.cuda.stream(shared):
+        plain = [make(s) for s in specs]
+        for a in plain:
+            a.initialize()
+        for _ in range(warm):
+            for a in plain:
+                a.step()
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(shared)
+        for _ in range(K):
+            for a in plain:
+                a.step()
+        p1.record(shared)
+        torch.cuda.synchronize()
+    plain_ms = p0.elapsed_time(p1)
+    identical = True
+    for i, a in enumerate(plain):
+        r_b, r_p = batch.result(i), a.result()
+        identical &= bool(torch.equal(r_b.auxiliary_indices, r_p.auxiliary_indices))
+        identical &= bool(torch.equal(r_b.objectives, r_p.objectives))
+    n = len(specs)
+    out = {"workload": BATCH_WORKLOAD, "instances": n, "generations_timed": K,
+           "instance_gen_per_s": n * K / (batch_ms / 1e3),
+           "plain_loop_instance_gen_per_s": n * K / (plain_ms / 1e3),
+           "speedup_vs_plain_loop": plain_ms / batch_ms,
+           "identical_ranks": identical, "graph_kernels_per_generation": batch.graph_kernels,
+           "pair_tests_per_generation": sum((2 * s[2]) ** 2 for s in specs)}
+    batch.close()
+    del plain
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -165,6 +260,9 @@ def main() -> None:
     ap.add_argument("--seed", type=int, default=2887)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=40.0)
+    ap.add_argument("--batch-instances", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=5)
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -188,7 +286,7 @@ def main() -> None:
     N = args.population
     gens = args.warmup + args.steps + 1 + args.steps + 1
     algo = cm.NSGA3(population_size=N, max_generations=gens, problem=cm.DTLZ1(D_VAR, M_OBJ),
-                    reference_directions=cm.DasDennisDirections(PARTITIONS), seed=args.seed + rank,
+                    reference_directions=cm.DasDennisDirections(PARTITIONS), seed=replica_seed(args.seed, rank),
                     print_progress=False, device=local)
     stream = torch.cuda.current_stream()
     algo.initialize()
@@ -213,10 +311,7 @@ def main() -> None:
     if world > 1:
         dist.barrier()
     total_ms = sum(e0.elapsed_time(e1) for e0, e1 in events)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = over_ranks(total_ms, "max", world, "cuda")
     value = world * args.steps / (max_ms / 1000.0)
     graph_on, kernels = algo.graph_info
 
@@ -242,10 +337,7 @@ def main() -> None:
         torch.cuda.synchronize()
         h_vars.copy_(p.variables)
     e2e_ms = sum(e0.elapsed_time(e1) for e0, e1 in ev2)
-    t2 = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps / (float(t2.item()) / 1000.0)
+    e2e_value = world * args.steps / (over_ranks(e2e_ms, "max", world, "cuda") / 1000.0)
 
     # ---- per-stage device times of one generation (direct launches, events)
     stages = algo.profile_step()
@@ -260,6 +352,13 @@ def main() -> None:
     hbm, peak_kind = _peaks()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms == dom_ms else None
     pair_rate = (n_mix * n_mix) / (dom_ms / 1e3) if dom_ms == dom_ms else None
+
+    batched = None
+    if not args.no_batch:
+        del algo
+        torch.cuda.empty_cache()
+        batched = batched_measure(args, torch, cm)
+        batched["instance_gen_per_s"] = over_ranks(batched["instance_gen_per_s"], "sum", world, "cuda")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -287,6 +386,7 @@ def main() -> None:
                          "frac": (achieved / hbm) if achieved else None, "peak_source": peak_kind,
                          "traffic": None, "pair_tests_per_s": pair_rate},
             "cpu_baseline": cpu,
+            "batched": batched,
         }
         print(json.dumps(out))
     if world > 1:
