@@ -36,6 +36,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "NSGA-III gen/s @N=32768,M=3; batched instance-gen/s vs plain, identical ranks"
 WORKLOAD = "NSGA-III DTLZ1 M=3 D=7 N=32768, Das-Dennis H=254 (32640 directions), 1 generation per step"
 N_POP, D_VAR, M_OBJ, PARTITIONS = 32768, 7, 3, 254
+TILES_DRAM_BYTES = 3.00e6 + 210.55e6
 
 
 def _peaks():
@@ -384,7 +385,10 @@ def main() -> None:
             "roofline": {"kernel": "nds_tiles (dominance rows)", "bound": "hbm",
                          "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None, "peak_source": peak_kind,
-                         "traffic": None, "pair_tests_per_s": pair_rate},
+                         # dram__bytes_read.sum + dram__bytes_write.sum of one nds_tiles launch
+                         # at this workload (ncu --set full, profiles/nds_tiles_dtlz1_n65536.md)
+                         "traffic": TILES_DRAM_BYTES if N == N_POP else None,
+                         "algorithmic_bytes": dom_bytes, "pair_tests_per_s": pair_rate},
             "cpu_baseline": cpu,
             "batched": batched,
         }
