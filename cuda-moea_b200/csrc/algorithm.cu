@@ -841,6 +841,14 @@ moea_status moea_algorithm_device_status(moea_algorithm* a, int* h_status)
 
 struct moea_batch {
     std::vector<moea_algorithm*> inst;
+    // fused mode: one launch per stage for each group of instances; the
+    // groups run side by side on their own streams (graph branches)
+    bool fused = false;
+    int fused_groups = 16;
+    BatchInst* d_inst[2] = {};
+    std::vector<FusedGroup> groups;
+    std::vector<cudaStream_t> gstream;
+    std::vector<cudaEvent_t> gjoin;
     std::vector<cudaStream_t> branch;
     std::vector<cudaEvent_t> join;
     cudaEvent_t fork = nullptr;
@@ -849,6 +857,7 @@ struct moea_batch {
     int device = 0;
     int T = 0;
     int generation = 0;
+    bool use_fused = true;
     cudaGraphExec_t graph[2] = {};
     int graph_kernels = 0;
 
@@ -857,6 +866,17 @@ struct moea_batch {
         if (stream) cudaStreamSynchronize(stream);
         for (auto& g : graph)
             if (g) cudaGraphExecDestroy(g);
+        for (auto& d : d_inst)
+            if (d) cudaFree(d);
+        for (auto& g : groups) {
+            if (g.d_ids) cudaFree(g.d_ids);
+            for (auto& b : g.buckets) {
+                if (b.d_ids) cudaFree(b.d_ids);
+                if (b.d_tile_prefix) cudaFree(b.d_tile_prefix);
+            }
+        }
+        for (cudaStream_t gs : gstream) cudaStreamDestroy(gs);
+        for (cudaEvent_t e : gjoin) cudaEventDestroy(e);
         for (moea_algorithm* a : inst) delete a;
         for (cudaStream_t s : branch) cudaStreamDestroy(s);
         for (cudaEvent_t e : join) cudaEventDestroy(e);
@@ -864,12 +884,157 @@ struct moea_batch {
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 
-    int capture(cudaGraphExec_t* out)
+    // Whether every instance fits the fused generation: NSGA-III, built-in
+    // unconstrained problems with at most 256 g-terms, built-in mating, fixed
+    // directions searched by the cone tree, no CV quantisation, 2N <= 8192.
+    static bool fusable(const moea_algorithm* a)
+    {
+        const moea_algorithm_config& c = a->cfg;
+        const int k = c.problem_kind == 7 ? a->D - a->M + 1 : a->D - (a->M - 1);
+        return a->nsga3() && c.problem_kind >= 1 && c.problem_kind <= 8 && k >= 1 && k <= 256 &&
+               2 * a->N <= kFusedMaxPoints && c.mating != MOEA_MATING_CALLBACK &&
+               c.directions != MOEA_DIRS_ADAPTIVE && c.cv_bins <= 0 &&
+               a->assoc_mode() == MOEA_ASSOC_TREE && direction_tree_ready(a->ws, a->refs, a->M, a->H) &&
+               a->ws.tree_depth <= kDirTreeMaxDepth;
+    }
+
+    static BatchInst describe(moea_algorithm* a, int P, int X)
+    {
+        const moea_algorithm_config& c = a->cfg;
+        Workspace& w = a->ws;
+        BatchInst b{};
+        b.N = a->N; b.D = a->D; b.M = a->M; b.H = a->H; b.n = 2 * a->N; b.n_max = w.n_max; b.W = w.words;
+        b.kind = c.problem_kind; b.tournament = c.mating == MOEA_MATING_TOURNAMENT; b.mutate = c.mutation;
+        b.T = a->T;
+        b.sbx_eta0 = c.sbx_eta_initial; b.sbx_eta1 = c.sbx_eta_final; b.sbx_prob = c.sbx_probability;
+        b.sbx_copy = c.sbx_copy_probability; b.pm_eta0 = c.pm_eta_initial; b.pm_eta1 = c.pm_eta_final;
+        b.pm_prob = c.pm_probability;
+        b.seed = a->gen_seed(); b.nich_seed = a->seed;
+        b.varsP = a->vars[P]; b.objsP = a->objs[P]; b.cvP = a->cv[P]; b.rankP = a->rank[P];
+        b.varsO = a->vars[1]; b.objsO = a->objs[1]; b.cvO = a->cv[1];
+        b.varsX = a->vars[X]; b.objsX = a->objs[X]; b.cvX = a->cv[X]; b.rankX = a->rank[X];
+        b.bounds = a->bounds; b.pidx = a->parent_idx; b.d_gen = a->d_gen; b.ideal = a->ideal_last;
+        b.key0 = w.key0; b.key64 = w.key64[0]; b.perm = w.perm[0]; b.vals = w.sel_vals[0];
+        b.sorted_f = w.sorted_f; b.qinfo = w.qinfo; b.blocker = w.blocker; b.front_sorted = w.front_sorted;
+        b.front_list = w.front_list; b.counters = w.counters; b.rows = w.rows; b.chunk_keys = w.chunk_keys;
+        b.chunk_bits = w.chunk_bits; b.fronts = w.fronts; b.nds_gidx = w.nds_gidx; b.sizes = w.sizes;
+        b.nds_objs = w.nds_objs; b.rcp_b = w.rcp_b; b.extreme = w.extreme; b.assoc_idx = w.assoc_idx;
+        b.assoc_dist = w.assoc_dist; b.rho = w.rho; b.selected = w.selected; b.flags = w.flags;
+        b.survivors = a->survivors; b.offset = w.offset_dev;
+        b.t_dirs_orig = a->refs;
+        b.t_dirs = w.tree_dirs; b.t_order = w.tree_order; b.t_center = w.tree_center; b.t_cos = w.tree_cos;
+        b.t_sin = w.tree_sin; b.t_link = w.tree_link; b.t_nodes = w.tree_nodes; b.t_delta = w.tree_delta;
+        return b;
+    }
+
+    int setup_fused()
+    {
+        for (moea_algorithm* a : inst)
+            if (!fusable(a)) return MOEA_OK;
+        for (moea_algorithm* a : inst)
+            if (a->P != 0 || a->X != 2) return MOEA_OK;
+        MOEA_TRY(fused_ndsort_configure());
+        MOEA_TRY(fused_select_configure());
+        const int count = (int)inst.size();
+        for (int parity = 0; parity < 2; ++parity) {
+            std::vector<BatchInst> h(count);
+            for (int i = 0; i < count; ++i) h[i] = describe(inst[i], parity == 0 ? 0 : 2, parity == 0 ? 2 : 0);
+            MOEA_CUDA_TRY(cudaMalloc((void**)&d_inst[parity], sizeof(BatchInst) * count));
+            MOEA_CUDA_TRY(cudaMemcpy(d_inst[parity], h.data(), sizeof(BatchInst) * count, cudaMemcpyHostToDevice));
+        }
+        // groups: longest-processing-time assignment by the pair tests of one
+        // generation, (2N)^2, so that every group carries a similar share
+        const int G = std::max(1, std::min(fused_groups, count));
+        std::vector<int> order(count);
+        for (int i = 0; i < count; ++i) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](int x, int y) {
+            const double cx = (double)inst[x]->N * inst[x]->N, cy = (double)inst[y]->N * inst[y]->N;
+            return cx > cy || (cx == cy && x < y);
+        });
+        std::vector<std::vector<int>> members(G);
+        std::vector<double> load(G, 0.0);
+        for (int i : order) {
+            const int g = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            members[g].push_back(i);
+            load[g] += (double)inst[i]->N * inst[i]->N;
+        }
+        for (int gi = 0; gi < G; ++gi) {
+            std::vector<int>& ids = members[gi];
+            std::sort(ids.begin(), ids.end());
+            FusedGroup g;
+            g.count = (int)ids.size();
+            for (int i : ids) {
+                g.max_n = std::max(g.max_n, 2 * inst[i]->N);
+                g.max_N = std::max(g.max_N, inst[i]->N);
+                g.max_D = std::max(g.max_D, inst[i]->D);
+                g.max_M = std::max(g.max_M, inst[i]->M);
+            }
+            MOEA_CUDA_TRY(cudaMalloc((void**)&g.d_ids, sizeof(int) * ids.size()));
+            MOEA_CUDA_TRY(cudaMemcpy(g.d_ids, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
+            for (int m = 1; m <= kMaxObjectives; ++m) {
+                std::vector<int> bids, prefix{0};
+                int mn = 0;
+                for (int i : ids) {
+                    if (inst[i]->M != m) continue;
+                    bids.push_back(i);
+                    const int n = 2 * inst[i]->N;
+                    prefix.push_back(prefix.back() + fused_tile_blocks(m, n));
+                    mn = std::max(mn, n);
+                }
+                if (bids.empty()) continue;
+                FusedBucket b;
+                b.M = m;
+                b.count = (int)bids.size();
+                b.max_n = mn;
+                b.tile_blocks = prefix.back();
+                MOEA_CUDA_TRY(cudaMalloc((void**)&b.d_ids, sizeof(int) * bids.size()));
+                MOEA_CUDA_TRY(cudaMalloc((void**)&b.d_tile_prefix, sizeof(int) * prefix.size()));
+                MOEA_CUDA_TRY(cudaMemcpy(b.d_ids, bids.data(), sizeof(int) * bids.size(), cudaMemcpyHostToDevice));
+                MOEA_CUDA_TRY(cudaMemcpy(b.d_tile_prefix, prefix.data(), sizeof(int) * prefix.size(),
+                                         cudaMemcpyHostToDevice));
+                g.buckets.push_back(b);
+            }
+            groups.push_back(std::move(g));
+            cudaStream_t gs = nullptr;
+            cudaEvent_t ge = nullptr;
+            MOEA_CUDA_TRY(cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking));
+            gstream.push_back(gs);
+            MOEA_CUDA_TRY(cudaEventCreateWithFlags(&ge, cudaEventDisableTiming));
+            gjoin.push_back(ge);
+        }
+        fused = true;
+        return MOEA_OK;
+    }
+
+    int fused_body(int parity)
+    {
+        const BatchInst* d = d_inst[parity];
+        MOEA_CUDA_TRY(cudaEventRecord(fork, stream));
+        for (size_t gi = 0; gi < groups.size(); ++gi) {
+            const FusedGroup& g = groups[gi];
+            cudaStream_t gs = gstream[gi];
+            MOEA_CUDA_TRY(cudaStreamWaitEvent(gs, fork, 0));
+            MOEA_TRY(fused_reproduce(d, g, gs));
+            MOEA_TRY(fused_evaluate(d, g, gs));
+            MOEA_TRY(fused_ndsort(d, g, gs));
+            MOEA_TRY(fused_select(d, g, gs));
+            MOEA_CUDA_TRY(cudaEventRecord(gjoin[gi], gs));
+            MOEA_CUDA_TRY(cudaStreamWaitEvent(stream, gjoin[gi], 0));
+        }
+        return MOEA_OK;
+    }
+
+    int capture(cudaGraphExec_t* out, int parity)
     {
         MOEA_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         int st = MOEA_OK;
-        cudaError_t ce = cudaEventRecord(fork, stream);
-        for (size_t i = 0; i < inst.size() && st == MOEA_OK && ce == cudaSuccess; ++i) {
+        cudaError_t ce = cudaSuccess;
+        if (fused) {
+            st = fused_body(parity);
+        } else {
+            ce = cudaEventRecord(fork, stream);
+        }
+        for (size_t i = 0; !fused && i < inst.size() && st == MOEA_OK && ce == cudaSuccess; ++i) {
             moea_algorithm* a = inst[i];
             ce = cudaStreamWaitEvent(branch[i], fork, 0);
             if (ce != cudaSuccess) break;
@@ -911,7 +1076,7 @@ struct moea_batch {
         MOEA_CUDA_TRY(cudaSetDevice(device));
         for (moea_algorithm* a : inst) MOEA_TRY(a->pre_step());
         const int parity = (inst[0]->P == 0) ? 0 : 1;
-        if (!graph[parity]) MOEA_TRY(capture(&graph[parity]));
+        if (!graph[parity]) MOEA_TRY(capture(&graph[parity], parity));
         MOEA_CUDA_TRY(cudaGraphLaunch(graph[parity], stream));
         for (moea_algorithm* a : inst) MOEA_TRY(a->post_step());
         ++generation;
@@ -921,7 +1086,8 @@ struct moea_batch {
 
 extern "C" {
 
-moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void* stream, moea_batch** out)
+moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void* stream, int flags,
+                              moea_batch** out)
 {
     if (!cfgs || count < 1 || !out) return set_error(MOEA_ERR_INVALID_ARGUMENT, "batch: bad arguments");
     *out = nullptr;
@@ -941,6 +1107,8 @@ moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void
     if (!b) return set_error(MOEA_ERR_OUT_OF_MEMORY, "host allocation failed");
     b->device = device;
     b->T = T;
+    b->use_fused = (flags & MOEA_BATCH_NO_FUSION) == 0;
+    if (((flags >> 8) & 0xFF) > 0) b->fused_groups = (flags >> 8) & 0xFF;
     int st = MOEA_OK;
     cudaError_t ce = cudaSuccess;
     if (stream) {
@@ -976,6 +1144,7 @@ moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void
         cudaGetLastError();
         st = set_error(MOEA_ERR_CUDA, "batch: %s", cudaGetErrorString(ce));
     }
+    if (st == MOEA_OK && b->use_fused) st = b->setup_fused();
     if (st != MOEA_OK) {
         delete b;
         return st;
@@ -1023,9 +1192,11 @@ moea_status moea_batch_synchronize(moea_batch* b)
     return MOEA_OK;
 }
 
-moea_status moea_batch_info(moea_batch* b, int* h_count, int* h_generation, int* h_graph_kernels)
+moea_status moea_batch_info(moea_batch* b, int* h_count, int* h_generation, int* h_graph_kernels,
+                            int* h_fused)
 {
     if (!b) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL batch");
+    if (h_fused) *h_fused = b->fused ? 1 : 0;
     if (h_count) *h_count = (int)b->inst.size();
     if (h_generation) *h_generation = b->generation;
     if (h_graph_kernels) *h_graph_kernels = b->graph_kernels;

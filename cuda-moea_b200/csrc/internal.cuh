@@ -165,6 +165,62 @@ int run_flag_compaction(Workspace& ws, int n, int* out, cudaStream_t stream);
 
 size_t cub_temp_bytes_needed(int n_max);
 
+// ---- fused batch ------------------------------------------------------------
+// One NSGA-III instance of a fused batch: sizes, parameters and every buffer a
+// generation touches, for one parity of the slot rotation (P parents, O
+// offspring, X next).  The fused generation runs each stage once for all
+// instances: one CTA per instance where the stage needs a block-wide sort,
+// scan or barrier (n = 2N <= kFusedMaxPoints), flattened work items elsewhere.
+constexpr int kFusedMaxPoints = 8192;
+constexpr int kDirTreeMaxDepth = 8;   // stack depth of the tree association kernels
+constexpr int kFusedThreads = 1024;
+constexpr int kFusedItems = kFusedMaxPoints / kFusedThreads;
+
+struct BatchInst {
+    int N, D, M, H, n, n_max, W, kind, tournament, mutate, T;
+    float sbx_eta0, sbx_eta1, sbx_prob, sbx_copy, pm_eta0, pm_eta1, pm_prob;
+    uint64_t seed;        // draws of mating and variation
+    uint64_t nich_seed;   // niching tie-break hash
+    const float* varsP; const float* objsP; const float* cvP; const int* rankP;
+    float* varsO; float* objsO; float* cvO;
+    float* varsX; float* objsX; float* cvX; int* rankX;
+    const float* bounds; int* pidx; int* d_gen; float* ideal;
+    uint64_t* key0; uint64_t* key64; int* perm; int* vals; float* sorted_f; int* qinfo;
+    int* blocker; int* front_sorted; int* front_list; int* counters;
+    uint32_t* rows; uint32_t* chunk_keys; uint32_t* chunk_bits;
+    int* fronts; int* nds_gidx; int* sizes; float* nds_objs; float* rcp_b; int* extreme;
+    int* assoc_idx; float* assoc_dist; int* rho; int* selected; int* flags; int* survivors;
+    unsigned long long* offset;
+    const float* t_dirs_orig;  // (M, H) directions in their own order
+    const float* t_dirs; const int* t_order; const float* t_center; const float* t_cos;
+    const float* t_sin; const int2* t_link; int t_nodes; float t_delta;
+};
+
+// Launch plan of one M value: instance ids and the prefix of their tile blocks.
+struct FusedBucket {
+    int M = 0, count = 0, max_n = 0, tile_blocks = 0;
+    int* d_ids = nullptr;          // (count) instance indices
+    int* d_tile_prefix = nullptr;  // (count + 1) first tile block of each instance
+};
+
+// A group of instances that runs the fused chain of kernels on one stream:
+// its instance ids, size bounds and per-M buckets.
+struct FusedGroup {
+    int count = 0, max_n = 0, max_N = 0, max_D = 0, max_M = 0;
+    int* d_ids = nullptr;                // (count) instance indices
+    std::vector<FusedBucket> buckets;    // per objective count
+};
+
+int fused_reproduce(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s);
+int fused_evaluate(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s);
+int fused_ndsort(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s);
+int fused_select(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s);
+int fused_tile_blocks(int M, int n);  // tile CTAs of one instance
+// Kernel attributes (shared memory opt-in) of the fused stages, set once per
+// device before any capture.
+int fused_ndsort_configure();
+int fused_select_configure();
+
 }  // namespace moea
 
 struct moea_workspace {

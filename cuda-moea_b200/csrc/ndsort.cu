@@ -157,12 +157,10 @@ __device__ __forceinline__ uint32_t dom_key(float f)
 // boundary all lie inside the prefix, whatever their order.  Positions >= n
 // get the NaN key.  One warp per (word, objective): bitonic sort of
 // (key, lane) pairs, then an inclusive OR-scan of the lane bits.
-__global__ void nds_chunks(const float* __restrict__ sf, int sf_stride, int n, int W, int MF,
-                           uint32_t* __restrict__ ckeys, uint32_t* __restrict__ cbits)
+__device__ __forceinline__ void chunk_warp(int gw, int lane, const float* __restrict__ sf, int sf_stride,
+                                           int n, int W, uint32_t* __restrict__ ckeys,
+                                           uint32_t* __restrict__ cbits)
 {
-    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (gw >= W * MF) return;
     const int m = gw / W, w = gw - m * W;
     const int p = w * 32 + lane;
     const uint32_t key = (p < n) ? dom_key(sf[(size_t)m * sf_stride + p]) : 0xFFFFFFFFu;
@@ -188,6 +186,14 @@ __global__ void nds_chunks(const float* __restrict__ sf, int sf_stride, int n, i
     if (lane == 0) b[0] = 0u;
 }
 
+__global__ void nds_chunks(const float* __restrict__ sf, int sf_stride, int n, int W, int MF,
+                           uint32_t* __restrict__ ckeys, uint32_t* __restrict__ cbits)
+{
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (gw >= W * MF) return;
+    chunk_warp(gw, threadIdx.x & 31, sf, sf_stride, n, W, ckeys, cbits);
+}
+
 // Dominator words per tile CTA (32 positions each), sized so that the staged
 // word tables and the transposed output fit in 48 KB of shared memory.
 template <int M>
@@ -208,19 +214,20 @@ struct TileCfg {
 // dominator position seen, so that after the kernel blocker[q] == -1 exactly
 // for the points that nothing dominates (front 0).
 template <int M>
-__global__ void __launch_bounds__(kTileThreads)
-nds_tiles(const float* __restrict__ sf, int sf_stride, const int* __restrict__ qinfo,
-          const uint32_t* __restrict__ ckeys, const uint32_t* __restrict__ cbits, int n, int W,
-          int Wc, uint32_t* __restrict__ rows, int* __restrict__ blocker)
+__device__ __forceinline__ void tile_block(int bx, int by, const float* __restrict__ sf, int sf_stride,
+                                           const int* __restrict__ qinfo,
+                                           const uint32_t* __restrict__ ckeys,
+                                           const uint32_t* __restrict__ cbits, int n, int W, int Wc,
+                                           uint32_t* __restrict__ rows, int* __restrict__ blocker)
 {
     constexpr int PW = TileCfg<M>::kPW;
     constexpr int MF = TileCfg<M>::kMF;
-    const int q0 = blockIdx.y * kQB;
+    const int q0 = by * kQB;
     if (q0 >= n) return;
     const int qend = min(q0 + kQB, n);
     // dominators of the block lie at positions < qend - 1
     const int nwords = (qend - 1 + 31) >> 5;
-    const int w0 = blockIdx.x * PW;
+    const int w0 = bx * PW;
     if (w0 >= nwords) return;
     const int wcount = min(PW, nwords - w0);
 
@@ -299,6 +306,15 @@ nds_tiles(const float* __restrict__ sf, int sf_stride, const int* __restrict__ q
     }
 }
 
+template <int M>
+__global__ void __launch_bounds__(kTileThreads)
+nds_tiles(const float* __restrict__ sf, int sf_stride, const int* __restrict__ qinfo,
+          const uint32_t* __restrict__ ckeys, const uint32_t* __restrict__ cbits, int n, int W,
+          int Wc, uint32_t* __restrict__ rows, int* __restrict__ blocker)
+{
+    tile_block<M>(blockIdx.x, blockIdx.y, sf, sf_stride, qinfo, ckeys, cbits, n, W, Wc, rows, blocker);
+}
+
 // ---------------------------------------------------------------------------
 // 3. front peeling
 // ---------------------------------------------------------------------------
@@ -354,12 +370,18 @@ __device__ bool grid_barrier(int* counters, unsigned nblocks)
     return s_ok != 0;
 }
 
-__global__ void __launch_bounds__(kPeelThreads)
-nds_peel(const uint32_t* __restrict__ rows, int W, int n, int target, const int* __restrict__ qinfo,
-         int* __restrict__ blocker, int* __restrict__ front_sorted, int* __restrict__ list,
-         int* counters)
+// Body of the peel, run by CTA `block` of `nblocks` co-resident CTAs; U is the
+// CTA's bitmask of unassigned positions (W words of shared memory).  blocker
+// may point to global or to shared memory.  kInflight groups of 32 points are
+// examined per round by one warp: their blockers and probe words are loaded
+// before any of them is examined.
+template <int kInflight>
+__device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
+                                          const uint32_t* __restrict__ rows, int W, int n, int target,
+                                          const int* __restrict__ qinfo, int* __restrict__ blocker,
+                                          int* __restrict__ front_sorted, int* __restrict__ list,
+                                          int* counters)
 {
-    extern __shared__ uint32_t U[];  // unassigned positions, one bit each
     __shared__ int s_len;
     for (int w = threadIdx.x; w < W; w += blockDim.x) {
         const int lo = w * 32;
@@ -367,88 +389,115 @@ nds_peel(const uint32_t* __restrict__ rows, int W, int n, int target, const int*
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
-    const int gwarp = blockIdx.x * wpb + warp;
-    const int twarps = gridDim.x * wpb;
+    const int gwarp = block * wpb + warp;
+    const int twarps = nblocks * wpb;
     const int ngroups = (n + 31) >> 5;
     int len_prev = 0, total = 0, k = 0;
     __syncthreads();
 
     for (;;) {
-        for (int g = gwarp; g < ngroups; g += twarps) {
-            const int q = g * 32 + lane;
-            const bool alive = q < n && ((U[q >> 5] >> (q & 31)) & 1u);
-            // blocker[q] is an unassigned dominator of q, or -1 when nothing dominates q
-            bool is_free = false, need = false;
-            int start_w = -1;
-            if (alive) {
-                const int b = blocker[q];
-                if (b < 0) {
-                    is_free = true;
-                } else if (!((U[b >> 5] >> (b & 31)) & 1u)) {
-                    // blocker assigned: probe its word and the one below; bits
-                    // above it were already free of unassigned dominators
-                    const uint32_t* row = rows + (size_t)q * W;
-                    int w = b >> 5;
-                    uint32_t bits = __ldg(row + w) & U[w];
-                    if (!bits && w > 0) {
-                        --w;
-                        bits = __ldg(row + w) & U[w];
-                    }
-                    if (bits) {
-                        blocker[q] = w * 32 + (31 - __clz(bits));
-                    } else if (w == 0) {
-                        is_free = true;
-                    } else {
-                        need = true;
-                        start_w = w - 1;
-                    }
+        for (int g0 = gwarp; g0 < ngroups; g0 += twarps * kInflight) {
+            int qv[kInflight], bv[kInflight];
+            uint32_t hiw[kInflight], low[kInflight];
+            bool alive[kInflight], probe[kInflight];
+#pragma unroll
+            for (int u = 0; u < kInflight; ++u) {
+                const int g = g0 + u * twarps;
+                const int q = g * 32 + lane;
+                qv[u] = q;
+                alive[u] = g < ngroups && q < n && ((U[q >> 5] >> (q & 31)) & 1u);
+                // blocker[q] is an unassigned dominator of q, or -1 when nothing dominates q
+                bv[u] = alive[u] ? blocker[q] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < kInflight; ++u) {
+                const int b = bv[u];
+                // blocker assigned: probe its word and the one below; bits
+                // above it were already free of unassigned dominators
+                probe[u] = alive[u] && b >= 0 && !((U[b >> 5] >> (b & 31)) & 1u);
+                hiw[u] = 0u;
+                low[u] = 0u;
+                if (probe[u]) {
+                    const uint32_t* row = rows + (size_t)qv[u] * W;
+                    const int w = b >> 5;
+                    hiw[u] = __ldg(row + w);
+                    if (w > 0) low[u] = __ldg(row + w - 1);
                 }
             }
-            // rows not resolved by the probe: the whole warp scans each of
-            // them downwards, 8 coalesced words per lane in flight
-            unsigned needm = __ballot_sync(0xFFFFFFFFu, need);
-            while (needm) {
-                const int L = __ffs(needm) - 1;
-                needm &= needm - 1;
-                const int qL = g * 32 + L;
-                const uint32_t* row = rows + (size_t)qL * W;
-                const int sw = __shfl_sync(0xFFFFFFFFu, start_w, L);
-                int found = -1;
-                for (int w0 = sw; w0 >= 0 && found < 0; w0 -= 256) {
-                    uint32_t acc[8];
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const int w = w0 - lane - 32 * i;
-                        acc[i] = (w >= 0) ? (__ldg(row + w) & U[w]) : 0u;
-                    }
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const unsigned nz = __ballot_sync(0xFFFFFFFFu, acc[i] != 0u);
-                        if (nz) {
-                            const int src = __ffs(nz) - 1;
-                            const uint32_t bb = __shfl_sync(0xFFFFFFFFu, acc[i], src);
-                            found = (w0 - src - 32 * i) * 32 + (31 - __clz(bb));
-                            break;
+            for (int u = 0; u < kInflight; ++u) {
+                const int g = g0 + u * twarps;
+                if (g >= ngroups) break;  // warp-uniform
+                const int q = qv[u];
+                bool is_free = false, need = false;
+                int start_w = -1;
+                if (alive[u]) {
+                    const int b = bv[u];
+                    if (b < 0) {
+                        is_free = true;
+                    } else if (probe[u]) {
+                        int w = b >> 5;
+                        uint32_t bits = hiw[u] & U[w];
+                        if (!bits && w > 0) {
+                            --w;
+                            bits = low[u] & U[w];
+                        }
+                        if (bits) {
+                            blocker[q] = w * 32 + (31 - __clz(bits));
+                        } else if (w == 0) {
+                            is_free = true;
+                        } else {
+                            need = true;
+                            start_w = w - 1;
                         }
                     }
                 }
-                if (lane == L) {
-                    if (found >= 0) blocker[q] = found;
-                    else is_free = true;
+                // rows not resolved by the probe: the whole warp scans each of
+                // them downwards, 8 coalesced words per lane in flight
+                unsigned needm = __ballot_sync(0xFFFFFFFFu, need);
+                while (needm) {
+                    const int L = __ffs(needm) - 1;
+                    needm &= needm - 1;
+                    const int qL = g * 32 + L;
+                    const uint32_t* row = rows + (size_t)qL * W;
+                    const int sw = __shfl_sync(0xFFFFFFFFu, start_w, L);
+                    int found = -1;
+                    for (int w0 = sw; w0 >= 0 && found < 0; w0 -= 256) {
+                        uint32_t acc[8];
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            const int w = w0 - lane - 32 * i;
+                            acc[i] = (w >= 0) ? (__ldg(row + w) & U[w]) : 0u;
+                        }
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            const unsigned nz = __ballot_sync(0xFFFFFFFFu, acc[i] != 0u);
+                            if (nz) {
+                                const int src = __ffs(nz) - 1;
+                                const uint32_t bb = __shfl_sync(0xFFFFFFFFu, acc[i], src);
+                                found = (w0 - src - 32 * i) * 32 + (31 - __clz(bb));
+                                break;
+                            }
+                        }
+                    }
+                    if (lane == L) {
+                        if (found >= 0) blocker[q] = found;
+                        else is_free = true;
+                    }
                 }
-            }
-            const unsigned fm = __ballot_sync(0xFFFFFFFFu, is_free);
-            if (fm) {
-                int base = 0;
-                if (lane == 0) base = atomicAdd(counters + 1, __popc(fm));
-                base = __shfl_sync(0xFFFFFFFFu, base, 0);
-                if (is_free) {
-                    list[base + __popc(fm & ((1u << lane) - 1u))] = q;
-                    front_sorted[q] = k;
+                const unsigned fm = __ballot_sync(0xFFFFFFFFu, is_free);
+                if (fm) {
+                    int base = 0;
+                    if (lane == 0) base = atomicAdd(counters + 1, __popc(fm));
+                    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                    if (is_free) {
+                        list[base + __popc(fm & ((1u << lane) - 1u))] = q;
+                        front_sorted[q] = k;
+                    }
                 }
             }
         }
-        if (!grid_barrier(counters, gridDim.x)) return;
+        if (!grid_barrier(counters, (unsigned)nblocks)) return;
         if (threadIdx.x == 0) s_len = *((volatile int*)counters + 9);
         __syncthreads();
         const int len = s_len;
@@ -461,7 +510,7 @@ nds_peel(const uint32_t* __restrict__ rows, int W, int n, int target, const int*
         total += ck;
         len_prev = len;
         if (total >= target || ck == 0) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) {
+            if (block == 0 && threadIdx.x == 0) {
                 counters[2] = k;
                 counters[3] = total;
                 if (ck == 0 && total < target) atomicExch(counters + 6, kDevPeelInconsistent);
@@ -470,6 +519,15 @@ nds_peel(const uint32_t* __restrict__ rows, int W, int n, int target, const int*
         }
         ++k;
     }
+}
+
+__global__ void __launch_bounds__(kPeelThreads, 1)
+nds_peel(const uint32_t* __restrict__ rows, int W, int n, int target, const int* __restrict__ qinfo,
+         int* __restrict__ blocker, int* __restrict__ front_sorted, int* __restrict__ list,
+         int* counters)
+{
+    extern __shared__ uint32_t U[];  // unassigned positions, one bit each
+    peel_body<1>(blockIdx.x, gridDim.x, U, rows, W, n, target, qinfo, blocker, front_sorted, list, counters);
 }
 
 __global__ void nds_scatter_fronts(int n, const int* __restrict__ perm,
@@ -499,6 +557,328 @@ void launch_tiles(const Workspace& ws, int n, cudaStream_t stream)
     nds_tiles<M><<<grid, kTileThreads, 0, stream>>>(ws.sorted_f, ws.n_max, ws.qinfo, ws.chunk_keys,
                                                      ws.chunk_bits, n, ws.words, maxw, ws.rows,
                                                      ws.blocker);
+}
+
+// ---------------------------------------------------------------------------
+// fused batch: one launch per stage for every instance (n = 2N <= 8192)
+// ---------------------------------------------------------------------------
+
+using FusedSort32 = cub::BlockRadixSort<uint32_t, kFusedThreads, kFusedItems, int>;
+using FusedSort64 = cub::BlockRadixSort<uint64_t, kFusedThreads, kFusedItems, int>;
+using FusedScan = cub::BlockScan<int, kFusedThreads>;
+union FusedSortStorage {
+    typename FusedSort32::TempStorage s32;
+    typename FusedSort64::TempStorage s64;
+    typename FusedScan::TempStorage scan;
+};
+
+// Classification, lexicographic order, sorted objectives, dup positions and
+// peel state of one instance per CTA: the stages of run_ndsort up to the
+// dominance rows, with the same stable LSD passes (objectives M-1..1, then
+// class and f0) done by block radix sorts.  Items beyond n carry keys above
+// every real key and stay behind the real ones.
+__global__ void __launch_bounds__(kFusedThreads)
+fused_lexsort(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    extern __shared__ __align__(16) unsigned char fused_smem[];
+    FusedSortStorage& tmp = *reinterpret_cast<FusedSortStorage*>(fused_smem);
+    __shared__ int s_feas;
+    const BatchInst& I = insts[ids[blockIdx.x]];
+    const SplitPop pop{I.objsP, I.objsO, I.cvP, I.cvO, I.N, I.N, I.N, I.n};
+    const int n = I.n, M = I.M, t = threadIdx.x;
+    if (t == 0) s_feas = 0;
+    __syncthreads();
+    int feas = 0;
+    for (int i = t; i < n; i += kFusedThreads) {
+        const float cv = pop.cvv(i);
+        uint32_t cls, val = 0;
+        if (cv == 0.0f) {
+            bool nan = false;
+            for (int m = 0; m < M; ++m) nan |= isnan(pop.obj(m, i));
+            cls = nan ? 1u : 0u;
+            if (!nan) val = float_order_key(pop.obj(0, i));
+        } else {
+            cls = isnan(cv) ? 3u : 2u;
+            if (cls == 2u) val = float_order_key(cv);
+        }
+        I.key0[i] = ((uint64_t)cls << 32) | val;
+        feas += cls <= 1u;
+    }
+    atomicAdd(&s_feas, feas);
+    __syncthreads();
+    int vals[kFusedItems];
+#pragma unroll
+    for (int j = 0; j < kFusedItems; ++j) vals[j] = t * kFusedItems + j;
+    for (int m = M - 1; m >= 1; --m) {
+        uint32_t keys[kFusedItems];
+#pragma unroll
+        for (int j = 0; j < kFusedItems; ++j) {
+            const int pt = vals[j];
+            keys[j] = (pt < n) ? (((I.key0[pt] >> 32) == 0) ? float_order_key(pop.obj(m, pt)) : 0u)
+                               : 0xFFFFFFFFu;
+        }
+        FusedSort32(tmp.s32).Sort(keys, vals);
+        __syncthreads();
+    }
+    {
+        uint64_t keys[kFusedItems];
+#pragma unroll
+        for (int j = 0; j < kFusedItems; ++j) keys[j] = (vals[j] < n) ? I.key0[vals[j]] : 0x3FFFFFFFFull;
+        FusedSort64(tmp.s64).Sort(keys, vals, 0, 34);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < kFusedItems; ++j) {
+        const int pos = t * kFusedItems + j;
+        if (pos < n) I.perm[pos] = vals[j];
+    }
+    __syncthreads();
+    int heads[kFusedItems];
+#pragma unroll
+    for (int j = 0; j < kFusedItems; ++j) {
+        const int pos = t * kFusedItems + j;
+        heads[j] = 0;
+        if (pos >= n) continue;
+        const int pt = vals[j];
+        const uint64_t k0 = I.key0[pt];
+        const uint32_t cls = (uint32_t)(k0 >> 32);
+        for (int m = 1; m < M; ++m) I.sorted_f[(size_t)(m - 1) * I.n_max + pos] = pop.obj(m, pt);
+        bool is_head = true;
+        if (pos > 0) {
+            const int pp = I.perm[pos - 1];
+            if (I.key0[pp] == k0) {
+                if (cls == 0u) {
+                    bool same = true;
+                    for (int m = 1; m < M; ++m)
+                        same &= float_order_key(pop.obj(m, pt)) == float_order_key(pop.obj(m, pp));
+                    is_head = !same;
+                } else {
+                    is_head = false;
+                }
+            }
+        }
+        heads[j] = is_head ? pos : 0;
+    }
+    FusedScan(tmp.scan).InclusiveScan(heads, heads, cub::Max());
+    __syncthreads();
+    const int feasible = s_feas;
+#pragma unroll
+    for (int j = 0; j < kFusedItems; ++j) {
+        const int pos = t * kFusedItems + j;
+        if (pos >= n) continue;
+        const uint32_t cls = (uint32_t)(I.key0[vals[j]] >> 32);
+        uint32_t d;
+        switch (cls) {
+        case 0u: d = (uint32_t)heads[j]; break;
+        case 1u: d = 0u; break;
+        case 2u: d = (uint32_t)heads[j] | kInfeasibleBit; break;
+        default: d = (uint32_t)feasible | kInfeasibleBit; break;
+        }
+        I.qinfo[pos] = (int)d;
+        I.blocker[pos] = -1;
+        I.front_sorted[pos] = -1;
+    }
+    if (t == 0) {
+        I.counters[0] = feasible;
+        for (int c = 1; c <= 4; ++c) I.counters[c] = 0;
+    }
+}
+
+__global__ void fused_chunks(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    const BatchInst& I = insts[ids[blockIdx.y]];
+    const int W = (I.n + 31) >> 5;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (gw >= W * (I.M - 1)) return;
+    chunk_warp(gw, threadIdx.x & 31, I.sorted_f, I.n_max, I.n, W, I.chunk_keys, I.chunk_bits);
+}
+
+// Tile CTAs of all instances with M objectives, flattened: CTA b belongs to
+// the instance whose range [prefix[k], prefix[k+1]) contains b.
+template <int M>
+__global__ void __launch_bounds__(kTileThreads)
+fused_tiles(const BatchInst* __restrict__ insts, const int* __restrict__ ids,
+            const int* __restrict__ prefix, int count)
+{
+    const int b = blockIdx.x;
+    int lo = 0, hi = count;  // largest k with prefix[k] <= b
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(prefix + mid) <= b) lo = mid; else hi = mid;
+    }
+    const BatchInst& I = insts[__ldg(ids + lo)];
+    const int maxw = (I.n + 31) >> 5;
+    const int gx = (maxw + TileCfg<M>::kPW - 1) / TileCfg<M>::kPW;
+    const int lb = b - __ldg(prefix + lo);
+    tile_block<M>(lb % gx, lb / gx, I.sorted_f, I.n_max, I.qinfo, I.chunk_keys, I.chunk_bits, I.n, I.W, maxw,
+                  I.rows, I.blocker);
+}
+
+constexpr int kFusedPeelThreads = 1024;
+
+// Peel of one instance per CTA with the blockers, the front list and a queue
+// of woken points in shared memory.  Once front k is known and removed from
+// the unassigned set U, one parallel pass over the blockers queues the
+// points whose blocker was in front k; each queued point (one lane each)
+// probes its row from the former blocker's word downwards (bits above it stay
+// free of unassigned dominators) and either records the next unassigned
+// dominator found as its blocker or, having none, joins front k + 1.  A front
+// costs three block barriers and one or two memory latencies.  Shared memory:
+// U (W words), blocker, list and queue (n ints each).
+__global__ void __launch_bounds__(kFusedPeelThreads, 1)
+fused_peel(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    extern __shared__ __align__(16) uint32_t fp_smem[];
+    __shared__ int s_cnt, s_qn;
+    const BatchInst& I = insts[ids[blockIdx.x]];
+    const int n = I.n, W = I.W, target = I.N;
+    uint32_t* U = fp_smem;
+    int* blk = reinterpret_cast<int*>(fp_smem + W);
+    int* list = blk + n;
+    int* queue = list + n;
+    const uint32_t* rows = I.rows;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nwarps = blockDim.x >> 5;
+
+    for (int w = t; w < W; w += blockDim.x) {
+        const int lo = w * 32;
+        U[w] = (lo + 32 <= n) ? 0xFFFFFFFFu : (lo >= n ? 0u : ((1u << (n - lo)) - 1u));
+    }
+    if (t == 0) s_cnt = 0;
+    __syncthreads();
+    for (int q = t; q < n; q += blockDim.x) {
+        const int b = I.blocker[q];
+        blk[q] = b;
+        if (b < 0) {
+            list[atomicAdd(&s_cnt, 1)] = q;
+            I.front_sorted[q] = 0;
+        }
+    }
+    __syncthreads();
+    int len_prev = 0, len = s_cnt, total = 0, k = 0;
+    for (;;) {
+        const int ck = len - len_prev;
+        total += ck;
+        if (total >= target || ck == 0) {
+            if (t == 0) {
+                I.counters[1] = len;
+                I.counters[2] = k;
+                I.counters[3] = total;
+                if (ck == 0 && total < target) atomicExch(I.counters + 6, kDevPeelInconsistent);
+            }
+            for (int i = t; i < len; i += blockDim.x) I.front_list[i] = list[i];
+            return;
+        }
+        if (t == 0) s_qn = 0;
+        for (int i = t; i < ck; i += blockDim.x) {
+            const int p = list[len_prev + i];
+            atomicAnd(U + (p >> 5), ~(1u << (p & 31)));
+        }
+        __syncthreads();
+        // points still unassigned whose blocker has just been assigned
+        for (int q = t; q < n; q += blockDim.x) {
+            const int b = blk[q];
+            if (b >= 0 && ((U[q >> 5] >> (q & 31)) & 1u) && !((U[b >> 5] >> (b & 31)) & 1u))
+                queue[atomicAdd(&s_qn, 1)] = q;
+        }
+        __syncthreads();
+        const int qn = s_qn;
+        // entries interleaved over the warps: a short queue uses every warp
+        for (int r = 0; r * 32 * nwarps < qn; ++r) {
+            const int e = warp + nwarps * (r * 32 + lane);
+            const bool act = e < qn;
+            const int q = act ? queue[e] : 0;
+            bool is_free = false, need = false;
+            int start_w = -1;
+            if (act) {
+                const uint32_t* row = rows + (size_t)q * W;
+                int w = blk[q] >> 5;
+                const uint32_t hiw = __ldg(row + w);
+                const uint32_t low = (w > 0) ? __ldg(row + w - 1) : 0u;
+                uint32_t bits = hiw & U[w];
+                if (!bits && w > 0) {
+                    --w;
+                    bits = low & U[w];
+                }
+                if (bits) {
+                    blk[q] = w * 32 + (31 - __clz(bits));
+                } else if (w == 0) {
+                    is_free = true;
+                } else {
+                    need = true;
+                    start_w = w - 1;
+                }
+            }
+            // rows not resolved by the probe: the whole warp scans each of
+            // them downwards over the words that still hold unassigned points
+            unsigned needm = __ballot_sync(0xFFFFFFFFu, need);
+            while (needm) {
+                const int L = __ffs(needm) - 1;
+                needm &= needm - 1;
+                const int qL = __shfl_sync(0xFFFFFFFFu, q, L);
+                const uint32_t* row = rows + (size_t)qL * W;
+                const int sw = __shfl_sync(0xFFFFFFFFu, start_w, L);
+                int found = -1;
+                for (int w0 = sw; w0 >= 0 && found < 0; w0 -= 256) {
+                    uint32_t acc[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const int w = w0 - lane - 32 * i;
+                        const uint32_t u = (w >= 0) ? U[w] : 0u;
+                        acc[i] = u ? (__ldg(row + w) & u) : 0u;
+                    }
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const unsigned nz = __ballot_sync(0xFFFFFFFFu, acc[i] != 0u);
+                        if (nz) {
+                            const int src = __ffs(nz) - 1;
+                            const uint32_t bb = __shfl_sync(0xFFFFFFFFu, acc[i], src);
+                            found = (w0 - src - 32 * i) * 32 + (31 - __clz(bb));
+                            break;
+                        }
+                    }
+                }
+                if (lane == L) {
+                    if (found >= 0) blk[q] = found;
+                    else is_free = true;
+                }
+            }
+            const unsigned fm = __ballot_sync(0xFFFFFFFFu, is_free);
+            if (fm) {
+                int slot = 0;
+                if (lane == 0) slot = atomicAdd(&s_cnt, __popc(fm));
+                slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+                if (is_free) {
+                    list[slot + __popc(fm & ((1u << lane) - 1u))] = q;
+                    blk[q] = -1;
+                    I.front_sorted[q] = k + 1;
+                }
+            }
+        }
+        __syncthreads();
+        len_prev = len;
+        len = s_cnt;
+        ++k;
+    }
+}
+
+__global__ void fused_scatter(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    const BatchInst& I = insts[ids[blockIdx.y]];
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos < I.n) I.fronts[I.perm[pos]] = I.front_sorted[pos];
+}
+
+template <int M>
+int tile_blocks_of(int n)
+{
+    const int maxw = ceil_div(n, 32);
+    return ceil_div(maxw, TileCfg<M>::kPW) * ceil_div(n, kQB);
+}
+
+template <int M>
+void launch_fused_tiles(const BatchInst* d_inst, const FusedBucket& b, cudaStream_t s)
+{
+    fused_tiles<M><<<b.tile_blocks, kTileThreads, 0, s>>>(d_inst, b.d_ids, b.d_tile_prefix, b.count);
 }
 
 }  // namespace
@@ -638,6 +1018,57 @@ int configure_peel(Workspace& ws)
         return set_error(MOEA_ERR_UNSUPPORTED, "peel kernel does not fit on an SM (smem %zu)", smem);
     ws.peel_grid = sms * (per_sm > 2 ? 2 : per_sm);
     ws.peel_smem = (int)smem;
+    return MOEA_OK;
+}
+
+int fused_tile_blocks(int M, int n)
+{
+    switch (M) {
+#define MOEA_TB_CASE(K) case K: return tile_blocks_of<K>(n);
+    MOEA_TB_CASE(1) MOEA_TB_CASE(2) MOEA_TB_CASE(3) MOEA_TB_CASE(4)
+    MOEA_TB_CASE(5) MOEA_TB_CASE(6) MOEA_TB_CASE(7) MOEA_TB_CASE(8)
+    MOEA_TB_CASE(9) MOEA_TB_CASE(10) MOEA_TB_CASE(11) MOEA_TB_CASE(12)
+    MOEA_TB_CASE(13) MOEA_TB_CASE(14) MOEA_TB_CASE(15) MOEA_TB_CASE(16)
+#undef MOEA_TB_CASE
+    default: return 0;
+    }
+}
+
+size_t fused_peel_smem(int n) { return (size_t)ceil_div(n, 32) * sizeof(uint32_t) + 3 * (size_t)n * sizeof(int); }
+
+int fused_ndsort_configure()
+{
+    MOEA_CUDA_TRY(cudaFuncSetAttribute(fused_lexsort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(FusedSortStorage)));
+    MOEA_CUDA_TRY(cudaFuncSetAttribute(fused_peel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)fused_peel_smem(kFusedMaxPoints)));
+    return MOEA_OK;
+}
+
+int fused_ndsort(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s)
+{
+    const int sort_smem = (int)sizeof(FusedSortStorage);
+    fused_lexsort<<<g.count, kFusedThreads, sort_smem, s>>>(d_inst, g.d_ids);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    if (g.max_M > 1) {
+        const int warps = ceil_div(g.max_n, 32) * (g.max_M - 1);
+        fused_chunks<<<dim3(ceil_div(warps, 8), g.count), 256, 0, s>>>(d_inst, g.d_ids);
+    }
+    for (const FusedBucket& b : g.buckets) {
+        switch (b.M) {
+#define MOEA_FT_CASE(K) case K: launch_fused_tiles<K>(d_inst, b, s); break;
+        MOEA_FT_CASE(1) MOEA_FT_CASE(2) MOEA_FT_CASE(3) MOEA_FT_CASE(4)
+        MOEA_FT_CASE(5) MOEA_FT_CASE(6) MOEA_FT_CASE(7) MOEA_FT_CASE(8)
+        MOEA_FT_CASE(9) MOEA_FT_CASE(10) MOEA_FT_CASE(11) MOEA_FT_CASE(12)
+        MOEA_FT_CASE(13) MOEA_FT_CASE(14) MOEA_FT_CASE(15) MOEA_FT_CASE(16)
+#undef MOEA_FT_CASE
+        default: return set_error(MOEA_ERR_UNSUPPORTED, "fused ndsort: M=%d", b.M);
+        }
+    }
+    MOEA_CUDA_TRY(cudaGetLastError());
+    fused_peel<<<g.count, kFusedPeelThreads, fused_peel_smem(g.max_n), s>>>(d_inst, g.d_ids);
+    fused_scatter<<<dim3(ceil_div(g.max_n, 256), g.count), 256, 0, s>>>(d_inst, g.d_ids);
+    MOEA_CUDA_TRY(cudaGetLastError());
     return MOEA_OK;
 }
 

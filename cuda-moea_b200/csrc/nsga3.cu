@@ -11,6 +11,7 @@
 // whole generation runs without a host round trip.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -234,38 +235,17 @@ __device__ __forceinline__ double warp_sum_d(double v)
 // ill-conditioning tests and row-maximum fallback
 // (normalization.cu:739-856, 1302-1394).  Run by one block of 256 threads.
 template <int M>
-__global__ void __launch_bounds__(kNormThreads)
-norm_finalize(const float* __restrict__ nds, int nds_stride, const float* __restrict__ part_val,
-              const int* __restrict__ part_idx, const float* __restrict__ part_max, int nblocks,
-              float* __restrict__ rcp_out, int* __restrict__ extreme_out, int* __restrict__ ill_out)
+__device__ __forceinline__ void norm_solve(const float* __restrict__ nds, int nds_stride,
+                                           const int* s_ext, const float* s_max,
+                                           float* __restrict__ rcp_out, int* __restrict__ extreme_out,
+                                           int* __restrict__ ill_out)
 {
-    __shared__ int s_ext[M];
-    __shared__ float s_max[M];
     __shared__ double sA[M][M];
     __shared__ double sV[M][M];
     __shared__ double s_sigma[M];
     __shared__ int s_bad;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_bad = 0;
-    for (int j = warp; j < M; j += kNormThreads / 32) {
-        float a = INFINITY;
-        int ai = -1;
-        float mx = -INFINITY;
-        for (int b = lane; b < nblocks; b += 32) {
-            float v = part_val[b * M + j];
-            v = isnan(v) ? INFINITY : v;
-            if (asf_better(v, part_idx[b * M + j], a, ai)) { a = v; ai = part_idx[b * M + j]; }
-            mx = fmaxf(mx, part_max[b * M + j]);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const float ov = __shfl_down_sync(0xFFFFFFFFu, a, o);
-            const int oi = __shfl_down_sync(0xFFFFFFFFu, ai, o);
-            if (asf_better(ov, oi, a, ai)) { a = ov; ai = oi; }
-            mx = fmaxf(mx, __shfl_down_sync(0xFFFFFFFFu, mx, o));
-        }
-        if (lane == 0) { s_ext[j] = ai; s_max[j] = mx; }
-    }
     __syncthreads();
     for (int t = threadIdx.x; t < M * M; t += blockDim.x) {
         const int r = t / M, m = t % M;  // row r = extreme point of axis r
@@ -340,6 +320,43 @@ norm_finalize(const float* __restrict__ nds, int nds_stride, const float* __rest
         }
         if (lane == 0 && ill_out) *ill_out = bad;
     }
+}
+
+// Intercepts from the extreme points: one-sided Jacobi SVD in FP64 of the
+// matrix whose row r is extreme point r, pseudo-inverse applied to the ones
+// vector with singular values <= 1e-5 dropped, and the reference's
+// ill-conditioning tests and row-maximum fallback
+// (normalization.cu:739-856, 1302-1394).  Run by one block of 256 threads.
+template <int M>
+__global__ void __launch_bounds__(kNormThreads)
+norm_finalize(const float* __restrict__ nds, int nds_stride, const float* __restrict__ part_val,
+              const int* __restrict__ part_idx, const float* __restrict__ part_max, int nblocks,
+              float* __restrict__ rcp_out, int* __restrict__ extreme_out, int* __restrict__ ill_out)
+{
+    __shared__ int s_ext[M];
+    __shared__ float s_max[M];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int j = warp; j < M; j += kNormThreads / 32) {
+        float a = INFINITY;
+        int ai = -1;
+        float mx = -INFINITY;
+        for (int b = lane; b < nblocks; b += 32) {
+            float v = part_val[b * M + j];
+            v = isnan(v) ? INFINITY : v;
+            if (asf_better(v, part_idx[b * M + j], a, ai)) { a = v; ai = part_idx[b * M + j]; }
+            mx = fmaxf(mx, part_max[b * M + j]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_down_sync(0xFFFFFFFFu, a, o);
+            const int oi = __shfl_down_sync(0xFFFFFFFFu, ai, o);
+            if (asf_better(ov, oi, a, ai)) { a = ov; ai = oi; }
+            mx = fmaxf(mx, __shfl_down_sync(0xFFFFFFFFu, mx, o));
+        }
+        if (lane == 0) { s_ext[j] = ai; s_max[j] = mx; }
+    }
+    __syncthreads();
+    norm_solve<M>(nds, nds_stride, s_ext, s_max, rcp_out, extreme_out, ill_out);
 }
 
 __global__ void norm_scale(float* __restrict__ nds, int stride, const int* __restrict__ d_n, int M,
@@ -440,19 +457,22 @@ __global__ void dir_delta_kernel(const float* __restrict__ refs, int M, int H, f
     }
 }
 
+// One block of points (bx) against one range of directions (by).  With
+// best_out the packed (d2, index) minimum is merged atomically across ranges;
+// without it the block covers every direction and writes idx/dist directly.
 template <int M>
-__global__ void __launch_bounds__(kAssocThreads)
-assoc_plain(const float* __restrict__ x, int x_stride, const float* __restrict__ scale,
-            const float* __restrict__ refs, int H, const int* __restrict__ d_n, int split_len,
-            const float* __restrict__ d_delta, unsigned long long* __restrict__ best_out)
+__device__ __forceinline__ void assoc_scan_block(int bx, int by, const float* __restrict__ x, int x_stride,
+                                                 const float* __restrict__ scale,
+                                                 const float* __restrict__ refs, int H, int n, int split_len,
+                                                 float delta, unsigned long long* __restrict__ best_out,
+                                                 int* __restrict__ idx_out, float* __restrict__ dist_out)
 {
     constexpr int TL = DirTile<M>::kLen;
     __shared__ __align__(16) float s_dir[TL * ((M <= 4) ? 4 : M)];
-    const int n = *d_n;
-    const int i = blockIdx.x * kAssocThreads + threadIdx.x;
-    const int j_begin = blockIdx.y * split_len;
+    const int i = bx * kAssocThreads + threadIdx.x;
+    const int j_begin = by * split_len;
     const int j_end = min(H, j_begin + split_len);
-    if (blockIdx.x * kAssocThreads >= n || j_begin >= j_end) return;
+    if (bx * kAssocThreads >= n || j_begin >= j_end) return;
     const bool valid = i < n;
     float xr[M];
     float xx = 0.0f;
@@ -463,7 +483,7 @@ assoc_plain(const float* __restrict__ x, int x_stride, const float* __restrict__
         xr[m] = v;
         xx = fmaf(v, v, xx);
     }
-    const float margin = assoc_margin(M, xx, *d_delta);
+    const float margin = assoc_margin(M, xx, delta);
     // coarse pre-pass over a strided subset to start with a tight threshold
     float maxd = -INFINITY;
     for (int j = j_begin; j < j_end; j += 61) {
@@ -527,11 +547,27 @@ assoc_plain(const float* __restrict__ x, int x_stride, const float* __restrict__
             }
         }
     }
-    if (valid && best < INFINITY) {
-        const unsigned long long packed =
-            ((unsigned long long)__float_as_uint(best) << 32) | (unsigned)bj;
-        atomicMin(best_out + i, packed);
+    if (best_out) {
+        if (valid && best < INFINITY) {
+            const unsigned long long packed =
+                ((unsigned long long)__float_as_uint(best) << 32) | (unsigned)bj;
+            atomicMin(best_out + i, packed);
+        }
+    } else if (valid) {
+        const bool found = best < INFINITY;
+        idx_out[i] = found ? bj : -1;
+        dist_out[i] = found ? sqrtf(best) : INFINITY;
     }
+}
+
+template <int M>
+__global__ void __launch_bounds__(kAssocThreads)
+assoc_plain(const float* __restrict__ x, int x_stride, const float* __restrict__ scale,
+            const float* __restrict__ refs, int H, const int* __restrict__ d_n, int split_len,
+            const float* __restrict__ d_delta, unsigned long long* __restrict__ best_out)
+{
+    assoc_scan_block<M>(blockIdx.x, blockIdx.y, x, x_stride, scale, refs, H, *d_n, split_len, *d_delta, best_out,
+                        nullptr, nullptr);
 }
 
 __global__ void assoc_reset(unsigned long long* best, int n_cap)
@@ -591,7 +627,10 @@ void launch_assoc(const float* x, int x_stride, const float* scale, const float*
 // by the 2 dc slack) and |r|^2 <= 1 + delta.
 
 constexpr int kTreeWarps = 8;
-constexpr int kTreeMaxDepth = 8;
+constexpr int kTreeMaxDepth = kDirTreeMaxDepth;
+// Above this many objectives the cones prune little and one thread per point
+// over all directions is cheaper than one warp per point over the tree.
+constexpr int kTreeMaxObjectives = 5;
 
 struct TreeArgs {
     const float* dirs;    // (M, H) in tree order
@@ -605,14 +644,15 @@ struct TreeArgs {
 };
 
 template <int M>
-__global__ void __launch_bounds__(kTreeWarps * 32)
-assoc_tree(const float* __restrict__ x, int x_stride, const float* __restrict__ scale, TreeArgs t,
-           const int* __restrict__ d_n, int* __restrict__ idx_out, float* __restrict__ dist_out)
+__device__ __forceinline__ void assoc_tree_block(int block, const float* __restrict__ x, int x_stride,
+                                                 const float* __restrict__ scale, const TreeArgs& t,
+                                                 const int* __restrict__ d_n, int* __restrict__ idx_out,
+                                                 float* __restrict__ dist_out)
 {
     __shared__ float s_bound[kTreeWarps][kTreeMaxDepth][32];
     __shared__ float s_proj[kTreeWarps][kTreeMaxDepth][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * kTreeWarps + warp;
+    const int i = block * kTreeWarps + warp;
     if (i >= *d_n) return;
     float xr[M];
     float xx = 0.0f;
@@ -750,6 +790,14 @@ assoc_tree(const float* __restrict__ x, int x_stride, const float* __restrict__ 
     }
 }
 
+template <int M>
+__global__ void __launch_bounds__(kTreeWarps * 32)
+assoc_tree(const float* __restrict__ x, int x_stride, const float* __restrict__ scale, TreeArgs t,
+           const int* __restrict__ d_n, int* __restrict__ idx_out, float* __restrict__ dist_out)
+{
+    assoc_tree_block<M>(blockIdx.x, x, x_stride, scale, t, d_n, idx_out, dist_out);
+}
+
 // ---------------------------------------------------------------------------
 // niching
 // ---------------------------------------------------------------------------
@@ -845,6 +893,296 @@ int sm_count(int device)
     cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, device);
     if (device >= 0 && device < 64) cached[device] = s;
     return s;
+}
+
+// ---------------------------------------------------------------------------
+// fused batch: selection stages of every instance, one launch per stage
+// ---------------------------------------------------------------------------
+
+using FusedSortK64 = cub::BlockRadixSort<uint64_t, kFusedThreads, kFusedItems, int>;
+using FusedScanInt = cub::BlockScan<int, kFusedThreads>;
+union FusedSelStorage {
+    typename FusedSortK64::TempStorage sort;
+    typename FusedScanInt::TempStorage scan;
+};
+
+// Extraction of [prior; last] in ascending index order, running ideal point
+// over the offspring, translation and intercepts of one instance per CTA:
+// run_extract, run_ideal and run_normalize_split of the single-instance path.
+template <int M>
+__global__ void __launch_bounds__(kFusedThreads)
+fused_prep(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    __shared__ typename FusedScanInt::TempStorage scan_tmp;
+    __shared__ float s_red[32];
+    __shared__ float s_val[kFusedThreads / 32][M];
+    __shared__ int s_idx[kFusedThreads / 32][M];
+    __shared__ float s_mx[kFusedThreads / 32][M];
+    __shared__ int s_ext[M];
+    __shared__ float s_max[M];
+    __shared__ int s_tot;
+    const BatchInst& I = insts[ids[blockIdx.x]];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int n = I.n, N = I.N;
+    const SplitPop pop{I.objsP, I.objsO, I.cvP, I.cvO, N, N, N, n};
+
+    // ordered two-class compaction: class 0 = fronts below the last, 1 = the last
+    const int mf = I.counters[2];
+    int cls[kFusedItems];
+    int ca = 0, cb = 0;
+#pragma unroll
+    for (int j = 0; j < kFusedItems; ++j) {
+        const int i = t * kFusedItems + j;
+        int c = -1;
+        if (i < n) {
+            const int f = I.fronts[i];
+            c = (f >= 0 && f < mf) ? 0 : (f == mf ? 1 : -1);
+        }
+        cls[j] = c;
+        ca += c == 0;
+        cb += c == 1;
+    }
+    int packed = ca | (cb << 16), total;
+    FusedScanInt(scan_tmp).ExclusiveSum(packed, packed, total);
+    const int ta = total & 0xFFFF, tb = total >> 16;
+    int pa = packed & 0xFFFF, pb = ta + (packed >> 16);
+#pragma unroll
+    for (int j = 0; j < kFusedItems; ++j) {
+        const int i = t * kFusedItems + j;
+        if (cls[j] == 0) I.nds_gidx[pa++] = i;
+        else if (cls[j] == 1) I.nds_gidx[pb++] = i;
+    }
+    if (t == 0) {
+        I.sizes[0] = ta;
+        I.sizes[1] = tb;
+        I.sizes[2] = N - ta;
+        I.sizes[3] = ta + tb;
+        s_tot = ta + tb;
+    }
+    // ideal point: the reduction order of ideal_kernel (512 threads)
+    for (int m = 0; m < M; ++m) {
+        float v = INFINITY;
+        if (t < 512)
+            for (int i = t; i < N; i += 512) v = fminf(v, I.objsO[(size_t)m * N + i]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_down_sync(0xFFFFFFFFu, v, o));
+        if (lane == 0 && warp < 16) s_red[warp] = v;
+        __syncthreads();
+        if (t == 0) {
+            float r = INFINITY;
+            for (int w = 0; w < 16; ++w) r = fminf(r, s_red[w]);
+            I.ideal[m] = fminf(I.ideal[m], r);
+        }
+        __syncthreads();
+    }
+    // translated nds objectives, ASF argmin per axis, per-objective maximum
+    const int n_nds = s_tot;
+    float ideal[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) ideal[m] = I.ideal[m];
+    float a[M], mx[M];
+    int ai[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) { a[j] = INFINITY; ai[j] = -1; mx[j] = -INFINITY; }
+    for (int i = t; i < n_nds; i += kFusedThreads) {
+        const int g = I.nds_gidx[i];
+        float v[M];
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            float x = pop.obj(m, g) - ideal[m];
+            if (isfinite(x)) x = fmaxf(x, 0.0f);
+            v[m] = x;
+            I.nds_objs[(size_t)m * I.n_max + i] = x;
+        }
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+            float sv = -INFINITY;
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                const float x = isnan(v[m]) ? INFINITY : v[m];
+                sv = fmaxf(sv, x * ((m == j) ? 1.0f : 1e6f));
+            }
+            if (asf_better(sv, i, a[j], ai[j])) { a[j] = sv; ai[j] = i; }
+            mx[j] = fmaxf(mx[j], isnan(v[j]) ? -INFINITY : v[j]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_down_sync(0xFFFFFFFFu, a[j], o);
+            const int oi = __shfl_down_sync(0xFFFFFFFFu, ai[j], o);
+            if (asf_better(ov, oi, a[j], ai[j])) { a[j] = ov; ai[j] = oi; }
+            mx[j] = fmaxf(mx[j], __shfl_down_sync(0xFFFFFFFFu, mx[j], o));
+        }
+        if (lane == 0) { s_val[warp][j] = a[j]; s_idx[warp][j] = ai[j]; s_mx[warp][j] = mx[j]; }
+    }
+    __syncthreads();
+    if (t < M) {
+        float b = INFINITY, bm = -INFINITY;
+        int bi = -1;
+        for (int w = 0; w < kFusedThreads / 32; ++w) {
+            if (asf_better(s_val[w][t], s_idx[w][t], b, bi)) { b = s_val[w][t]; bi = s_idx[w][t]; }
+            bm = fmaxf(bm, s_mx[w][t]);
+        }
+        s_ext[t] = bi;
+        s_max[t] = bm;
+    }
+    __syncthreads();
+    norm_solve<M>(I.nds_objs, I.n_max, s_ext, s_max, I.rcp_b, I.extreme, nullptr);
+}
+
+template <int M>
+__global__ void __launch_bounds__(kAssocThreads)
+fused_scan(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    const BatchInst& I = insts[ids[blockIdx.y]];
+    assoc_scan_block<M>(blockIdx.x, 0, I.nds_objs, I.n_max, I.rcp_b, I.t_dirs_orig, I.H, I.sizes[3], I.H,
+                        I.t_delta, nullptr, I.assoc_idx, I.assoc_dist);
+}
+
+template <int M>
+__global__ void __launch_bounds__(kTreeWarps * 32)
+fused_assoc(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    const BatchInst& I = insts[ids[blockIdx.y]];
+    const TreeArgs t{I.t_dirs, I.t_order, I.t_center, I.t_cos, I.t_sin, I.t_link, I.H, I.t_nodes, I.t_delta};
+    assoc_tree_block<M>(blockIdx.x, I.nds_objs, I.n_max, I.rcp_b, t, I.sizes + 3, I.assoc_idx, I.assoc_dist);
+}
+
+// Run starts of the sorted keys (by direction index, the high word) into
+// rs[] for this thread's items at positions < n; the keys are staged in
+// `stage`, which holds n entries.
+__device__ __forceinline__ void fused_run_starts(const uint64_t (&keys)[kFusedItems], uint64_t* stage, int n,
+                                                 FusedScanInt::TempStorage& tmp, int (&rs)[kFusedItems])
+{
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int j = 0; j < kFusedItems; ++j)
+        if (t * kFusedItems + j < n) stage[t * kFusedItems + j] = keys[j];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kFusedItems; ++j) {
+        const int pos = t * kFusedItems + j;
+        const bool h = pos < n &&
+                       (pos == 0 || (uint32_t)(keys[j] >> 32) != (uint32_t)(stage[pos - 1] >> 32));
+        rs[j] = h ? pos : 0;
+    }
+    FusedScanInt(tmp).InclusiveScan(rs, rs, cub::Max());
+    __syncthreads();
+}
+
+// Niche selection of one instance per CTA: run_niching with block sorts.
+__global__ void __launch_bounds__(kFusedThreads)
+fused_niching(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    extern __shared__ __align__(16) unsigned char fused_smem[];
+    FusedSelStorage& tmp = *reinterpret_cast<FusedSelStorage*>(fused_smem);
+    const BatchInst& I = insts[ids[blockIdx.x]];
+    const int t = threadIdx.x;
+    const int np = I.sizes[0], nl = I.sizes[1], nrem = I.sizes[2], H = I.H;
+    const unsigned long long off = *I.offset;
+    for (int r = t; r < H; r += kFusedThreads) I.rho[r] = 0;
+    __syncthreads();
+    for (int i = t; i < np; i += kFusedThreads) {
+        I.selected[i] = I.nds_gidx[i];
+        const int r = I.assoc_idx[i];
+        if (r >= 0 && r < H) atomicAdd(I.rho + r, 1);
+    }
+    uint64_t keys[kFusedItems];
+    int vals[kFusedItems];
+#pragma unroll
+    for (int j = 0; j < kFusedItems; ++j) {
+        const int p = t * kFusedItems + j;
+        keys[j] = (p < nl) ? (((uint64_t)(uint32_t)I.assoc_idx[np + p] << 32) |
+                              __float_as_uint(I.assoc_dist[np + p]))
+                           : ~0ull;
+        vals[j] = p;
+    }
+    __syncthreads();  // rho complete
+    for (int stage = 1; stage <= 3; ++stage) {
+        FusedSortK64(tmp.sort).Sort(keys, vals);
+        __syncthreads();
+        if (stage == 3) break;
+        int rs[kFusedItems];
+        fused_run_starts(keys, I.key64, I.n, tmp.scan, rs);
+#pragma unroll
+        for (int j = 0; j < kFusedItems; ++j) {
+            const int p = t * kFusedItems + j;
+            if (p >= nl) continue;
+            const uint32_t ref = (uint32_t)(keys[j] >> 32);
+            const int r_i = (int)ref;
+            const int rho_r = (r_i >= 0 && r_i < H) ? I.rho[r_i] : 0;
+            const int rank = p - rs[j];
+            if (stage == 1) {
+                const uint32_t rnd = splitmix_u32(off + (uint64_t)p, I.nich_seed);
+                const uint32_t low = (rho_r == 0 && rank == 0) ? 0u : (rnd | 1u);
+                keys[j] = ((uint64_t)ref << 32) | low;
+            } else {
+                const uint32_t rnd = splitmix_u32(off + (uint64_t)nl + (uint64_t)p, I.nich_seed);
+                keys[j] = ((uint64_t)(uint32_t)(rho_r + rank) << 32) | rnd;
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kFusedItems; ++j) {
+        const int i = t * kFusedItems + j;
+        if (i < nrem && i < nl) I.selected[np + i] = I.nds_gidx[np + vals[j]];
+    }
+    if (t == 0) *I.offset = off + 2ull * (unsigned long long)nl;
+}
+
+// Survivors in ascending mixed index (run_order_selection) of one instance per CTA.
+__global__ void __launch_bounds__(kFusedThreads)
+fused_order(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    __shared__ typename FusedScanInt::TempStorage scan_tmp;
+    __shared__ unsigned char s_flag[kFusedMaxPoints];
+    const BatchInst& I = insts[ids[blockIdx.x]];
+    const int t = threadIdx.x, n = I.n, N = I.N;
+    for (int i = t; i < kFusedMaxPoints; i += kFusedThreads) s_flag[i] = 0;
+    __syncthreads();
+    for (int i = t; i < N; i += kFusedThreads) s_flag[I.selected[i]] = 1;
+    __syncthreads();
+    int c = 0;
+#pragma unroll
+    for (int j = 0; j < kFusedItems; ++j) {
+        const int i = t * kFusedItems + j;
+        c += (i < n && s_flag[i]) ? 1 : 0;
+    }
+    FusedScanInt(scan_tmp).ExclusiveSum(c, c);
+#pragma unroll
+    for (int j = 0; j < kFusedItems; ++j) {
+        const int i = t * kFusedItems + j;
+        if (i < n && s_flag[i]) I.survivors[c++] = i;
+    }
+}
+
+// Next parents from the survivors (gather_next), then the generation counter.
+__global__ void fused_gather(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    const BatchInst& I = insts[ids[blockIdx.y]];
+    const int N = I.N, D = I.D, M = I.M;
+    const SplitPop pop{I.objsP, I.objsO, I.cvP, I.cvO, N, N, N, I.n};
+    const long long total = (long long)N * D;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(e / D), d = (int)(e % D);
+        const int s = I.survivors[r];
+        I.varsX[e] = (s < N) ? I.varsP[(size_t)s * D + d] : I.varsO[(size_t)(s - N) * D + d];
+    }
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
+        const int s = I.survivors[r];
+        for (int m = 0; m < M; ++m) I.objsX[(size_t)m * N + r] = pop.obj(m, s);
+        I.cvX[r] = pop.cvv(s);
+        I.rankX[r] = I.fronts[s];
+    }
+}
+
+__global__ void fused_bump(const BatchInst* __restrict__ insts, const int* __restrict__ ids, int count)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) *insts[ids[k]].d_gen += 1;
 }
 
 }  // namespace
@@ -968,7 +1306,7 @@ int run_associate(Workspace& ws, const float* x, int x_stride, const float* scal
     if (mode == MOEA_ASSOC_TREE) {
         if (!direction_tree_ready(ws, refs, M, H))
             return set_error(MOEA_ERR_STATE, "associate: no cone tree prepared for these directions");
-        if (ws.tree_depth <= kTreeMaxDepth) {
+        if (ws.tree_depth <= kTreeMaxDepth && M <= kTreeMaxObjectives) {
             const TreeArgs t{ws.tree_dirs, ws.tree_order, ws.tree_center, ws.tree_cos, ws.tree_sin,
                              ws.tree_link, H, ws.tree_nodes, ws.tree_delta};
             const int blocks = ceil_div(n_cap, kTreeWarps);
@@ -984,7 +1322,7 @@ int run_associate(Workspace& ws, const float* x, int x_stride, const float* scal
             MOEA_CUDA_TRY(cudaGetLastError());
             return MOEA_OK;
         }
-        // a tree deeper than the kernel's stack: visit every direction instead
+        // a tree deeper than the kernel's stack, or many objectives: scan instead
     }
     dir_delta_kernel<<<1, 1024, 0, stream>>>(refs, M, H, ws.dir_delta);
     assoc_reset<<<ceil_div(n_cap, 256), 256, 0, stream>>>(ws.assoc_best, n_cap);
@@ -1126,6 +1464,47 @@ int run_quantize_cv(const float* cv, float* out, int n, float eps, float clip, f
     const float inv_clip_log = (log_alpha > 0.0f) ? 1.0f / log1pf(log_alpha * clip) : 0.0f;
     cv_quant_kernel<<<ceil_div(n, 256), 256, 0, stream>>>(cv, out, n, eps, clip, inv_clip_log,
                                                           log_alpha, inv_clip, bins);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+int fused_select_configure()
+{
+    MOEA_CUDA_TRY(cudaFuncSetAttribute(fused_niching, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(FusedSelStorage)));
+    return MOEA_OK;
+}
+
+int fused_select(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s)
+{
+    const int sort_smem = (int)sizeof(FusedSelStorage);
+    for (const FusedBucket& b : g.buckets) {
+        switch (b.M) {
+#define MOEA_FP_CASE(K)                                                                              \
+        case K:                                                                                      \
+            fused_prep<K><<<b.count, kFusedThreads, 0, s>>>(d_inst, b.d_ids);                        \
+            if (K <= kTreeMaxObjectives)                                                             \
+                fused_assoc<K><<<dim3(ceil_div(b.max_n, kTreeWarps), b.count), kTreeWarps * 32, 0,    \
+                                 s>>>(d_inst, b.d_ids);                                              \
+            else                                                                                     \
+                fused_scan<K><<<dim3(ceil_div(b.max_n, kAssocThreads), b.count), kAssocThreads, 0,    \
+                                s>>>(d_inst, b.d_ids);                                               \
+            break;
+        MOEA_FP_CASE(1) MOEA_FP_CASE(2) MOEA_FP_CASE(3) MOEA_FP_CASE(4)
+        MOEA_FP_CASE(5) MOEA_FP_CASE(6) MOEA_FP_CASE(7) MOEA_FP_CASE(8)
+        MOEA_FP_CASE(9) MOEA_FP_CASE(10) MOEA_FP_CASE(11) MOEA_FP_CASE(12)
+        MOEA_FP_CASE(13) MOEA_FP_CASE(14) MOEA_FP_CASE(15) MOEA_FP_CASE(16)
+#undef MOEA_FP_CASE
+        default: return set_error(MOEA_ERR_UNSUPPORTED, "fused select: M=%d", b.M);
+        }
+    }
+    MOEA_CUDA_TRY(cudaGetLastError());
+    fused_niching<<<g.count, kFusedThreads, sort_smem, s>>>(d_inst, g.d_ids);
+    fused_order<<<g.count, kFusedThreads, 0, s>>>(d_inst, g.d_ids);
+    const long long per = (long long)g.max_N * g.max_D;
+    const unsigned gx = (unsigned)std::min<long long>(64, (per + 255) / 256);
+    fused_gather<<<dim3(gx, g.count), 256, 0, s>>>(d_inst, g.d_ids);
+    fused_bump<<<ceil_div(g.count, 256), 256, 0, s>>>(d_inst, g.d_ids, g.count);
     MOEA_CUDA_TRY(cudaGetLastError());
     return MOEA_OK;
 }

@@ -75,78 +75,68 @@ __device__ __forceinline__ float fold_partials(const float* ws)
 
 __device__ __forceinline__ float safe_cos_hp(float v) { return fmaxf(0.0f, cosf(v * M_PI / 2.0f)); }
 
-// Objectives of one row from its g partial sum (thread-serial, like the
-// reference's thread 0).  x points at the row.
+// Objective m of one row from its g sum; x points at the row.  Each
+// objective is the reference's expression for it (dtlz_kernels.cu:28-716),
+// evaluated independently, so different threads may compute different m.
 template <int B>
-__device__ void row_objectives(float total_sum, const float* __restrict__ x, int D, int M, int N,
-                               int row, float* __restrict__ objs)
+__device__ float row_objective(int m, float total_sum, const float* __restrict__ x, int D, int M)
 {
     const int k = D - (M - 1);
     if (B == kDTLZ1) {
         const float g = 100.0f * (static_cast<float>(k) + total_sum);
         const float scalar = 0.5f * (1.0f + g);
-        for (int m = 0; m < M; ++m) {
-            float f = scalar;
-            for (int j = 0; j < M - 1 - m; ++j) f *= fmaxf(0.0f, fminf(1.0f, x[j]));
-            if (m > 0) f *= fmaxf(0.0f, 1.0f - x[M - 1 - m]);
-            objs[(size_t)m * N + row] = f;
-        }
+        float f = scalar;
+        for (int j = 0; j < M - 1 - m; ++j) f *= fmaxf(0.0f, fminf(1.0f, x[j]));
+        if (m > 0) f *= fmaxf(0.0f, 1.0f - x[M - 1 - m]);
+        return f;
     } else if (B == kDTLZ2 || B == kDTLZ3 || B == kConvexDTLZ2 || B == kDTLZ4) {
         const float g = (B == kDTLZ3) ? 100.0f * (static_cast<float>(k) + total_sum) : total_sum;
-        for (int m = 0; m < M; ++m) {
-            float f = 1.0f + g;
-            for (int j = 0; j < M - 1 - m; ++j)
-                f *= (B == kDTLZ4) ? fmaxf(0.0f, cosf(powf(x[j], 100.0f) * M_PI / 2.0f))
-                                   : safe_cos_hp(x[j]);
-            if (m > 0)
-                f *= (B == kDTLZ4) ? sinf(powf(x[M - 1 - m], 100.0f) * M_PI / 2.0f)
-                                   : sinf(x[M - 1 - m] * M_PI / 2.0f);
-            if (B == kConvexDTLZ2) {
-                if (m < M - 1) { f = f * f; f = f * f; } else { f = f * f; }
-            }
-            objs[(size_t)m * N + row] = f;
+        float f = 1.0f + g;
+        for (int j = 0; j < M - 1 - m; ++j)
+            f *= (B == kDTLZ4) ? fmaxf(0.0f, cosf(powf(x[j], 100.0f) * M_PI / 2.0f))
+                               : safe_cos_hp(x[j]);
+        if (m > 0)
+            f *= (B == kDTLZ4) ? sinf(powf(x[M - 1 - m], 100.0f) * M_PI / 2.0f)
+                               : sinf(x[M - 1 - m] * M_PI / 2.0f);
+        if (B == kConvexDTLZ2) {
+            if (m < M - 1) { f = f * f; f = f * f; } else { f = f * f; }
         }
+        return f;
     } else if (B == kDTLZ5 || B == kDTLZ6) {
         const float g = total_sum;
-        float theta[kMaxObjectives];
-        theta[0] = x[0];
         const float denom = 2.0f * (1.0f + g);
-        for (int i = 1; i < M - 1; ++i) {
-            const float xi = x[i];
-            theta[i] = (1.0f + 2.0f * g * xi) / denom;
-            if (B == kDTLZ5) theta[i] = fmaxf(0.0f, fminf(1.0f, theta[i]));
-        }
-        for (int m = 0; m < M; ++m) {
-            float f = 1.0f + g;
-            for (int j = 0; j < M - 1 - m; ++j)
-                f *= (B == kDTLZ5) ? fmaxf(0.0f, __cosf(theta[j] * M_PI * 0.5f))
-                                   : fmaxf(0.0f, cosf(theta[j] * M_PI * 0.5f));
-            if (m > 0)
-                f *= (B == kDTLZ5) ? __sinf(theta[M - 1 - m] * M_PI * 0.5f)
-                                   : sinf(theta[M - 1 - m] * M_PI * 0.5f);
-            objs[(size_t)m * N + row] = f;
-        }
-    } else if (B == kDTLZ7) {
+        auto theta = [&](int i) -> float {
+            if (i == 0) return x[0];
+            float t = (1.0f + 2.0f * g * x[i]) / denom;
+            if (B == kDTLZ5) t = fmaxf(0.0f, fminf(1.0f, t));
+            return t;
+        };
+        float f = 1.0f + g;
+        for (int j = 0; j < M - 1 - m; ++j)
+            f *= (B == kDTLZ5) ? fmaxf(0.0f, __cosf(theta(j) * M_PI * 0.5f))
+                               : fmaxf(0.0f, cosf(theta(j) * M_PI * 0.5f));
+        if (m > 0)
+            f *= (B == kDTLZ5) ? __sinf(theta(M - 1 - m) * M_PI * 0.5f)
+                               : sinf(theta(M - 1 - m) * M_PI * 0.5f);
+        return f;
+    } else {  // kDTLZ7
+        if (m < M - 1) return x[m];
         const float g = 1.0f + (9.0f / static_cast<float>(k)) * total_sum;
         float h_sum = 0.0f;
         for (int i = 0; i < M - 1; ++i) {
             const float fi = x[i];
-            objs[(size_t)i * N + row] = fi;
             h_sum += (fi / (1.0f + g)) * (1.0f + sinf(3.0f * M_PI * fi));
         }
         const float h = static_cast<float>(M) - h_sum;
-        objs[(size_t)(M - 1) * N + row] = (1.0f + g) * h;
+        return (1.0f + g) * h;
     }
 }
 
 // One warp per row; valid when the row has at most 256 g-terms.
 template <int B>
-__global__ void __launch_bounds__(256)
-dtlz_warp_rows(const float* __restrict__ vars, int N, int D, int M, float* __restrict__ objs)
+__device__ __forceinline__ void dtlz_warp_row(int row, int lane, const float* __restrict__ vars, int N,
+                                              int D, int M, float* __restrict__ objs)
 {
-    const int row = blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (row >= N) return;
     const float* x = vars + (size_t)row * D;
     const int start = (B == kDTLZ7) ? D - (D - M + 1) : M - 1;
     const int k = D - start;
@@ -158,7 +148,41 @@ dtlz_warp_rows(const float* __restrict__ vars, int N, int D, int M, float* __res
         if (t < k) a = g_accumulate<B>(a, x[start + t]);
         ws[w] = warp_tree(a);
     }
-    if (lane == 0) row_objectives<B>(fold_partials<B>(ws), x, D, M, N, row, objs);
+    float total = (lane == 0) ? fold_partials<B>(ws) : 0.0f;
+    total = __shfl_sync(0xFFFFFFFFu, total, 0);
+    if (lane < M) objs[(size_t)lane * N + row] = row_objective<B>(lane, total, x, D, M);
+}
+
+template <int B>
+__global__ void __launch_bounds__(256)
+dtlz_warp_rows(const float* __restrict__ vars, int N, int D, int M, float* __restrict__ objs)
+{
+    const int row = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (row >= N) return;
+    dtlz_warp_row<B>(row, threadIdx.x & 31, vars, N, D, M, objs);
+}
+
+// Fused batch: offspring objectives of every instance (blockIdx.y), problem
+// kinds 1..8 with at most 256 g-terms; their constraint violation is zero.
+__global__ void __launch_bounds__(256) fused_dtlz(const BatchInst* __restrict__ insts,
+                                                  const int* __restrict__ ids)
+{
+    const BatchInst& I = insts[ids[blockIdx.y]];
+    const int row = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (row >= I.N) return;
+    const int lane = threadIdx.x & 31;
+    switch (I.kind) {
+    case kDTLZ1: dtlz_warp_row<kDTLZ1>(row, lane, I.varsO, I.N, I.D, I.M, I.objsO); break;
+    case kDTLZ2: dtlz_warp_row<kDTLZ2>(row, lane, I.varsO, I.N, I.D, I.M, I.objsO); break;
+    case kDTLZ3: dtlz_warp_row<kDTLZ3>(row, lane, I.varsO, I.N, I.D, I.M, I.objsO); break;
+    case kDTLZ4: dtlz_warp_row<kDTLZ4>(row, lane, I.varsO, I.N, I.D, I.M, I.objsO); break;
+    case kDTLZ5: dtlz_warp_row<kDTLZ5>(row, lane, I.varsO, I.N, I.D, I.M, I.objsO); break;
+    case kDTLZ6: dtlz_warp_row<kDTLZ6>(row, lane, I.varsO, I.N, I.D, I.M, I.objsO); break;
+    case kDTLZ7: dtlz_warp_row<kDTLZ7>(row, lane, I.varsO, I.N, I.D, I.M, I.objsO); break;
+    case kConvexDTLZ2: dtlz_warp_row<kConvexDTLZ2>(row, lane, I.varsO, I.N, I.D, I.M, I.objsO); break;
+    default: break;
+    }
+    if (lane == 0) I.cvO[row] = 0.0f;
 }
 
 // One 256-thread block per row, the reference's strided accumulation.
@@ -175,13 +199,16 @@ dtlz_block_rows(const float* __restrict__ vars, int N, int D, int M, float* __re
     for (int i = threadIdx.x; i < k; i += 256) a = g_accumulate<B>(a, __ldg(x + start + i));
     a = warp_tree(a);
     __shared__ float ws[8];
+    __shared__ float s_total;
     if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = a;
     __syncthreads();
     if (threadIdx.x == 0) {
         float w8[8];
         for (int w = 0; w < 8; ++w) w8[w] = ws[w];
-        row_objectives<B>(fold_partials<B>(w8), x, D, M, N, row, objs);
+        s_total = fold_partials<B>(w8);
     }
+    __syncthreads();
+    if ((int)threadIdx.x < M) objs[(size_t)threadIdx.x * N + row] = row_objective<B>(threadIdx.x, s_total, x, D, M);
 }
 
 // Constraint violation from the objectives (dtlz_kernels.cu:824-1090).
@@ -330,6 +357,17 @@ void launch_rows(const float* x, int N, int D, int M, float* objs, cudaStream_t 
     else
         dtlz_block_rows<B><<<N, 256, 0, s>>>(x, N, D, M, objs);
 }
+
+}  // namespace
+
+int fused_evaluate(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s)
+{
+    fused_dtlz<<<dim3(ceil_div(g.max_N, 8), g.count), 256, 0, s>>>(d_inst, g.d_ids);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+namespace {
 
 float cv_radius(int kind, int M)
 {

@@ -129,15 +129,10 @@ __global__ void pm_explicit(float* __restrict__ off, const float* __restrict__ b
 }
 
 // Mating with Philox draws: child i draws block (i, generation, kTagMating).
-__global__ void mating_philox(const float* __restrict__ cv, const int* __restrict__ rank,
-                              const int* __restrict__ d_active, int active_host, int n_off,
-                              uint64_t seed, const int* __restrict__ d_gen, uint32_t gen_host,
-                              int* __restrict__ pidx)
+__device__ __forceinline__ void mating_child(int i, const float* __restrict__ cv,
+                                             const int* __restrict__ rank, int active, uint64_t seed,
+                                             uint32_t gen, int* __restrict__ pidx)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_off) return;
-    const int active = d_active ? *d_active : active_host;
-    const uint32_t gen = d_gen ? (uint32_t)*d_gen : gen_host;
     uint32_t r[4];
     rng_block(seed, (uint64_t)i, gen, kTagMating, r);
     const int a = (int)(r[0] % (uint32_t)active);
@@ -149,8 +144,53 @@ __global__ void mating_philox(const float* __restrict__ cv, const int* __restric
     pidx[i] = tournament_pick(a, b, cv, rank);
 }
 
+__global__ void mating_philox(const float* __restrict__ cv, const int* __restrict__ rank,
+                              const int* __restrict__ d_active, int active_host, int n_off,
+                              uint64_t seed, const int* __restrict__ d_gen, uint32_t gen_host,
+                              int* __restrict__ pidx)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_off) return;
+    const int active = d_active ? *d_active : active_host;
+    const uint32_t gen = d_gen ? (uint32_t)*d_gen : gen_host;
+    mating_child(i, cv, rank, active, seed, gen, pidx);
+}
+
 // SBX + PM for pair element e = p*D + d: one Philox block drives the SBX
 // draws (u1, u2, sign, copy), a second one the mutation draws of both children.
+__device__ __forceinline__ void variation_element(long long e, const float* __restrict__ parents,
+                                                  const int* __restrict__ pidx,
+                                                  const float* __restrict__ bounds,
+                                                  float* __restrict__ off, int pairs, int D,
+                                                  float eta_c, float sbx_prob, float copy_prob,
+                                                  int mutate, float eta_m, float pm_prob,
+                                                  uint64_t seed, uint32_t gen)
+{
+    const int p = (int)(e / D), d = (int)(e % D);
+    const float lo = bounds[2 * d], hi = bounds[2 * d + 1];
+    const int ca = 2 * p, cb = ca + 1;
+    float c1, c2;
+    if (p < pairs) {
+        const float x1 = parents[(size_t)pidx[ca] * D + d];
+        const float x2 = parents[(size_t)pidx[cb] * D + d];
+        uint32_t r[4];
+        rng_block(seed, (uint64_t)e, gen, kTagCrossover, r);
+        sbx_pair(x1, x2, u32_to_unit(r[0]), u32_to_unit(r[1]), (int)(r[2] & 1u),
+                 u32_to_unit(r[3]), eta_c, sbx_prob, copy_prob, lo, hi, c1, c2);
+    } else {
+        c1 = parents[(size_t)pidx[ca] * D + d];  // odd population: last child copies its parent
+        c2 = 0.0f;
+    }
+    if (mutate) {
+        uint32_t r[4];
+        rng_block(seed, (uint64_t)e, gen, kTagMutation, r);
+        c1 = pm_value(c1, u32_to_unit(r[0]), u32_to_unit(r[1]), eta_m, pm_prob, D, lo, hi);
+        c2 = pm_value(c2, u32_to_unit(r[2]), u32_to_unit(r[3]), eta_m, pm_prob, D, lo, hi);
+    }
+    off[(size_t)ca * D + d] = c1;
+    if (p < pairs) off[(size_t)cb * D + d] = c2;
+}
+
 __global__ void variation_philox(const float* __restrict__ parents, const int* __restrict__ pidx,
                                  const float* __restrict__ bounds, float* __restrict__ off,
                                  int n_off, int D, float sbx_eta0, float sbx_eta1, float sbx_prob,
@@ -164,31 +204,32 @@ __global__ void variation_philox(const float* __restrict__ parents, const int* _
     const float eta_c = annealed_eta(sbx_eta0, sbx_eta1, (int)gen, total);
     const float eta_m = annealed_eta(pm_eta0, pm_eta1, (int)gen, total);
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < count;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int p = (int)(e / D), d = (int)(e % D);
-        const float lo = bounds[2 * d], hi = bounds[2 * d + 1];
-        const int ca = 2 * p, cb = ca + 1;
-        float c1, c2;
-        if (p < pairs) {
-            const float x1 = parents[(size_t)pidx[ca] * D + d];
-            const float x2 = parents[(size_t)pidx[cb] * D + d];
-            uint32_t r[4];
-            rng_block(seed, (uint64_t)e, gen, kTagCrossover, r);
-            sbx_pair(x1, x2, u32_to_unit(r[0]), u32_to_unit(r[1]), (int)(r[2] & 1u),
-                     u32_to_unit(r[3]), eta_c, sbx_prob, copy_prob, lo, hi, c1, c2);
-        } else {
-            c1 = parents[(size_t)pidx[ca] * D + d];  // odd population: last child copies its parent
-            c2 = 0.0f;
-        }
-        if (mutate) {
-            uint32_t r[4];
-            rng_block(seed, (uint64_t)e, gen, kTagMutation, r);
-            c1 = pm_value(c1, u32_to_unit(r[0]), u32_to_unit(r[1]), eta_m, pm_prob, D, lo, hi);
-            c2 = pm_value(c2, u32_to_unit(r[2]), u32_to_unit(r[3]), eta_m, pm_prob, D, lo, hi);
-        }
-        off[(size_t)ca * D + d] = c1;
-        if (p < pairs) off[(size_t)cb * D + d] = c2;
-    }
+         e += (long long)gridDim.x * blockDim.x)
+        variation_element(e, parents, pidx, bounds, off, pairs, D, eta_c, sbx_prob, copy_prob, mutate,
+                          eta_m, pm_prob, seed, gen);
+}
+
+// ---- fused batch: mating then variation of every instance (blockIdx.y) ----
+__global__ void fused_mating(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    const BatchInst& I = insts[ids[blockIdx.y]];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= I.N) return;
+    mating_child(i, I.cvP, I.tournament ? I.rankP : nullptr, I.N, I.seed, (uint32_t)*I.d_gen, I.pidx);
+}
+
+__global__ void fused_variation(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    const BatchInst& I = insts[ids[blockIdx.y]];
+    const int pairs = I.N / 2;
+    const long long count = (long long)(pairs + (I.N & 1)) * I.D;
+    const uint32_t gen = (uint32_t)*I.d_gen;
+    const float eta_c = annealed_eta(I.sbx_eta0, I.sbx_eta1, (int)gen, I.T);
+    const float eta_m = annealed_eta(I.pm_eta0, I.pm_eta1, (int)gen, I.T);
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < count;
+         e += (long long)gridDim.x * blockDim.x)
+        variation_element(e, I.varsP, I.pidx, I.bounds, I.varsO, pairs, I.D, eta_c, I.sbx_prob, I.sbx_copy,
+                          I.mutate, eta_m, I.pm_prob, I.seed, gen);
 }
 
 __global__ void rng_blocks_kernel(uint64_t seed, uint32_t gen, uint32_t tag, long long count,
@@ -242,6 +283,15 @@ int run_variation(const float* parents, const int* pidx, const float* bounds, fl
     variation_philox<<<grid_for(count, 256), 256, 0, stream>>>(
         parents, pidx, bounds, off, n_off, D, sbx_eta0, sbx_eta1, sbx_prob, copy_prob, mutate,
         pm_eta0, pm_eta1, pm_prob, total, seed, d_gen, gen);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+int fused_reproduce(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s)
+{
+    fused_mating<<<dim3(ceil_div(g.max_N, 256), g.count), 256, 0, s>>>(d_inst, g.d_ids);
+    const long long per = (long long)(g.max_N / 2 + 1) * g.max_D;
+    fused_variation<<<dim3((unsigned)grid_for(per, 256, 64), g.count), 256, 0, s>>>(d_inst, g.d_ids);
     MOEA_CUDA_TRY(cudaGetLastError());
     return MOEA_OK;
 }

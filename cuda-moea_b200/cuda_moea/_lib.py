@@ -120,12 +120,12 @@ _SIGNATURES = [
     ("moea_algorithm_profile_step", c_int, [vp, ctypes.c_char_p, c_size_t, fp, c_int, ip]),
     ("moea_algorithm_selection_stats", c_int, [vp, ip, ip]),
     ("moea_algorithm_device_status", c_int, [vp, ip]),
-    ("moea_batch_create", c_int, [ctypes.POINTER(AlgorithmConfig), c_int, vp, ctypes.POINTER(vp)]),
+    ("moea_batch_create", c_int, [ctypes.POINTER(AlgorithmConfig), c_int, vp, c_int, ctypes.POINTER(vp)]),
     ("moea_batch_destroy", None, [vp]),
     ("moea_batch_step", c_int, [vp]),
     ("moea_batch_run", c_int, [vp, c_int, ctypes.POINTER(ctypes.c_double)]),
     ("moea_batch_synchronize", c_int, [vp]),
-    ("moea_batch_info", c_int, [vp, ip, ip, ip]),
+    ("moea_batch_info", c_int, [vp, ip, ip, ip, ip]),
     ("moea_batch_view", c_int, [vp, c_int, ctypes.POINTER(PopulationViewC)]),
 ]
 

@@ -21,7 +21,7 @@ class Batch:
     """Advance ``algorithms`` (not yet initialised, built-in problems and
     mating, same device and max_generations) as one batch."""
 
-    def __init__(self, algorithms: Sequence[Algorithm]):
+    def __init__(self, algorithms: Sequence[Algorithm], *, fuse: bool = True, groups: int = 0):
         if not algorithms:
             raise ValueError("Batch needs at least one algorithm")
         n = len(algorithms)
@@ -40,7 +40,10 @@ class Batch:
         with torch.cuda.device(self._device):
             self.stream = torch.cuda.Stream(self._device)
         handle = ctypes.c_void_p()
-        check(lib().moea_batch_create(cfgs, n, ctypes.c_void_p(self.stream.cuda_stream), ctypes.byref(handle)))
+        # MOEA_BATCH_NO_FUSION = 1; MOEA_BATCH_GROUPS(g) = g << 8 (0: library default)
+        flags = (0 if fuse else 1) | ((int(groups) & 0xFF) << 8)
+        check(lib().moea_batch_create(cfgs, n, ctypes.c_void_p(self.stream.cuda_stream), flags,
+                                      ctypes.byref(handle)))
         self._handle = handle
         self._count = n
         self._total_ms = 0.0
@@ -75,10 +78,16 @@ class Batch:
     def synchronize(self) -> None:
         check(lib().moea_batch_synchronize(self._handle))
 
-    def _info(self) -> tuple[int, int, int]:
-        c, g, k = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        check(lib().moea_batch_info(self._handle, ctypes.byref(c), ctypes.byref(g), ctypes.byref(k)))
-        return c.value, g.value, k.value
+    def _info(self) -> tuple[int, int, int, int]:
+        c, g, k, f = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().moea_batch_info(self._handle, ctypes.byref(c), ctypes.byref(g), ctypes.byref(k),
+                                    ctypes.byref(f)))
+        return c.value, g.value, k.value, f.value
+
+    @property
+    def fused(self) -> bool:
+        """True when every stage runs as one launch for all instances."""
+        return bool(self._info()[3])
 
     @property
     def generation(self) -> int:

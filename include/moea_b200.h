@@ -341,20 +341,31 @@ moea_status moea_algorithm_device_status(moea_algorithm* alg, int* h_status);
  * Batched instances (the batching form; no counterpart in the reference,
  * whose algorithms run one at a time).  count independent algorithms with
  * built-in problems and mating, one device and one max_generations, advance
- * together: one CUDA graph launch per generation holds every instance's
- * generation as a parallel branch.  Each instance's results equal those of
- * running it alone with moea_algorithm_*.  cfgs[i].stream and use_graphs are
- * ignored; stream (NULL = internal) orders all of the batch's work.
+ * together with one CUDA graph launch per generation.  Each instance's
+ * results equal those of running it alone with moea_algorithm_*.
+ *   Fused mode (when every instance is NSGA-III on a built-in unconstrained
+ *   problem with at most 256 g-terms, 2N <= 8192, fixed directions, no CV
+ *   quantisation): every stage is one launch for all instances.
+ *   The fused instances are split into groups of similar pair-test load
+ *   (MOEA_BATCH_GROUPS(g) in flags, default 16); each group's chain of
+ *   kernels is a parallel branch of the graph.
+ *   Otherwise (or with MOEA_BATCH_NO_FUSION): each instance's generation is
+ *   a parallel branch of the graph.
+ * cfgs[i].stream and use_graphs are ignored; stream (NULL = internal) orders
+ * all of the batch's work.
  * ====================================================================== */
 typedef struct moea_batch moea_batch;
-moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void* stream,
+#define MOEA_BATCH_NO_FUSION 1
+#define MOEA_BATCH_GROUPS(g) (((g) & 0xFF) << 8)
+moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void* stream, int flags,
                               moea_batch** out);
 void moea_batch_destroy(moea_batch* b);
 moea_status moea_batch_step(moea_batch* b);
 /* generations < 0: run to max_generations.  *h_total_ms: device time. */
 moea_status moea_batch_run(moea_batch* b, int generations, double* h_total_ms);
 moea_status moea_batch_synchronize(moea_batch* b);
-moea_status moea_batch_info(moea_batch* b, int* h_count, int* h_generation, int* h_graph_kernels);
+moea_status moea_batch_info(moea_batch* b, int* h_count, int* h_generation, int* h_graph_kernels,
+                            int* h_fused);
 /* Population view of instance `index` (same contract as moea_algorithm_view). */
 moea_status moea_batch_view(moea_batch* b, int index, moea_population_view* out);
 

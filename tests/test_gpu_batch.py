@@ -41,6 +41,7 @@ def test_batch_equals_instances_run_alone():
     specs = _specs(12, 7)
     batch = cm.Batch([_make(s, T) for s in specs])
     assert len(batch) == 12
+    assert batch.fused  # NSGA-III on DTLZ1-7 with 2N <= 8192: one launch per stage
     batch.run(3)
     mid = [batch.result(i) for i in range(len(specs))]
     batch.run()
@@ -98,3 +99,25 @@ def test_batch_rejects_callbacks_and_mismatched_generations():
     with pytest.raises(MoeaError):
         cm.Batch([cm.NSGA3(population_size=32, max_generations=3, problem=cm.DTLZ2(12, 3), print_progress=False),
                   cm.NSGA3(population_size=32, max_generations=4, problem=cm.DTLZ2(12, 3), print_progress=False)])
+
+
+@pytest.mark.parametrize("seed,n_hi", [(21, 4096), (22, 200)])
+def test_fused_batch_equals_branch_batch(seed, n_hi):
+    """The fused batch (one launch per stage) against the graph-branch batch on
+    the same instances, including the largest fused size (N = 4096) and tiny
+    populations."""
+    T = 4
+    specs = _specs(9, seed, n_lo=92, n_hi=n_hi)
+    if n_hi == 4096:
+        specs[0] = ("DTLZ1", 3, 4096, 12, 7)
+        specs[1] = ("DTLZ7", 8, 4096, 27, 8)
+    fused = cm.Batch([_make(s, T) for s in specs])
+    branch = cm.Batch([_make(s, T) for s in specs], fuse=False)
+    assert fused.fused and not branch.fused
+    for _ in range(T):
+        fused.step()
+        branch.step()
+        for i in range(len(specs)):
+            a, b = fused.result(i), branch.result(i)
+            _same(a, b)
+            np.testing.assert_array_equal(a.auxiliary_indices.cpu().numpy(), b.auxiliary_indices.cpu().numpy())
