@@ -244,7 +244,8 @@ def batched_measure(args, torch, cm):
            "instance_gen_per_s": n * K / (batch_ms / 1e3),
            "plain_loop_instance_gen_per_s": n * K / (plain_ms / 1e3),
            "speedup_vs_plain_loop": plain_ms / batch_ms,
-           "identical_ranks": identical, "graph_kernels_per_generation": batch.graph_kernels,
+           "identical_ranks": identical, "fused": batch.fused,
+           "graph_kernels_per_generation": batch.graph_kernels,
            "pair_tests_per_generation": sum((2 * s[2]) ** 2 for s in specs)}
     batch.close()
     del plain

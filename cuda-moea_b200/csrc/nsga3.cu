@@ -1377,10 +1377,17 @@ int run_niching(Workspace& ws, uint64_t seed, const int* nds_gidx, const float* 
     nich_prior<<<G, T, 0, stream>>>(nds_gidx, idx, sizes, H, ws.rho, selected);
     nich_keys1<<<G, T, 0, stream>>>(idx, dist, sizes, n_cap, ws.key64[0], ws.sel_vals[0]);
     size_t tmp = ws.cub_bytes;
+    // Bits that order the keys: the high word holds a direction index below
+    // H (0xFFFFFFFF for none) in stages 1-2 and rho + rank <= 2N in stage 3;
+    // padding keys are all ones, the maximum of any bit range, and an index
+    // 0xFFFFFFFF truncated to the range still sorts after every valid index.
+    auto bits_for = [](long long v) { int b = 1; while ((1ll << b) <= v) ++b; return b; };
+    const int end12 = std::min(64, 32 + bits_for((long long)H + 1));
+    const int end3 = std::min(64, 32 + bits_for(2ll * N + 1));
     for (int stage = 1; stage <= 3; ++stage) {
         MOEA_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp, tmp, ws.key64[0], ws.key64[1],
-                                                      ws.sel_vals[0], ws.sel_vals[1], n_cap, 0, 64,
-                                                      stream));
+                                                      ws.sel_vals[0], ws.sel_vals[1], n_cap, 0,
+                                                      stage == 3 ? end3 : end12, stream));
         std::swap(ws.key64[0], ws.key64[1]);
         std::swap(ws.sel_vals[0], ws.sel_vals[1]);
         if (stage == 3) break;
