@@ -118,6 +118,18 @@ int dmalloc(T** p, size_t count)
 
 using namespace moea;
 
+struct moea_algorithm;
+
+namespace {
+// Fused generation (one launch per stage for a group of instances): whether
+// an algorithm qualifies, its descriptor for one parity of the slot
+// rotation, and the launch plan of a group of instances.
+bool fused_eligible(const moea_algorithm* a);
+BatchInst fused_describe(moea_algorithm* a, int P, int X);
+int fused_build_group(const std::vector<moea_algorithm*>& inst, const std::vector<int>& ids, FusedGroup& g);
+void fused_free_group(FusedGroup& g);
+}  // namespace
+
 struct moea_algorithm {
     moea_algorithm_config cfg{};
     std::vector<float> lower, upper, user_dirs, init_pop;
@@ -162,6 +174,13 @@ struct moea_algorithm {
     cudaGraphExec_t graph[2] = {};
     bool graph_failed = false;
     int graph_kernels = 0;
+    // small populations: the generation as the fused kernels of a one-instance group
+    bool fused_single = false;
+    BatchInst* f_inst[2] = {};
+    FusedGroup f_group;
+
+    int setup_single_fused();
+    int describe_single_fused();
 
     void drop_graphs()
     {
@@ -175,6 +194,10 @@ struct moea_algorithm {
     {
         for (auto& g : graph)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        for (auto& d : f_inst)
+            if (d) { cudaFree(d); d = nullptr; }
+        fused_free_group(f_group);
+        fused_single = false;
         void* ptrs[] = {vars[0], vars[1], vars[2], objs[0], objs[1], objs[2], cv[0], cv[1], cv[2],
                         rank[0], rank[1], rank[2], cv_sort[0], cv_sort[1], bounds, parent_idx, refs,
                         refs0, gamma, ideal_last, d_gen, d_active, ps_table, cv_table, t_buf, theta,
@@ -401,6 +424,7 @@ struct moea_algorithm {
         }
         MOEA_TRY(start_population());
         initialized = true;
+        if (cfg.fused_small && fused_eligible(this)) MOEA_TRY(setup_single_fused());
         return MOEA_OK;
     }
 
@@ -433,6 +457,13 @@ struct moea_algorithm {
     // is replayed from a CUDA graph.
     int generation_body()
     {
+        if (fused_single) {
+            const BatchInst* d = f_inst[P == 0 ? 0 : 1];
+            MOEA_TRY(fused_reproduce(d, f_group, stream));
+            MOEA_TRY(fused_evaluate(d, f_group, stream));
+            MOEA_TRY(fused_ndsort(d, f_group, stream));
+            return fused_select(d, f_group, stream);
+        }
         const uint64_t s = gen_seed();
         if (cfg.mating == MOEA_MATING_CALLBACK) {
             const int rc = cfg.mate(cfg.mate_user, vars[P], objs[P], cv[P], nsga3() ? rank[P] : nullptr,
@@ -613,7 +644,10 @@ struct moea_algorithm {
         }
         total_ms = 0.0;
         frontzero_count = 0;
-        return start_population();
+        MOEA_TRY(start_population());
+        // the draws of the new epoch use another seed
+        if (fused_single) MOEA_TRY(describe_single_fused());
+        return MOEA_OK;
     }
 };
 
@@ -645,6 +679,7 @@ void moea_algorithm_config_defaults(moea_algorithm_config* c, int algorithm)
     c->sparse_ratio = 0.5f;
     c->rvea_alpha = 2.0f;
     c->use_graphs = 1;
+    c->fused_small = 1;
 }
 
 moea_status moea_algorithm_create(const moea_algorithm_config* cfg, moea_algorithm** out)
@@ -839,6 +874,124 @@ moea_status moea_algorithm_device_status(moea_algorithm* a, int* h_status)
 // branches may run side by side.
 // ---------------------------------------------------------------------------
 
+namespace {
+
+// Every instance of a fused generation: NSGA-III, built-in unconstrained
+// problems with at most 256 g-terms, built-in mating, fixed directions
+// searched by the cone tree, no CV quantisation, 2N <= 8192, slots at the
+// start of their rotation.
+bool fused_eligible(const moea_algorithm* a)
+{
+    const moea_algorithm_config& c = a->cfg;
+    const int k = c.problem_kind == 7 ? a->D - a->M + 1 : a->D - (a->M - 1);
+    return a->nsga3() && c.problem_kind >= 1 && c.problem_kind <= 8 && k >= 1 && k <= 256 &&
+           2 * a->N <= kFusedMaxPoints && c.mating != MOEA_MATING_CALLBACK &&
+           c.directions != MOEA_DIRS_ADAPTIVE && c.cv_bins <= 0 && a->assoc_mode() == MOEA_ASSOC_TREE &&
+           direction_tree_ready(a->ws, a->refs, a->M, a->H) && a->ws.tree_depth <= kDirTreeMaxDepth &&
+           a->P == 0 && a->X == 2;
+}
+
+BatchInst fused_describe(moea_algorithm* a, int P, int X)
+{
+    const moea_algorithm_config& c = a->cfg;
+    Workspace& w = a->ws;
+    BatchInst b{};
+    b.N = a->N; b.D = a->D; b.M = a->M; b.H = a->H; b.n = 2 * a->N; b.n_max = w.n_max; b.W = w.words;
+    b.kind = c.problem_kind; b.tournament = c.mating == MOEA_MATING_TOURNAMENT; b.mutate = c.mutation;
+    b.T = a->T;
+    b.sbx_eta0 = c.sbx_eta_initial; b.sbx_eta1 = c.sbx_eta_final; b.sbx_prob = c.sbx_probability;
+    b.sbx_copy = c.sbx_copy_probability; b.pm_eta0 = c.pm_eta_initial; b.pm_eta1 = c.pm_eta_final;
+    b.pm_prob = c.pm_probability;
+    b.seed = a->gen_seed(); b.nich_seed = a->seed;
+    b.varsP = a->vars[P]; b.objsP = a->objs[P]; b.cvP = a->cv[P]; b.rankP = a->rank[P];
+    b.varsO = a->vars[1]; b.objsO = a->objs[1]; b.cvO = a->cv[1];
+    b.varsX = a->vars[X]; b.objsX = a->objs[X]; b.cvX = a->cv[X]; b.rankX = a->rank[X];
+    b.bounds = a->bounds; b.pidx = a->parent_idx; b.d_gen = a->d_gen; b.ideal = a->ideal_last;
+    b.key0 = w.key0; b.key64 = w.key64[0]; b.perm = w.perm[0]; b.vals = w.sel_vals[0];
+    b.sorted_f = w.sorted_f; b.qinfo = w.qinfo; b.blocker = w.blocker; b.front_sorted = w.front_sorted;
+    b.front_list = w.front_list; b.counters = w.counters; b.rows = w.rows; b.chunk_keys = w.chunk_keys;
+    b.chunk_bits = w.chunk_bits; b.fronts = w.fronts; b.nds_gidx = w.nds_gidx; b.sizes = w.sizes;
+    b.nds_objs = w.nds_objs; b.rcp_b = w.rcp_b; b.extreme = w.extreme; b.assoc_idx = w.assoc_idx;
+    b.assoc_dist = w.assoc_dist; b.rho = w.rho; b.selected = w.selected; b.flags = w.flags;
+    b.survivors = a->survivors; b.offset = w.offset_dev;
+    b.t_dirs_orig = a->refs;
+    b.t_dirs = w.tree_dirs; b.t_order = w.tree_order; b.t_center = w.tree_center; b.t_cos = w.tree_cos;
+    b.t_sin = w.tree_sin; b.t_link = w.tree_link; b.t_nodes = w.tree_nodes; b.t_delta = w.tree_delta;
+    return b;
+}
+
+int fused_build_group(const std::vector<moea_algorithm*>& inst, const std::vector<int>& ids, FusedGroup& g)
+{
+    g = FusedGroup{};
+    g.count = (int)ids.size();
+    for (int i : ids) {
+        g.max_n = std::max(g.max_n, 2 * inst[i]->N);
+        g.max_N = std::max(g.max_N, inst[i]->N);
+        g.max_D = std::max(g.max_D, inst[i]->D);
+        g.max_M = std::max(g.max_M, inst[i]->M);
+    }
+    MOEA_CUDA_TRY(cudaMalloc((void**)&g.d_ids, sizeof(int) * ids.size()));
+    MOEA_CUDA_TRY(cudaMemcpy(g.d_ids, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
+    for (int m = 1; m <= kMaxObjectives; ++m) {
+        std::vector<int> bids, prefix{0};
+        int mn = 0;
+        for (int i : ids) {
+            if (inst[i]->M != m) continue;
+            bids.push_back(i);
+            const int n = 2 * inst[i]->N;
+            prefix.push_back(prefix.back() + fused_tile_blocks(m, n));
+            mn = std::max(mn, n);
+        }
+        if (bids.empty()) continue;
+        FusedBucket b;
+        b.M = m;
+        b.count = (int)bids.size();
+        b.max_n = mn;
+        b.tile_blocks = prefix.back();
+        MOEA_CUDA_TRY(cudaMalloc((void**)&b.d_ids, sizeof(int) * bids.size()));
+        MOEA_CUDA_TRY(cudaMalloc((void**)&b.d_tile_prefix, sizeof(int) * prefix.size()));
+        MOEA_CUDA_TRY(cudaMemcpy(b.d_ids, bids.data(), sizeof(int) * bids.size(), cudaMemcpyHostToDevice));
+        MOEA_CUDA_TRY(cudaMemcpy(b.d_tile_prefix, prefix.data(), sizeof(int) * prefix.size(),
+                                 cudaMemcpyHostToDevice));
+        g.buckets.push_back(b);
+    }
+    return MOEA_OK;
+}
+
+void fused_free_group(FusedGroup& g)
+{
+    if (g.d_ids) cudaFree(g.d_ids);
+    for (auto& b : g.buckets) {
+        if (b.d_ids) cudaFree(b.d_ids);
+        if (b.d_tile_prefix) cudaFree(b.d_tile_prefix);
+    }
+    g = FusedGroup{};
+}
+
+}  // namespace
+
+// One-instance fused plan: descriptors of both parities (instance index 0).
+int moea_algorithm::describe_single_fused()
+{
+    for (int parity = 0; parity < 2; ++parity) {
+        const BatchInst h = fused_describe(this, parity == 0 ? 0 : 2, parity == 0 ? 2 : 0);
+        if (!f_inst[parity]) MOEA_CUDA_TRY(cudaMalloc((void**)&f_inst[parity], sizeof(BatchInst)));
+        MOEA_CUDA_TRY(cudaMemcpy(f_inst[parity], &h, sizeof(BatchInst), cudaMemcpyHostToDevice));
+    }
+    return MOEA_OK;
+}
+
+int moea_algorithm::setup_single_fused()
+{
+    MOEA_TRY(fused_ndsort_configure());
+    MOEA_TRY(fused_select_configure());
+    MOEA_TRY(describe_single_fused());
+    std::vector<moea_algorithm*> self{this};
+    MOEA_TRY(fused_build_group(self, {0}, f_group));
+    fused_single = true;
+    return MOEA_OK;
+}
+
 struct moea_batch {
     std::vector<moea_algorithm*> inst;
     // fused mode: one launch per stage for each group of instances; the
@@ -868,13 +1021,7 @@ struct moea_batch {
             if (g) cudaGraphExecDestroy(g);
         for (auto& d : d_inst)
             if (d) cudaFree(d);
-        for (auto& g : groups) {
-            if (g.d_ids) cudaFree(g.d_ids);
-            for (auto& b : g.buckets) {
-                if (b.d_ids) cudaFree(b.d_ids);
-                if (b.d_tile_prefix) cudaFree(b.d_tile_prefix);
-            }
-        }
+        for (auto& g : groups) fused_free_group(g);
         for (cudaStream_t gs : gstream) cudaStreamDestroy(gs);
         for (cudaEvent_t e : gjoin) cudaEventDestroy(e);
         for (moea_algorithm* a : inst) delete a;
@@ -884,53 +1031,10 @@ struct moea_batch {
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 
-    // Whether every instance fits the fused generation: NSGA-III, built-in
-    // unconstrained problems with at most 256 g-terms, built-in mating, fixed
-    // directions searched by the cone tree, no CV quantisation, 2N <= 8192.
-    static bool fusable(const moea_algorithm* a)
-    {
-        const moea_algorithm_config& c = a->cfg;
-        const int k = c.problem_kind == 7 ? a->D - a->M + 1 : a->D - (a->M - 1);
-        return a->nsga3() && c.problem_kind >= 1 && c.problem_kind <= 8 && k >= 1 && k <= 256 &&
-               2 * a->N <= kFusedMaxPoints && c.mating != MOEA_MATING_CALLBACK &&
-               c.directions != MOEA_DIRS_ADAPTIVE && c.cv_bins <= 0 &&
-               a->assoc_mode() == MOEA_ASSOC_TREE && direction_tree_ready(a->ws, a->refs, a->M, a->H) &&
-               a->ws.tree_depth <= kDirTreeMaxDepth;
-    }
-
-    static BatchInst describe(moea_algorithm* a, int P, int X)
-    {
-        const moea_algorithm_config& c = a->cfg;
-        Workspace& w = a->ws;
-        BatchInst b{};
-        b.N = a->N; b.D = a->D; b.M = a->M; b.H = a->H; b.n = 2 * a->N; b.n_max = w.n_max; b.W = w.words;
-        b.kind = c.problem_kind; b.tournament = c.mating == MOEA_MATING_TOURNAMENT; b.mutate = c.mutation;
-        b.T = a->T;
-        b.sbx_eta0 = c.sbx_eta_initial; b.sbx_eta1 = c.sbx_eta_final; b.sbx_prob = c.sbx_probability;
-        b.sbx_copy = c.sbx_copy_probability; b.pm_eta0 = c.pm_eta_initial; b.pm_eta1 = c.pm_eta_final;
-        b.pm_prob = c.pm_probability;
-        b.seed = a->gen_seed(); b.nich_seed = a->seed;
-        b.varsP = a->vars[P]; b.objsP = a->objs[P]; b.cvP = a->cv[P]; b.rankP = a->rank[P];
-        b.varsO = a->vars[1]; b.objsO = a->objs[1]; b.cvO = a->cv[1];
-        b.varsX = a->vars[X]; b.objsX = a->objs[X]; b.cvX = a->cv[X]; b.rankX = a->rank[X];
-        b.bounds = a->bounds; b.pidx = a->parent_idx; b.d_gen = a->d_gen; b.ideal = a->ideal_last;
-        b.key0 = w.key0; b.key64 = w.key64[0]; b.perm = w.perm[0]; b.vals = w.sel_vals[0];
-        b.sorted_f = w.sorted_f; b.qinfo = w.qinfo; b.blocker = w.blocker; b.front_sorted = w.front_sorted;
-        b.front_list = w.front_list; b.counters = w.counters; b.rows = w.rows; b.chunk_keys = w.chunk_keys;
-        b.chunk_bits = w.chunk_bits; b.fronts = w.fronts; b.nds_gidx = w.nds_gidx; b.sizes = w.sizes;
-        b.nds_objs = w.nds_objs; b.rcp_b = w.rcp_b; b.extreme = w.extreme; b.assoc_idx = w.assoc_idx;
-        b.assoc_dist = w.assoc_dist; b.rho = w.rho; b.selected = w.selected; b.flags = w.flags;
-        b.survivors = a->survivors; b.offset = w.offset_dev;
-        b.t_dirs_orig = a->refs;
-        b.t_dirs = w.tree_dirs; b.t_order = w.tree_order; b.t_center = w.tree_center; b.t_cos = w.tree_cos;
-        b.t_sin = w.tree_sin; b.t_link = w.tree_link; b.t_nodes = w.tree_nodes; b.t_delta = w.tree_delta;
-        return b;
-    }
-
     int setup_fused()
     {
         for (moea_algorithm* a : inst)
-            if (!fusable(a)) return MOEA_OK;
+            if (!fused_eligible(a)) return MOEA_OK;
         for (moea_algorithm* a : inst)
             if (a->P != 0 || a->X != 2) return MOEA_OK;
         MOEA_TRY(fused_ndsort_configure());
@@ -938,7 +1042,7 @@ struct moea_batch {
         const int count = (int)inst.size();
         for (int parity = 0; parity < 2; ++parity) {
             std::vector<BatchInst> h(count);
-            for (int i = 0; i < count; ++i) h[i] = describe(inst[i], parity == 0 ? 0 : 2, parity == 0 ? 2 : 0);
+            for (int i = 0; i < count; ++i) h[i] = fused_describe(inst[i], parity == 0 ? 0 : 2, parity == 0 ? 2 : 0);
             MOEA_CUDA_TRY(cudaMalloc((void**)&d_inst[parity], sizeof(BatchInst) * count));
             MOEA_CUDA_TRY(cudaMemcpy(d_inst[parity], h.data(), sizeof(BatchInst) * count, cudaMemcpyHostToDevice));
         }
@@ -962,38 +1066,7 @@ struct moea_batch {
             std::vector<int>& ids = members[gi];
             std::sort(ids.begin(), ids.end());
             FusedGroup g;
-            g.count = (int)ids.size();
-            for (int i : ids) {
-                g.max_n = std::max(g.max_n, 2 * inst[i]->N);
-                g.max_N = std::max(g.max_N, inst[i]->N);
-                g.max_D = std::max(g.max_D, inst[i]->D);
-                g.max_M = std::max(g.max_M, inst[i]->M);
-            }
-            MOEA_CUDA_TRY(cudaMalloc((void**)&g.d_ids, sizeof(int) * ids.size()));
-            MOEA_CUDA_TRY(cudaMemcpy(g.d_ids, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
-            for (int m = 1; m <= kMaxObjectives; ++m) {
-                std::vector<int> bids, prefix{0};
-                int mn = 0;
-                for (int i : ids) {
-                    if (inst[i]->M != m) continue;
-                    bids.push_back(i);
-                    const int n = 2 * inst[i]->N;
-                    prefix.push_back(prefix.back() + fused_tile_blocks(m, n));
-                    mn = std::max(mn, n);
-                }
-                if (bids.empty()) continue;
-                FusedBucket b;
-                b.M = m;
-                b.count = (int)bids.size();
-                b.max_n = mn;
-                b.tile_blocks = prefix.back();
-                MOEA_CUDA_TRY(cudaMalloc((void**)&b.d_ids, sizeof(int) * bids.size()));
-                MOEA_CUDA_TRY(cudaMalloc((void**)&b.d_tile_prefix, sizeof(int) * prefix.size()));
-                MOEA_CUDA_TRY(cudaMemcpy(b.d_ids, bids.data(), sizeof(int) * bids.size(), cudaMemcpyHostToDevice));
-                MOEA_CUDA_TRY(cudaMemcpy(b.d_tile_prefix, prefix.data(), sizeof(int) * prefix.size(),
-                                         cudaMemcpyHostToDevice));
-                g.buckets.push_back(b);
-            }
+            MOEA_TRY(fused_build_group(inst, ids, g));
             groups.push_back(std::move(g));
             cudaStream_t gs = nullptr;
             cudaEvent_t ge = nullptr;
@@ -1122,6 +1195,7 @@ moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void
         moea_algorithm_config c = cfgs[i];
         c.stream = b->stream;
         c.use_graphs = 0;
+        c.fused_small = 0;  // the batch fuses its instances itself
         moea_algorithm* a = nullptr;
         st = moea_algorithm_create(&c, &a);
         if (st != MOEA_OK) break;

@@ -52,7 +52,7 @@ class AlgorithmConfig(ctypes.Structure):
         ("sparse_ratio", c_float), ("cv_bins", c_int), ("cv_clip_upper", c_float),
         ("cv_log_alpha", c_float), ("feasibility_epsilon", c_float),
         ("association_mode", c_int), ("rvea_alpha", c_float),
-        ("h_initial_population", fp), ("use_graphs", c_int),
+        ("h_initial_population", fp), ("use_graphs", c_int), ("fused_small", c_int),
     ]
 
 

@@ -109,7 +109,7 @@ class Algorithm:
                  seed: int | None = None, enable_warmup: bool | None = None,
                  progress_interval: int = 100, print_progress: bool = True,
                  save_data: str | Path | None = None,
-                 save_interval: int = 1, use_graphs: bool = True) -> None:
+                 save_interval: int = 1, use_graphs: bool = True, fuse_small: bool = True) -> None:
         kind = algorithm.upper().replace("-", "")
         if kind not in {"NSGA3", "RVEA"}:
             raise ValueError("algorithm must be 'NSGA3' or 'RVEA'")
@@ -142,6 +142,7 @@ class Algorithm:
         self._save_interval = save_interval
         self._device = int(cuda.device_id)
         self._use_graphs = bool(use_graphs)
+        self._fuse_small = bool(fuse_small)
         self._initial = None
         if initial_population is not None:
             t = torch.as_tensor(initial_population).detach().to("cpu", torch.float32).contiguous()
@@ -195,6 +196,7 @@ class Algorithm:
             self.stream = cur
             cfg.stream = cur.cuda_stream
         cfg.use_graphs = 1 if self._use_graphs else 0
+        cfg.fused_small = 1 if self._fuse_small else 0
         D, M = self._problem_info
         cfg.dimension, cfg.objectives = D, M
         p = self._specs["problem"]

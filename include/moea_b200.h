@@ -287,6 +287,9 @@ typedef struct moea_algorithm_config {
     /* initial population (N,D) row-major on the host, or NULL */
     const float* h_initial_population;
     int use_graphs;           /* capture one generation into a CUDA graph when possible */
+    int fused_small;          /* run an eligible population with 2N <= 8192 (NSGA-III, built-in
+                                 unconstrained DTLZ, fixed directions) as the fused generation:
+                                 same results, about 20 launches instead of about 80 */
 } moea_algorithm_config;
 
 /* Fills cfg with the reference defaults (nat/src/factory/algorithm_factory.cu:25-118). */

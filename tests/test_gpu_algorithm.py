@@ -191,3 +191,26 @@ def test_errors_raise():
     with pytest.raises(Exception):
         cm.RVEA(population_size=32, max_generations=2, mating=cm.TournamentMating(),
                 print_progress=False).run()
+
+
+@pytest.mark.parametrize("problem,D,M,N", [("DTLZ2", 12, 3, 92), ("DTLZ7", 24, 5, 500), ("DTLZ1", 12, 8, 1000),
+                                           ("DTLZ4", 12, 3, 4096)])
+@pytest.mark.parametrize("graphs", [True, False])
+def test_small_population_fused_equals_staged(problem, D, M, N, graphs):
+    """Populations with 2N <= 8192 run as the fused generation by default;
+    every generation equals the staged path's."""
+    runs = []
+    for fuse in (True, False):
+        a = cm.NSGA3(population_size=N, max_generations=8, problem=getattr(cm, problem)(D, M), seed=17,
+                     print_progress=False, use_graphs=graphs, fuse_small=fuse)
+        a.initialize()
+        gens = []
+        for _ in range(8):
+            a.step()
+            r = a.result()
+            gens.append((r.variables.cpu(), r.objectives.cpu(), r.auxiliary_indices.cpu()))
+        runs.append(gens)
+    for g, (x, y) in enumerate(zip(runs[0], runs[1])):
+        torch.testing.assert_close(x[0], y[0], rtol=0, atol=0, msg=f"variables, generation {g}")
+        torch.testing.assert_close(x[1], y[1], rtol=0, atol=0, msg=f"objectives, generation {g}")
+        torch.testing.assert_close(x[2], y[2], rtol=0, atol=0, msg=f"fronts, generation {g}")
