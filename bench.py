@@ -252,6 +252,66 @@ def batched_measure(args, torch, cm):
     return out
 
 
+# Further workloads of the path (one JSON line each, same timing rules): the
+# small NSGA-III run, RVEA at large D (HBM-bound variation and evaluation) and
+# constrained NSGA-III with ten objectives.
+OTHER_WORKLOADS = {
+    "dtlz2-small": dict(desc="NSGA-III DTLZ2 M=3 D=12 N=92, Das-Dennis H=12 (91 directions), 100-generation run",
+                        algo="NSGA3", problem=("DTLZ2", 12, 3), N=92, T=100, dirs=("dd", 12)),
+    "rvea-large-d": dict(desc="RVEA DTLZ2 M=8 D=131072 N=1024, adaptive two-layer directions, 100-generation run",
+                         algo="RVEA", problem=("DTLZ2", 131072, 8), N=1024, T=100, dirs=None),
+    "c1dtlz1-m10": dict(desc="constrained NSGA-III C1-DTLZ1 M=10 D=14 N=16384, 100-generation run",
+                        algo="NSGA3", problem=("C1DTLZ1", 14, 10), N=16384, T=100, dirs=None),
+}
+
+
+def other_workload(args, torch, cm):
+    w = OTHER_WORKLOADS[args.workload]
+    kind, D, M = w["problem"]
+    kw = {}
+    if w["dirs"]:
+        kw["reference_directions"] = cm.DasDennisDirections(w["dirs"][1])
+    algo = cm.Algorithm(w["algo"], population_size=w["N"], max_generations=w["T"],
+                        problem=getattr(cm, kind)(D, M), seed=args.seed, print_progress=False, **kw)
+    stream = torch.cuda.current_stream()
+    algo.initialize()
+    for _ in range(args.warmup):
+        algo.step()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clocks:
+        for e0, e1 in events:
+            flush.fill_(1)
+            e0.record(stream)
+            algo.step()
+            e1.record(stream)
+        torch.cuda.synchronize()
+    total_ms = sum(e0.elapsed_time(e1) for e0, e1 in events)
+    graph_on, kernels = algo.graph_info
+    out = {"metric": f"{w['algo']} gen/s", "value": args.steps / (total_ms / 1e3), "unit": "gen/s",
+           "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+           "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": w["desc"], "cuda_graph": graph_on, "kernels_per_generation": kernels,
+                      "l2": "flushed (256 MiB write) before every timed generation"},
+           "clocks": clocks.summary()}
+    if args.workload == "rvea-large-d":
+        # streamed bytes of one generation's variation + evaluation: read the two
+        # parents of every child and write the child (8 N D), read the child for
+        # the objectives (4 N D)
+        stages = dict(algo.profile_step())
+        t = stages.get("variation", 0.0) + stages.get("evaluate", 0.0)
+        bytes_ = 12.0 * w["N"] * D
+        hbm, kind_ = _peaks()
+        out["stages_ms"] = stages
+        out["roofline"] = {"kernel": "variation_philox + dtlz_block_rows", "bound": "hbm",
+                           "achieved": bytes_ / (t / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                           "frac": bytes_ / (t / 1e3) / 1e9 / hbm, "peak_source": kind_,
+                           "algorithmic_bytes": bytes_}
+    print(json.dumps(out))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -265,6 +325,7 @@ def main() -> None:
     ap.add_argument("--batch-instances", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--workload", default="dtlz1-n32768", choices=["dtlz1-n32768", *OTHER_WORKLOADS])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -272,6 +333,11 @@ def main() -> None:
     args.warmup = max(args.warmup, 3)
 
     import torch
+    if args.workload != "dtlz1-n32768":
+        import cuda_moea as cm
+        torch.cuda.set_stream(torch.cuda.Stream(0))
+        other_workload(args, torch, cm)
+        return
     import torch.distributed as dist
     import cuda_moea as cm
 

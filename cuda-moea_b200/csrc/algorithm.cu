@@ -66,24 +66,48 @@ int normalize_user_directions(std::vector<float>& v, int M, int count);
 
 namespace {
 
+// Next parents from the survivors: variables row by row (float4 when D is a
+// multiple of 4, several rows per block when rows are short), then
+// objectives, violations and fronts.
 __global__ void gather_next(const float* __restrict__ vars_a, const float* __restrict__ vars_b,
                             SplitPop pop, const int* __restrict__ surv, const int* __restrict__ fronts,
                             int N, int D, int M, float* __restrict__ vars, float* __restrict__ objs,
                             float* __restrict__ cv, int* __restrict__ rank)
 {
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < (long long)N * D) {
-        const int r = (int)(e / D), d = (int)(e % D);
+    const int vec = (D & 3) == 0 ? 4 : 1;
+    const int units = D / vec;                                    // per row
+    const int lanes = units >= (int)blockDim.x ? (int)blockDim.x : (units < 1 ? 1 : units);
+    const int rows_per_block = (int)blockDim.x / lanes;
+    const int sub = (int)threadIdx.x / lanes, lane = (int)threadIdx.x % lanes;
+    for (int r = blockIdx.x * rows_per_block + sub; r < N && sub < rows_per_block;
+         r += gridDim.x * rows_per_block) {
         const int s = surv[r];
-        vars[e] = (s < pop.n_a) ? vars_a[(size_t)s * D + d] : vars_b[(size_t)(s - pop.n_a) * D + d];
+        const float* src = (s < pop.n_a) ? vars_a + (size_t)s * D : vars_b + (size_t)(s - pop.n_a) * D;
+        float* dst = vars + (size_t)r * D;
+        if (vec == 4) {
+            for (int u = lane; u < units; u += lanes)
+                reinterpret_cast<float4*>(dst)[u] = __ldg(reinterpret_cast<const float4*>(src) + u);
+        } else {
+            for (int u = lane; u < units; u += lanes) dst[u] = __ldg(src + u);
+        }
     }
-    if (e < N) {
-        const int r = (int)e;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
         const int s = surv[r];
         for (int m = 0; m < M; ++m) objs[(size_t)m * N + r] = pop.obj(m, s);
         cv[r] = pop.cvv(s);
         if (rank) rank[r] = fronts[s];
     }
+}
+
+// Blocks of gather_next: its rows per block (as the kernel derives them), at
+// most 16 blocks per SM of a 148-SM part, at least enough for the objectives.
+int gather_blocks(int N, int D)
+{
+    const int units = (D % 4 == 0) ? D / 4 : D;
+    const int lanes = std::max(1, std::min(256, units));
+    const int rows_per_block = 256 / lanes;
+    const int blocks = std::max(ceil_div(N, rows_per_block), ceil_div(N, 256));
+    return std::max(1, std::min(148 * 16, blocks));
 }
 
 __global__ void bump_generation(int* gen) { *gen += 1; }
@@ -502,7 +526,7 @@ struct moea_algorithm {
             }
             MOEA_TRY(run_nsga3_select(ws, pop, M, N, refs, H, seed, ideal_last, survivors, nullptr,
                                       assoc_mode(), stream, &sort_pop));
-            gather_next<<<ceil_div((long long)N * D > N ? (long long)N * D : N, 256), 256, 0, stream>>>(
+            gather_next<<<gather_blocks(N, D), 256, 0, stream>>>(
                 vars[P], vars[O], pop, survivors, ws.fronts, N, D, M, vars[X], objs[X], cv[X], rank[X]);
             MOEA_CUDA_TRY(cudaGetLastError());
         } else {

@@ -51,7 +51,7 @@ __global__ void nds_classify(SplitPop pop, int M, uint64_t* __restrict__ key0,
                              int* __restrict__ perm, int* __restrict__ feasible_count)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    bool feasible_class = false;
+    bool feasible_class = false, infeasible2 = false, infeasible3 = false;
     if (i < pop.n) {
         const float cv = pop.cvv(i);
         uint32_t cls, val = 0;
@@ -67,9 +67,17 @@ __global__ void nds_classify(SplitPop pop, int M, uint64_t* __restrict__ key0,
         key0[i] = ((uint64_t)cls << 32) | val;
         perm[i] = i;
         feasible_class = cls <= 1u;
+        infeasible2 = cls == 2u;
+        infeasible3 = cls == 3u;
     }
     const unsigned fm = __ballot_sync(0xFFFFFFFFu, feasible_class);
-    if ((threadIdx.x & 31) == 0 && fm) atomicAdd(feasible_count, __popc(fm));
+    const unsigned m2 = __ballot_sync(0xFFFFFFFFu, infeasible2);
+    const unsigned m3 = __ballot_sync(0xFFFFFFFFu, infeasible3);
+    if ((threadIdx.x & 31) == 0) {
+        if (fm) atomicAdd(feasible_count, __popc(fm));
+        if (m2) atomicAdd(feasible_count + 10, __popc(m2));
+        if (m3) atomicAdd(feasible_count + 11, __popc(m3));
+    }
 }
 
 // Key of LSD pass m (m >= 1) for the current order.
@@ -393,7 +401,19 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
     const int twarps = nblocks * wpb;
     const int ngroups = (n + 31) >> 5;
     int len_prev = 0, total = 0, k = 0;
+    // With fewer feasible points than the target, the peel covers the
+    // feasible fronts only; the infeasible fronts follow in closed form
+    // (nds_infeasible_fronts).  Without feasible points there is nothing to peel.
+    const int feasible = counters[0];
+    const bool feasible_only = feasible < target;
     __syncthreads();
+    if (feasible_only && feasible == 0) {
+        if (block == 0 && threadIdx.x == 0) {
+            counters[2] = -1;
+            counters[12] = -1;
+        }
+        return;
+    }
 
     for (;;) {
         for (int g0 = gwarp; g0 < ngroups; g0 += twarps * kInflight) {
@@ -509,11 +529,13 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
         __syncthreads();
         total += ck;
         len_prev = len;
-        if (total >= target || ck == 0) {
+        if (total >= target || ck == 0 || (feasible_only && total >= feasible)) {
             if (block == 0 && threadIdx.x == 0) {
                 counters[2] = k;
                 counters[3] = total;
-                if (ck == 0 && total < target) atomicExch(counters + 6, kDevPeelInconsistent);
+                counters[12] = k;
+                if (ck == 0 && total < (feasible_only ? feasible : target))
+                    atomicExch(counters + 6, kDevPeelInconsistent);
             }
             return;
         }
@@ -530,6 +552,55 @@ nds_peel(const uint32_t* __restrict__ rows, int W, int n, int target, const int*
     peel_body<1>(blockIdx.x, gridDim.x, U, rows, W, n, target, qinfo, blocker, front_sorted, list, counters);
 }
 
+// Run heads among the infeasible class-2 positions (sorted by violation).
+__global__ void nds_infeasible_heads(int n, const int* __restrict__ qinfo, const int* __restrict__ counters,
+                                     int target, int* __restrict__ flags)
+{
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    const int fc = counters[0], n2 = counters[10];
+    int f = 0;
+    if (fc < target && pos >= fc && pos < fc + n2)
+        f = ((uint32_t)qinfo[pos] & ~kInfeasibleBit) == (uint32_t)pos ? 1 : 0;
+    flags[pos] = f;
+}
+
+// Closed-form fronts of the infeasible points when the feasible ones number
+// fewer than the target.  Every infeasible point is dominated by all feasible
+// points, a class-2 point also by every class-2 point of smaller violation,
+// a class-3 point (NaN violation) by the feasible points only.  With F the
+// last feasible front (-1 without feasible points): class 3 forms front F + 1
+// together with the first class-2 run, class-2 run j is front F + 1 + j.  The
+// stop rule of the peel keeps the fronts up to the first whose cumulative
+// count reaches the target: run j (j > 0) is kept when n3 + start_j < target.
+// rank[pos] = inclusive count of run heads up to pos.
+__global__ void nds_infeasible_fronts(int n, const int* __restrict__ qinfo, const int* __restrict__ rank,
+                                      int* counters, int target, int* __restrict__ front_sorted)
+{
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    const int fc = counters[0], n2 = counters[10], n3 = counters[11];
+    if (fc >= target) return;
+    const int F1 = counters[12] + 1;
+    if (pos < n && pos >= fc) {
+        if (pos < fc + n2) {
+            const int j = rank[pos] - 1;
+            const int start = (int)((uint32_t)qinfo[pos] & ~kInfeasibleBit);
+            if (j == 0 || n3 + start < target) front_sorted[pos] = F1 + j;
+        } else {
+            front_sorted[pos] = F1;
+        }
+    }
+    if (pos == 0) {
+        int last = F1;
+        if (n2 > 0) {
+            int p = target - n3 - 1;
+            p = p < fc ? fc : (p > fc + n2 - 1 ? fc + n2 - 1 : p);
+            last = F1 + rank[p] - 1;
+        }
+        counters[2] = last;
+    }
+}
+
 __global__ void nds_scatter_fronts(int n, const int* __restrict__ perm,
                                    const int* __restrict__ front_sorted, int* __restrict__ fronts)
 {
@@ -541,6 +612,7 @@ __global__ void nds_reset_counters(int* counters)
 {
     if (threadIdx.x < 4) counters[threadIdx.x] = 0;
     if (threadIdx.x == 4) counters[4] = 0;
+    if (threadIdx.x >= 10 && threadIdx.x <= 12) counters[threadIdx.x] = 0;
 }
 
 template <int M>
@@ -996,6 +1068,10 @@ int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_f
         MOEA_CUDA_TRY(cudaLaunchKernelExC(&cfg, (const void*)nds_peel, args));
     }
 
+    // infeasible fronts in closed form (no work when the feasible points suffice)
+    nds_infeasible_heads<<<G, T, 0, stream>>>(n, qinfo, ws.counters, target, ws.head);
+    MOEA_CUDA_TRY(cub::DeviceScan::InclusiveSum(ws.cub_tmp, tmp, ws.head, ws.run_start, n, stream));
+    nds_infeasible_fronts<<<G, T, 0, stream>>>(n, qinfo, ws.run_start, ws.counters, target, ws.front_sorted);
     nds_scatter_fronts<<<G, T, 0, stream>>>(n, perm, ws.front_sorted, fronts);
     MOEA_CUDA_TRY(cudaGetLastError());
     stage_mark("ndsort.peel", stream);

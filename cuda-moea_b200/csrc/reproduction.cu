@@ -158,7 +158,8 @@ __global__ void mating_philox(const float* __restrict__ cv, const int* __restric
 
 // SBX + PM for pair element e = p*D + d: one Philox block drives the SBX
 // draws (u1, u2, sign, copy), a second one the mutation draws of both children.
-__device__ __forceinline__ void variation_element(long long e, const float* __restrict__ parents,
+__device__ __forceinline__ void variation_element(long long e, int p, int d,
+                                                  const float* __restrict__ parents,
                                                   const int* __restrict__ pidx,
                                                   const float* __restrict__ bounds,
                                                   float* __restrict__ off, int pairs, int D,
@@ -166,7 +167,6 @@ __device__ __forceinline__ void variation_element(long long e, const float* __re
                                                   int mutate, float eta_m, float pm_prob,
                                                   uint64_t seed, uint32_t gen)
 {
-    const int p = (int)(e / D), d = (int)(e % D);
     const float lo = bounds[2 * d], hi = bounds[2 * d + 1];
     const int ca = 2 * p, cb = ca + 1;
     float c1, c2;
@@ -203,10 +203,18 @@ __global__ void variation_philox(const float* __restrict__ parents, const int* _
     const uint32_t gen = d_gen ? (uint32_t)*d_gen : gen_host;
     const float eta_c = annealed_eta(sbx_eta0, sbx_eta1, (int)gen, total);
     const float eta_m = annealed_eta(pm_eta0, pm_eta1, (int)gen, total);
+    if (count <= 0x7FFFFFFFll) {  // 32-bit row/column split
+        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < (int)count; e += gridDim.x * blockDim.x) {
+            const int p = e / D;
+            variation_element(e, p, e - p * D, parents, pidx, bounds, off, pairs, D, eta_c, sbx_prob, copy_prob,
+                              mutate, eta_m, pm_prob, seed, gen);
+        }
+        return;
+    }
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < count;
          e += (long long)gridDim.x * blockDim.x)
-        variation_element(e, parents, pidx, bounds, off, pairs, D, eta_c, sbx_prob, copy_prob, mutate,
-                          eta_m, pm_prob, seed, gen);
+        variation_element(e, (int)(e / D), (int)(e % D), parents, pidx, bounds, off, pairs, D, eta_c, sbx_prob,
+                          copy_prob, mutate, eta_m, pm_prob, seed, gen);
 }
 
 // ---- fused batch: mating then variation of every instance (blockIdx.y) ----
@@ -226,10 +234,11 @@ __global__ void fused_variation(const BatchInst* __restrict__ insts, const int* 
     const uint32_t gen = (uint32_t)*I.d_gen;
     const float eta_c = annealed_eta(I.sbx_eta0, I.sbx_eta1, (int)gen, I.T);
     const float eta_m = annealed_eta(I.pm_eta0, I.pm_eta1, (int)gen, I.T);
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < count;
-         e += (long long)gridDim.x * blockDim.x)
-        variation_element(e, I.varsP, I.pidx, I.bounds, I.varsO, pairs, I.D, eta_c, I.sbx_prob, I.sbx_copy,
-                          I.mutate, eta_m, I.pm_prob, I.seed, gen);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < (int)count; e += gridDim.x * blockDim.x) {
+        const int p = e / I.D;  // fused instances hold at most 4096 x 263 elements
+        variation_element(e, p, e - p * I.D, I.varsP, I.pidx, I.bounds, I.varsO, pairs, I.D, eta_c, I.sbx_prob,
+                          I.sbx_copy, I.mutate, eta_m, I.pm_prob, I.seed, gen);
+    }
 }
 
 __global__ void rng_blocks_kernel(uint64_t seed, uint32_t gen, uint32_t tag, long long count,

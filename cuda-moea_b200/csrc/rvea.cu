@@ -219,26 +219,33 @@ __global__ void elite_select(const int* __restrict__ first_vals, const int* __re
 }
 
 // Next population: active rows gathered, the rest sentinel rows.
+// Next parents: survivor rows of the variables (one row per block iteration,
+// float4 when D is a multiple of 4), then objectives and violations; rows at
+// or beyond `active` get the sentinels.
 __global__ void rvea_update(SplitPop pop, const float* __restrict__ vars_a,
                             const float* __restrict__ vars_b, const int* __restrict__ survivors,
                             const int* __restrict__ d_active, int N, int D, int M,
                             float* __restrict__ vars, float* __restrict__ objs,
                             float* __restrict__ cv)
 {
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int active = *d_active;
-    if (e < (long long)N * D) {
-        const int r = (int)(e / D), d = (int)(e % D);
-        float v;
+    for (int r = blockIdx.x; r < N; r += gridDim.x) {
+        float* dst = vars + (size_t)r * D;
         if (r < active) {
             const int s = survivors[r];
-            v = (s < pop.n_a) ? vars_a[(size_t)s * D + d] : vars_b[(size_t)(s - pop.n_a) * D + d];
+            const float* src = (s < pop.n_a) ? vars_a + (size_t)s * D : vars_b + (size_t)(s - pop.n_a) * D;
+            if ((D & 3) == 0) {
+                const float4* s4 = reinterpret_cast<const float4*>(src);
+                float4* d4 = reinterpret_cast<float4*>(dst);
+                for (int d = threadIdx.x; d < (D >> 2); d += blockDim.x) d4[d] = __ldg(s4 + d);
+            } else {
+                for (int d = threadIdx.x; d < D; d += blockDim.x) dst[d] = __ldg(src + d);
+            }
         } else {
-            v = CUDART_NAN_F;
+            for (int d = threadIdx.x; d < D; d += blockDim.x) dst[d] = CUDART_NAN_F;
         }
-        vars[e] = v;
     }
-    if (e < N) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N; e += gridDim.x * blockDim.x) {
         const int r = (int)e;
         if (r < active) {
             const int s = survivors[r];
@@ -403,9 +410,8 @@ int run_rvea_update(const SplitPop& pop, const float* vars_a, const float* vars_
                     const int* survivors, const int* d_active, int N, int D, int M, float* vars,
                     float* objs, float* cv, cudaStream_t s)
 {
-    const long long count = (long long)N * D > N ? (long long)N * D : N;
-    rvea_update<<<(int)((count + 255) / 256), 256, 0, s>>>(pop, vars_a, vars_b, survivors, d_active,
-                                                           N, D, M, vars, objs, cv);
+    const int blocks = N < 148 * 16 ? (N > 0 ? N : 1) : 148 * 16;
+    rvea_update<<<blocks, 256, 0, s>>>(pop, vars_a, vars_b, survivors, d_active, N, D, M, vars, objs, cv);
     MOEA_CUDA_TRY(cudaGetLastError());
     return MOEA_OK;
 }

@@ -64,13 +64,21 @@ def _cv(rng, n, mode):
         cv[rng.integers(0, n, 3)] = np.nan
     if mode == "negzero":
         cv[rng.integers(0, n, 5)] = -0.0
+    if mode in ("mostly_infeasible", "all_infeasible"):
+        # distinct and repeated violations: one front per violation value
+        share = 0.9 if mode == "mostly_infeasible" else 1.0
+        cv = np.where(rng.random(n) < share, rng.integers(1, n // 3 + 2, n).astype(np.float32) * 0.125, 0.0)
+        cv = cv.astype(np.float32)
+        cv[rng.integers(0, n, 4)] = np.nan
     return cv
 
 
 CASES = [(1, 64, "uniform", "feasible"), (2, 184, "ties", "mixed"), (3, 184, "uniform", "feasible"),
          (3, 2048, "dtlz1", "feasible"), (3, 2048, "ties", "mixed"), (3, 4097, "correlated", "feasible"),
          (5, 1500, "ties", "nan"), (8, 1024, "uniform", "mixed"), (10, 3000, "uniform", "negzero"),
-         (16, 700, "ties", "feasible"), (3, 8, "uniform", "feasible"), (3, 33, "ties", "mixed")]
+         (16, 700, "ties", "feasible"), (3, 8, "uniform", "feasible"), (3, 33, "ties", "mixed"),
+         (3, 4096, "uniform", "mostly_infeasible"), (10, 3000, "ties", "all_infeasible"),
+         (3, 16000, "dtlz1", "mostly_infeasible"), (2, 97, "uniform", "all_infeasible")]
 
 
 @pytest.mark.parametrize("M,n,kind,cvmode", CASES)
