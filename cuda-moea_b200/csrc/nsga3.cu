@@ -229,11 +229,9 @@ __device__ __forceinline__ double warp_sum_d(double v)
     return v;
 }
 
-// Intercepts from the extreme points: one-sided Jacobi SVD in FP64 of the
-// matrix whose row r is extreme point r, pseudo-inverse applied to the ones
-// vector with singular values <= 1e-5 dropped, and the reference's
-// ill-conditioning tests and row-maximum fallback
-// (normalization.cu:739-856, 1302-1394).  Run by one block of 256 threads.
+// Reciprocal intercepts from the extreme points s_ext (and the per-objective
+// maxima s_max for the fallback), by all threads of a block; the Jacobi
+// sweeps run in warp 0 with lane r holding row r.
 template <int M>
 __device__ __forceinline__ void norm_solve(const float* __restrict__ nds, int nds_stride,
                                            const int* s_ext, const float* s_max,
