@@ -73,7 +73,8 @@ void free_all(Workspace& ws)
                     ws.norm_part_idx, ws.rcp_b, ws.extreme, ws.ideal_tmp, ws.assoc_best,
                     ws.assoc_idx, ws.assoc_dist, ws.rho, ws.sel_vals[0], ws.sel_vals[1],
                     ws.rank, ws.selected, ws.flags, ws.offset_dev, ws.cub_tmp, ws.tree_dirs,
-                    ws.tree_order, ws.tree_center, ws.dir_delta, ws.chunk_keys, ws.chunk_bits};
+                    ws.tree_order, ws.tree_center, ws.dir_delta, ws.chunk_keys, ws.chunk_bits,
+                    ws.scalar_d};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     ws = Workspace{};
@@ -121,6 +122,7 @@ int workspace_init(Workspace& ws, int device, int n_max, int m_max, int h_max)
     A(ws.rank, n); A(ws.selected, n); A(ws.flags, n);
     A(ws.offset_dev, 1);
     A(ws.dir_delta, 1);
+    A(ws.scalar_d, 1);
 #undef A
     if (st == MOEA_OK) {
         ws.cub_bytes = cub_temp_bytes_needed(n_max);

@@ -115,6 +115,7 @@ struct Workspace {
     float* tree_sin = nullptr;      // (nodes)
     int2* tree_link = nullptr;      // (nodes)
     float* dir_delta = nullptr;     // (1) max | |r|^2 - 1 | of the last scanned directions
+    double* scalar_d = nullptr;     // (1) FP64 result word (IGD mean)
 
     // --- CUB temporary storage ---
     void* cub_tmp = nullptr;

@@ -9,6 +9,7 @@ import torch  # noqa: F401  -- CUDA tensors of the results
 
 from .algorithm import Algorithm, AlgorithmBuilder, NSGA3, Population, RVEA, Result
 from .batch import Batch
+from . import metrics
 from . import problem as _problem
 from .problem import *  # noqa: F401,F403
 from ._specs import (

@@ -145,6 +145,16 @@ moea_status moea_nsga3_select(moea_workspace* ws, const float* d_mix_cv,
                               int* d_survivors, int* d_survivor_fronts, int* d_sizes,
                               int assoc_mode, void* stream);
 
+/* Inverted generational distance in FP64: d_objs (M,n) objective-major
+ * approximation, d_ref (r,M) row-major FP64 reference front.  Rows with a
+ * non-finite objective are dropped; with filter_nondominated only the
+ * non-dominated rows count.  d_min_dist (r) receives each reference point's
+ * distance to its nearest kept row, *h_igd their mean (synchronises the
+ * stream).  Replaces igd / nondominated_mask of the reference's evaluation
+ * tooling (tests/evaluation/metrics/igd.py:8-47). */
+moea_status moea_igd(moea_workspace* ws, const float* d_objs, int n, int M, const double* d_ref, int r,
+                     int filter_nondominated, double* d_min_dist, double* h_igd, void* stream);
+
 /* Optional CV quantisation (nat/src/selection/nsga3/kernels/cv_quantization.cu:65). */
 moea_status moea_quantize_cv(const float* d_cv, float* d_out, int n, float eps_feas,
                              float clip_upper, float log_alpha, int bins, void* stream);
