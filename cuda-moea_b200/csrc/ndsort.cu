@@ -41,6 +41,9 @@ namespace {
 constexpr int kQB = 128;      // sorted positions (dominatees) per tile CTA
 constexpr int kTileThreads = 256;
 constexpr int kPeelThreads = 1024;
+constexpr int kScanQueue = 1024;   // rows per CTA and front for the chunked scan
+constexpr int kScanChunk = 256;    // words per chunk (8 per lane)
+constexpr int kFreeBuf = 2048;     // next-front points buffered per CTA
 constexpr uint32_t kInfeasibleBit = 0x80000000u;
 
 // ---------------------------------------------------------------------------
@@ -383,6 +386,24 @@ __device__ bool grid_barrier(int* counters, unsigned nblocks)
 // may point to global or to shared memory.  kInflight groups of 32 points are
 // examined per round by one warp: their blockers and probe words are loaded
 // before any of them is examined.
+// Appends the lanes with is_free to the CTA's buffer of the next front (one
+// shared atomic per warp); lanes beyond the buffer append to the global list.
+__device__ __forceinline__ void peel_append(bool is_free, int q, int k, int lane, int* s_free, int* s_nfree,
+                                            int* list, int* front_sorted, int* counters)
+{
+    const unsigned fm = __ballot_sync(0xFFFFFFFFu, is_free);
+    if (!fm) return;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(s_nfree, __popc(fm));
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (is_free) {
+        const int pos = base + __popc(fm & ((1u << lane) - 1u));
+        if (pos < kFreeBuf) s_free[pos] = q;
+        else list[atomicAdd(counters + 1, 1)] = q;
+        front_sorted[q] = k;
+    }
+}
+
 template <int kInflight>
 __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
                                           const uint32_t* __restrict__ rows, int W, int n, int target,
@@ -391,6 +412,18 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
                                           int* counters)
 {
     __shared__ int s_len;
+    // rows whose probe did not resolve them: scanned by the whole CTA in
+    // chunks of kScanChunk words after the groups of the front
+    __shared__ int s_nscan, s_ntask;
+    __shared__ int s_sq[kScanQueue], s_sw[kScanQueue], s_found[kScanQueue], s_cp[kScanQueue];
+    // points of the next front found by this CTA, appended to the global list
+    // with one atomic per CTA and front (directly when the buffer is full)
+    __shared__ int s_free[kFreeBuf];
+    __shared__ int s_nfree, s_base;
+    if (threadIdx.x == 0) {
+        s_nscan = 0;
+        s_nfree = 0;
+    }
     for (int w = threadIdx.x; w < W; w += blockDim.x) {
         const int lo = w * 32;
         U[w] = (lo + 32 <= n) ? 0xFFFFFFFFu : (lo >= n ? 0u : ((1u << (n - lo)) - 1u));
@@ -472,8 +505,17 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
                         }
                     }
                 }
-                // rows not resolved by the probe: the whole warp scans each of
-                // them downwards, 8 coalesced words per lane in flight
+                // rows not resolved by the probe go to the CTA's scan queue;
+                // when it is full the whole warp scans each of them
+                // downwards, 8 coalesced words per lane in flight
+                if (need) {
+                    const int slot = atomicAdd(&s_nscan, 1);
+                    if (slot < kScanQueue) {
+                        s_sq[slot] = qv[u];
+                        s_sw[slot] = start_w;
+                        need = false;
+                    }
+                }
                 unsigned needm = __ballot_sync(0xFFFFFFFFu, need);
                 while (needm) {
                     const int L = __ffs(needm) - 1;
@@ -505,17 +547,83 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
                         else is_free = true;
                     }
                 }
-                const unsigned fm = __ballot_sync(0xFFFFFFFFu, is_free);
-                if (fm) {
-                    int base = 0;
-                    if (lane == 0) base = atomicAdd(counters + 1, __popc(fm));
-                    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-                    if (is_free) {
-                        list[base + __popc(fm & ((1u << lane) - 1u))] = q;
-                        front_sorted[q] = k;
+                peel_append(is_free, q, k, lane, s_free, &s_nfree, list, front_sorted, counters);
+            }
+        }
+        __syncthreads();
+        const int nscan = min(s_nscan, kScanQueue);
+        if (nscan > 0) {
+            // chunks of the queued rows: row s covers words sw[s]..0 in
+            // chunks of kScanChunk from the top; cp[s] = first chunk of row s
+            if (warp == 0) {
+                int base = 0;
+                for (int s0 = 0; s0 < nscan; s0 += 32) {
+                    const int sidx = s0 + lane;
+                    const int c = (sidx < nscan) ? s_sw[sidx] / kScanChunk + 1 : 0;
+                    int incl = c;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int tv = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                        if (lane >= o) incl += tv;
+                    }
+                    if (sidx < nscan) {
+                        s_cp[sidx] = base + incl - c;
+                        s_found[sidx] = -1;
+                    }
+                    base += __shfl_sync(0xFFFFFFFFu, incl, 31);
+                }
+                if (lane == 0) s_ntask = base;
+            }
+            __syncthreads();
+            const int ntask = s_ntask;
+            for (int task = warp; task < ntask; task += wpb) {
+                int lo = 0, hi = nscan;  // last row with cp <= task
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s_cp[mid] <= task) lo = mid; else hi = mid;
+                }
+                const int top = s_sw[lo] - (task - s_cp[lo]) * kScanChunk;
+                const uint32_t* row = rows + (size_t)s_sq[lo] * W;
+                uint32_t acc[kScanChunk / 32];
+#pragma unroll
+                for (int i = 0; i < kScanChunk / 32; ++i) {
+                    const int w = top - lane - 32 * i;
+                    acc[i] = (w >= 0 && w > top - kScanChunk) ? (__ldg(row + w) & U[w]) : 0u;
+                }
+#pragma unroll
+                for (int i = 0; i < kScanChunk / 32; ++i) {
+                    const unsigned nz = __ballot_sync(0xFFFFFFFFu, acc[i] != 0u);
+                    if (nz) {
+                        const int src = __ffs(nz) - 1;
+                        const uint32_t bb = __shfl_sync(0xFFFFFFFFu, acc[i], src);
+                        if (lane == 0) atomicMax(s_found + lo, (top - src - 32 * i) * 32 + (31 - __clz(bb)));
+                        break;
                     }
                 }
             }
+            __syncthreads();
+            // highest unassigned dominator found: new blocker; none: free
+            for (int s0 = 0; s0 < nscan; s0 += blockDim.x) {
+                const int sidx = s0 + threadIdx.x;
+                bool is_free = false;
+                int q = 0;
+                if (sidx < nscan) {
+                    q = s_sq[sidx];
+                    const int f = s_found[sidx];
+                    if (f >= 0) blocker[q] = f;
+                    else is_free = true;
+                }
+                peel_append(is_free, q, k, lane, s_free, &s_nfree, list, front_sorted, counters);
+            }
+        }
+        __syncthreads();
+        const int nfree = min(s_nfree, kFreeBuf);
+        if (threadIdx.x == 0) s_base = nfree ? atomicAdd(counters + 1, nfree) : 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < nfree; i += blockDim.x) list[s_base + i] = s_free[i];
+        if (threadIdx.x == 0) {  // read again only after the barrier below
+            s_nscan = 0;
+            s_nfree = 0;
         }
         if (!grid_barrier(counters, (unsigned)nblocks)) return;
         if (threadIdx.x == 0) s_len = *((volatile int*)counters + 9);
