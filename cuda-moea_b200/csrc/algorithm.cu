@@ -359,9 +359,10 @@ struct moea_algorithm {
         if (cfg.mutation && (cfg.pm_eta_initial <= 0.0f || cfg.pm_eta_final <= 0.0f ||
                              cfg.pm_probability < 0.0f || cfg.pm_probability > 1.0f))
             return set_error(MOEA_ERR_INVALID_ARGUMENT, "Invalid polynomial-mutation configuration");
-        if (cfg.association_mode != MOEA_ASSOC_TREE && cfg.association_mode != MOEA_ASSOC_SCAN)
-            return set_error(MOEA_ERR_INVALID_ARGUMENT, "association_mode must be %d or %d", MOEA_ASSOC_TREE,
-                             MOEA_ASSOC_SCAN);
+        if (cfg.association_mode != MOEA_ASSOC_TREE && cfg.association_mode != MOEA_ASSOC_SCAN &&
+            cfg.association_mode != MOEA_ASSOC_TENSOR)
+            return set_error(MOEA_ERR_INVALID_ARGUMENT, "association_mode must be %d, %d or %d", MOEA_ASSOC_TREE,
+                             MOEA_ASSOC_SCAN, MOEA_ASSOC_TENSOR);
         if (cfg.mating == MOEA_MATING_CALLBACK && !cfg.mate)
             return set_error(MOEA_ERR_INVALID_ARGUMENT, "callback mating without a function");
         // only the NSGA-III selector provides ranks (mating_selection.cu:80-86)
@@ -437,6 +438,9 @@ struct moea_algorithm {
         ws_ready = true;
         if (nsga3() && assoc_mode() == MOEA_ASSOC_TREE)
             MOEA_TRY(prepare_direction_tree(ws, refs, nullptr, M, H, stream));
+        if (nsga3() && (assoc_mode() == MOEA_ASSOC_TENSOR ||
+                        (assoc_mode() == MOEA_ASSOC_TREE && tensor_preferred(M, 2 * N, H))))
+            MOEA_TRY(prepare_tensor_directions(ws, refs, M, H, stream));
         if (!init_pop.empty()) {
             for (int r = 0; r < N; ++r)
                 for (int d = 0; d < D; ++d) {

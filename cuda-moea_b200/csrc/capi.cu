@@ -74,7 +74,7 @@ void free_all(Workspace& ws)
                     ws.assoc_idx, ws.assoc_dist, ws.rho, ws.sel_vals[0], ws.sel_vals[1],
                     ws.rank, ws.selected, ws.flags, ws.offset_dev, ws.cub_tmp, ws.tree_dirs,
                     ws.tree_order, ws.tree_center, ws.dir_delta, ws.chunk_keys, ws.chunk_bits,
-                    ws.scalar_d};
+                    ws.scalar_d, ws.tc_dirs, ws.tc_rowmax};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     ws = Workspace{};
@@ -151,6 +151,8 @@ int workspace_check_status(Workspace& ws, cudaStream_t stream)
         cudaMemcpy(ws.counters + 6, &zero, sizeof(int), cudaMemcpyHostToDevice);
         if (st == kDevBarrierTimeout)
             return set_error(MOEA_ERR_DEVICE_TIMEOUT, "front peeling: grid barrier timed out");
+        if (st == kDevTensorTimeout)
+            return set_error(MOEA_ERR_DEVICE_TIMEOUT, "association: tensor-core wait timed out");
         return set_error(MOEA_ERR_CUDA, "front peeling: inconsistent dominance relation (status %d)", st);
     }
     return MOEA_OK;
@@ -254,10 +256,14 @@ moea_status moea_associate(moea_workspace* w, const float* d_x, const float* d_r
     if (n == 0) return MOEA_OK;
     Workspace& ws = w->ws;
     if (mode == MOEA_ASSOC_TREE) MOEA_TRY(prepare_direction_tree(ws, d_refs, nullptr, M, H, S(stream)));
+    const bool tensor = mode == MOEA_ASSOC_TENSOR || (mode == MOEA_ASSOC_TREE && tensor_preferred(M, n, H));
+    if (tensor) MOEA_TRY(prepare_tensor_directions(ws, d_refs, M, H, S(stream)));
     int hs[4] = {0, n, 0, n};
     MOEA_CUDA_TRY(cudaMemcpyAsync(ws.sizes + 4, &hs[3], sizeof(int), cudaMemcpyHostToDevice, S(stream)));
-    return run_associate(ws, d_x, n, nullptr, d_refs, M, ws.sizes + 4, n, H, d_idx, d_dist, mode,
-                         S(stream));
+    MOEA_TRY(run_associate(ws, d_x, n, nullptr, d_refs, M, ws.sizes + 4, n, H, d_idx, d_dist, mode,
+                           S(stream)));
+    if (tensor) return workspace_check_status(ws, S(stream));
+    return MOEA_OK;
 }
 
 moea_status moea_niching(moea_workspace* w, uint64_t seed, uint64_t* h_offset,
@@ -289,6 +295,8 @@ moea_status moea_nsga3_select(moea_workspace* w, const float* d_mix_cv, const fl
         N < 1 || 2 * N > ws.n_max || M < 1 || M > ws.m_max || H < 1 || H > ws.h_max)
         return set_error(MOEA_ERR_INVALID_ARGUMENT, "nsga3_select: bad arguments");
     if (assoc_mode == MOEA_ASSOC_TREE) MOEA_TRY(prepare_direction_tree(ws, d_refs, nullptr, M, H, S(stream)));
+    if (assoc_mode == MOEA_ASSOC_TENSOR || (assoc_mode == MOEA_ASSOC_TREE && tensor_preferred(M, 2 * N, H)))
+        MOEA_TRY(prepare_tensor_directions(ws, d_refs, M, H, S(stream)));
     unsigned long long off = *h_offset;
     MOEA_CUDA_TRY(cudaMemcpyAsync(ws.offset_dev, &off, sizeof(off), cudaMemcpyHostToDevice, S(stream)));
     SplitPop pop{d_mix_objs, d_mix_objs + N, d_mix_cv, d_mix_cv + N, 2 * N, 2 * N, N, 2 * N};

@@ -126,6 +126,7 @@ enum DeviceStatus : int {
     kDevOk = 0,
     kDevBarrierTimeout = 1,
     kDevPeelInconsistent = 2,
+    kDevTensorTimeout = 3,      // a wait of the tensor-core association ran out
 };
 
 }  // namespace moea

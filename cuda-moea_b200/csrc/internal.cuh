@@ -115,6 +115,15 @@ struct Workspace {
     float* tree_sin = nullptr;      // (nodes)
     int2* tree_link = nullptr;      // (nodes)
     float* dir_delta = nullptr;     // (1) max | |r|^2 - 1 | of the last scanned directions
+
+    // --- split TF32 operand of the directions for the tensor-core association ---
+    // Valid for the directions at tc_src (M = tc_M, H = tc_H) until prepared again.
+    const float* tc_src = nullptr;
+    int tc_M = 0, tc_H = 0;
+    size_t tc_cap = 0;              // floats allocated at tc_dirs
+    float* tc_dirs = nullptr;       // tiles of 128 directions in the MMA's shared-memory image,
+                                    // then one float: max | |r|^2 - 1 | of the directions
+    unsigned* tc_rowmax = nullptr;  // (n_max) largest |x.r_j| estimate per point (FP32 bits)
     double* scalar_d = nullptr;     // (1) FP64 result word (IGD mean)
 
     // --- CUB temporary storage ---
@@ -137,7 +146,44 @@ int run_extract(Workspace& ws, const int* fronts, int n, const int* d_max_front,
 int run_normalize_split(Workspace& ws, const SplitPop& pop, const int* nds_gidx,
                         const int* sizes, const float* ideal, int M, cudaStream_t stream);
 
-// mode MOEA_ASSOC_TREE needs prepare_direction_tree for these refs first.
+// Margin of the dot^2 candidate filter of the association for a point with
+// |x|^2 = xx.  For directions with | |r|^2 - 1 | <= delta, the reference's
+// FP32 distance (association.cu:139-170) differs from xx - dot^2 by at most
+// about (4M+5) 2^-24 xx plus xx (1 + delta) delta; the filter uses
+// (16M+64) 2^-24 xx + 2.5 delta xx.  Directions far from unit length
+// (delta > 1e-3) and non-finite points get an infinite margin: every
+// direction is re-scored.
+__device__ __forceinline__ float assoc_margin(int M, float xx, float delta)
+{
+    const float kEps = 5.9604645e-08f;  // 2^-24
+    float margin = xx * ((16.0f * M + 64.0f) * kEps + 2.5f * delta) + 1e-35f;
+    if (!isfinite(xx) || !(delta <= 1e-3f)) margin = INFINITY;
+    return margin;
+}
+
+// max_j | |r_j|^2 - 1 | of the directions (M,H) in FP64, rounded up to FP32.
+int run_dir_delta(const float* refs, int M, int H, float* out, cudaStream_t stream);
+
+// Packed (d2 bits, direction) minima of the association merged across
+// direction ranges: reset to "none", then unpacked into idx/dist.
+int run_assoc_reset(unsigned long long* best, int n_cap, cudaStream_t stream);
+int run_assoc_finish(const unsigned long long* best, const int* d_n, int n_cap, int* idx, float* dist,
+                     cudaStream_t stream);
+
+// Tensor-core association (MOEA_ASSOC_TENSOR): split TF32 operand of the
+// directions, built on the device; the association itself.  MOEA_ASSOC_TREE
+// also takes this search for more objectives than the cone tree handles when
+// there are at least kTensorMinPairs point-direction pairs (tensor_preferred)
+// and the operand was prepared.
+constexpr long long kTensorMinPairs = 1ll << 24;
+bool tensor_preferred(int M, int n_cap, int H);
+int prepare_tensor_directions(Workspace& ws, const float* d_refs, int M, int H, cudaStream_t stream);
+bool tensor_directions_ready(const Workspace& ws, const float* d_refs, int M, int H);
+int run_associate_tensor(Workspace& ws, const float* x, int x_stride, const float* scale, const float* refs,
+                         int M, const int* d_n, int n_cap, int H, int* idx, float* dist, cudaStream_t stream);
+
+// mode MOEA_ASSOC_TREE needs prepare_direction_tree for these refs first,
+// mode MOEA_ASSOC_TENSOR prepare_tensor_directions.
 int run_associate(Workspace& ws, const float* x, int x_stride, const float* scale,
                   const float* refs, int M, const int* d_n, int n_cap, int H, int* idx,
                   float* dist, int mode, cudaStream_t stream);

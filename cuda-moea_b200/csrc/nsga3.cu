@@ -418,19 +418,6 @@ struct DirTile {
     static constexpr int kLen = (M <= 4) ? kAssocTile : 512;  // directions per smem tile
 };
 
-// Margin of the dot^2 candidate filter for a point with |x|^2 = xx.  For
-// directions with | |r|^2 - 1 | <= delta, d2 = xx - dot^2 (2 - |r|^2) differs
-// from xx - dot^2 by at most xx (1 + delta) delta, hence the 2.5 delta term.
-// Directions far from unit length (delta > 1e-3) and non-finite points get an
-// infinite margin: every direction is re-scored.
-__device__ __forceinline__ float assoc_margin(int M, float xx, float delta)
-{
-    const float kEps = 5.9604645e-08f;  // 2^-24
-    float margin = xx * ((16.0f * M + 64.0f) * kEps + 2.5f * delta) + 1e-35f;
-    if (!isfinite(xx) || !(delta <= 1e-3f)) margin = INFINITY;
-    return margin;
-}
-
 // delta = max_j | |r_j|^2 - 1 | in FP64, rounded up to FP32 (one block).
 __global__ void dir_delta_kernel(const float* __restrict__ refs, int M, int H, float* __restrict__ out)
 {
@@ -626,8 +613,9 @@ void launch_assoc(const float* x, int x_stride, const float* scale, const float*
 
 constexpr int kTreeWarps = 8;
 constexpr int kTreeMaxDepth = kDirTreeMaxDepth;
-// Above this many objectives the cones prune little and one thread per point
-// over all directions is cheaper than one warp per point over the tree.
+// Above this many objectives the cones prune little: the tensor-core search
+// (large problems) or one thread per point over all directions is cheaper
+// than one warp per point over the tree.
 constexpr int kTreeMaxObjectives = 5;
 
 struct TreeArgs {
@@ -1293,14 +1281,46 @@ int prepare_direction_tree(Workspace& ws, const float* d_refs, const float* h_re
     return MOEA_OK;
 }
 
+bool tensor_preferred(int M, int n_cap, int H)
+{
+    return M > kTreeMaxObjectives && (long long)n_cap * H >= kTensorMinPairs;
+}
+
+int run_dir_delta(const float* refs, int M, int H, float* out, cudaStream_t stream)
+{
+    dir_delta_kernel<<<1, 1024, 0, stream>>>(refs, M, H, out);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+int run_assoc_reset(unsigned long long* best, int n_cap, cudaStream_t stream)
+{
+    assoc_reset<<<ceil_div(n_cap, 256), 256, 0, stream>>>(best, n_cap);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+int run_assoc_finish(const unsigned long long* best, const int* d_n, int n_cap, int* idx, float* dist,
+                     cudaStream_t stream)
+{
+    assoc_finish<<<ceil_div(n_cap, 256), 256, 0, stream>>>(best, d_n, idx, dist);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
 int run_associate(Workspace& ws, const float* x, int x_stride, const float* scale,
                   const float* refs, int M, const int* d_n, int n_cap, int H, int* idx,
                   float* dist, int mode, cudaStream_t stream)
 {
     if (n_cap <= 0) return MOEA_OK;
     if (H <= 0) return set_error(MOEA_ERR_INVALID_ARGUMENT, "associate: no directions");
-    if (mode != MOEA_ASSOC_TREE && mode != MOEA_ASSOC_SCAN)
+    if (mode != MOEA_ASSOC_TREE && mode != MOEA_ASSOC_SCAN && mode != MOEA_ASSOC_TENSOR)
         return set_error(MOEA_ERR_INVALID_ARGUMENT, "associate: mode %d", mode);
+    if (mode == MOEA_ASSOC_TENSOR) {
+        if (!tensor_directions_ready(ws, refs, M, H))
+            return set_error(MOEA_ERR_STATE, "associate: no tensor operand prepared for these directions");
+        return run_associate_tensor(ws, x, x_stride, scale, refs, M, d_n, n_cap, H, idx, dist, stream);
+    }
     if (mode == MOEA_ASSOC_TREE) {
         if (!direction_tree_ready(ws, refs, M, H))
             return set_error(MOEA_ERR_STATE, "associate: no cone tree prepared for these directions");
@@ -1320,7 +1340,11 @@ int run_associate(Workspace& ws, const float* x, int x_stride, const float* scal
             MOEA_CUDA_TRY(cudaGetLastError());
             return MOEA_OK;
         }
-        // a tree deeper than the kernel's stack, or many objectives: scan instead
+        // many objectives: the tensor-core search where it was prepared (the
+        // cones prune little), else -- and for a tree deeper than the
+        // kernel's stack -- the scan
+        if (tensor_preferred(M, n_cap, H) && tensor_directions_ready(ws, refs, M, H))
+            return run_associate_tensor(ws, x, x_stride, scale, refs, M, d_n, n_cap, H, idx, dist, stream);
     }
     dir_delta_kernel<<<1, 1024, 0, stream>>>(refs, M, H, ws.dir_delta);
     assoc_reset<<<ceil_div(n_cap, 256), 256, 0, stream>>>(ws.assoc_best, n_cap);

@@ -81,7 +81,8 @@ class NSGA3EnvironmentSelector(_Spec):
     cv_clip_upper: float = 0.0
     cv_log_alpha: float = 0.0
     feasibility_epsilon: float = 0.0
-    # B200 extension: 0 = cone-tree association search, 1 = full scan (same results)
+    # B200 extension: 0 = cone-tree association search, 1 = full scan, 2 = tensor-core
+    # dots with exact re-score of the candidates (all three give the same results)
     association_mode: int = 0
 
 

@@ -88,8 +88,9 @@ def normalize(ws: Workspace, objs: torch.Tensor, ideal: torch.Tensor):
     return f, rcp, ext
 
 
-ASSOC_TREE = 0  # cone-tree search (default)
-ASSOC_SCAN = 1  # every direction visited
+ASSOC_TREE = 0    # cone-tree search (default)
+ASSOC_SCAN = 1    # every direction visited
+ASSOC_TENSOR = 2  # dots on the tensor cores, exact FP32 re-score of the candidates
 
 
 def associate(ws: Workspace, x: torch.Tensor, refs: torch.Tensor, mode: int = ASSOC_TREE):

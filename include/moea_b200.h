@@ -97,16 +97,24 @@ moea_status moea_ideal_point(moea_workspace* ws, const float* d_objs, int M, int
 moea_status moea_normalize(moea_workspace* ws, float* d_objs, const float* d_ideal, int M,
                            int n, float* d_rcp_b, int* d_extreme, void* stream);
 
-/* Association modes; both give the reference's exact argmin. */
-#define MOEA_ASSOC_TREE 0  /* cone tree over the directions, one warp per point, subtrees
-                              pruned by a conservative bound on dot^2 (default) */
-#define MOEA_ASSOC_SCAN 1  /* every direction visited, FP32 re-score of the dot^2 candidates */
+/* Association modes; all give the reference's exact argmin. */
+#define MOEA_ASSOC_TREE 0    /* cone tree over the directions, one warp per point, subtrees
+                                pruned by a conservative bound on dot^2 (default); above 5
+                                objectives the tensor-core search of MOEA_ASSOC_TENSOR when
+                                points x directions >= 2^24, else the scan */
+#define MOEA_ASSOC_SCAN 1    /* every direction visited, FP32 re-score of the dot^2 candidates */
+#define MOEA_ASSOC_TENSOR 2  /* precision form: the point x direction dots on the tensor cores
+                                (split TF32 operands, FP32 accumulation), FP32 re-score of every
+                                direction within the proven error bound of the best */
 
 /* Association of normalised points d_x (M,n) to directions d_refs (M,H):
  * perpendicular distance with the reference's FP32 formula, ties to the
  * smaller direction index.  mode MOEA_ASSOC_TREE builds the cone tree of
  * d_refs on the host on every call (a read-back that synchronises the
- * stream); the algorithm object builds it once.  Replaces
+ * stream); the algorithm object builds it once.  mode MOEA_ASSOC_TENSOR packs
+ * the split TF32 operand of d_refs on the device on every call (the algorithm
+ * object packs it once) and reports a timed-out tensor-core wait as
+ * MOEA_ERR_DEVICE_TIMEOUT.  Replaces
  * execute_association (nat/src/selection/nsga3/kernels/association.cu:586). */
 moea_status moea_associate(moea_workspace* ws, const float* d_x, const float* d_refs, int M,
                            int n, int H, int* d_idx, float* d_dist, int mode, void* stream);
@@ -291,7 +299,7 @@ typedef struct moea_algorithm_config {
     float sparse_ratio;       /* validated for compatibility; the bitmask path needs no pair buffer */
     int cv_bins;
     float cv_clip_upper, cv_log_alpha, feasibility_epsilon;
-    int association_mode;     /* MOEA_ASSOC_TREE or MOEA_ASSOC_SCAN */
+    int association_mode;     /* MOEA_ASSOC_TREE, MOEA_ASSOC_SCAN or MOEA_ASSOC_TENSOR */
     /* RVEA selector */
     float rvea_alpha;
     /* initial population (N,D) row-major on the host, or NULL */

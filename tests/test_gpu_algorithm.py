@@ -132,7 +132,7 @@ def test_graph_replay_equals_direct_launches(kind):
 @pytest.mark.parametrize("problem,dirs", [("DTLZ1", None), ("DTLZ2", "user_unnormalised")])
 def test_association_modes_give_identical_runs(problem, dirs):
     runs = []
-    for mode in (0, 1):
+    for mode in (0, 1, 2):
         kw = {}
         if dirs == "user_unnormalised":
             d = torch.rand(150, 3, generator=torch.Generator().manual_seed(3)) * 2 + 0.05
@@ -143,8 +143,31 @@ def test_association_modes_give_identical_runs(problem, dirs):
                      print_progress=False, **kw)
         r = a.run()
         runs.append((r.variables.cpu(), r.objectives.cpu()))
-    torch.testing.assert_close(runs[0][0], runs[1][0], rtol=0, atol=0)
-    torch.testing.assert_close(runs[0][1], runs[1][1], rtol=0, atol=0)
+    for other in runs[1:]:
+        torch.testing.assert_close(runs[0][0], other[0], rtol=0, atol=0)
+        torch.testing.assert_close(runs[0][1], other[1], rtol=0, atol=0)
+
+
+def test_many_objective_default_search_equals_scan():
+    """Eight objectives, 6435 directions, 8400 merged points: the default mode
+    takes the tensor-core search there (the cone tree covers M <= 5); every
+    generation equals the full scan's and the explicit tensor mode's."""
+    runs = []
+    for mode in (0, 1, 2):
+        a = cm.NSGA3(population_size=4200, max_generations=6, problem=cm.DTLZ2(17, 8), seed=23,
+                     reference_directions=cm.DasDennisDirections(8), print_progress=False,
+                     environment_selector=cm.NSGA3EnvironmentSelector(association_mode=mode))
+        a.initialize()
+        gens = []
+        for _ in range(6):
+            a.step()
+            r = a.result()
+            gens.append((r.variables.cpu(), r.auxiliary_indices.cpu()))
+        runs.append(gens)
+    for other in runs[1:]:
+        for g, (x, y) in enumerate(zip(runs[0], other)):
+            torch.testing.assert_close(x[0], y[0], rtol=0, atol=0, msg=f"variables, generation {g}")
+            torch.testing.assert_close(x[1], y[1], rtol=0, atol=0, msg=f"fronts, generation {g}")
 
 
 def test_nsga3_dtlz2_quality():

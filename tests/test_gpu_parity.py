@@ -133,7 +133,7 @@ def test_extract_ideal_normalize_associate(st, ws, oracle):
     np.testing.assert_array_equal(dist_g.cpu().numpy(), dist_w)
 
 
-@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1, 2])
 @pytest.mark.parametrize("M,n,H_mode", [(3, 3000, (1, 254)), (3, 500, (1, 12)), (5, 2000, (0, 3000)),
                                         (8, 1500, (0, 900)), (10, 1200, (0, 2000)), (2, 4096, (1, 999))])
 def test_association_bit_exact(st, ws, oracle, M, n, H_mode, mode):
@@ -185,7 +185,7 @@ def test_association_tree_adversarial(st, ws, oracle, M, H, n, kind):
     x[:, 21] = 3e18
     x[1 % M, 22] = np.nan
     idx_w, dist_w = oracle.associate(x, refs)
-    for mode in (0, 1):
+    for mode in (0, 1, 2):
         idx_g, dist_g = st.associate(ws, _t(x), _t(refs), mode)
         np.testing.assert_array_equal(idx_g.cpu().numpy(), idx_w, err_msg=f"mode {mode}")
         np.testing.assert_array_equal(dist_g.cpu().numpy(), dist_w, err_msg=f"mode {mode}")
@@ -193,8 +193,8 @@ def test_association_tree_adversarial(st, ws, oracle, M, H, n, kind):
 
 def test_association_tree_full_size(st, oracle):
     """M=3 with the 32640 Das-Dennis directions of 254 partitions (the bench
-    workload's direction set), 16384 points: tree search == full scan, and a
-    sample against the oracle."""
+    workload's direction set), 16384 points: tree search == tensor-core
+    search == full scan, and a sample against the oracle."""
     rng = np.random.default_rng(32640)
     refs = oracle.reference_directions(1, 254, 3)
     n = 16384
@@ -203,14 +203,55 @@ def test_association_tree_full_size(st, oracle):
     try:
         a_i, a_d = st.associate(w, _t(x), _t(refs), 0)
         b_i, b_d = st.associate(w, _t(x), _t(refs), 1)
+        c_i, c_d = st.associate(w, _t(x), _t(refs), 2)
     finally:
         w.close()
     np.testing.assert_array_equal(a_i.cpu().numpy(), b_i.cpu().numpy())
     np.testing.assert_array_equal(a_d.cpu().numpy(), b_d.cpu().numpy())
+    np.testing.assert_array_equal(c_i.cpu().numpy(), b_i.cpu().numpy())
+    np.testing.assert_array_equal(c_d.cpu().numpy(), b_d.cpu().numpy())
     sample = rng.choice(n, 512, replace=False)
     idx_w, dist_w = oracle.associate(np.ascontiguousarray(x[:, sample]), refs)
     np.testing.assert_array_equal(a_i.cpu().numpy()[sample], idx_w)
     np.testing.assert_array_equal(a_d.cpu().numpy()[sample], dist_w)
+
+
+@pytest.mark.parametrize("M,n,H_mode,kind", [(3, 65536, (1, 254), "dtlz1"), (8, 16000, (1, 8), "uniform"),
+                                             (10, 8192, (1, 6), "uniform"), (5, 20000, (1, 20), "cluster"),
+                                             (3, 129, (1, 15), "uniform"), (16, 4000, (1, 3), "uniform")])
+def test_association_tensor_equals_scan(st, oracle, M, n, H_mode, kind):
+    """The tensor-core association (split TF32 dots, re-score within the error
+    bound) against the FP32 full scan: identical indices and distances,
+    including points on the bisector of two directions (exact ties) and
+    points clustered around one direction; a sample against the oracle."""
+    rng = np.random.default_rng(M * 7 + n)
+    refs = oracle.reference_directions(H_mode[0], H_mode[1], M)
+    H = refs.shape[1]
+    if kind == "dtlz1":
+        x = (rng.random((M, n)) ** 2 * rng.random(n) * 4).astype(np.float32)
+    elif kind == "cluster":
+        c = refs[:, H // 3:H // 3 + 1]
+        x = (c * (1 + rng.random(n)) + 1e-4 * rng.standard_normal((M, n))).astype(np.float32)
+    else:
+        x = (rng.random((M, n)) * rng.random(n) * 2).astype(np.float32)
+    pairs = min(64, n // 4, H - 1)
+    a = rng.integers(0, H - 1, pairs)
+    x[:, :pairs] = refs[:, a] + refs[:, a + 1]          # equidistant from two directions
+    x[:, pairs:2 * pairs] = refs[:, a] * 3.0             # on a direction
+    w = st.Workspace(max_points=n, max_objectives=M, max_directions=H)
+    try:
+        s_i, s_d = st.associate(w, _t(x), _t(refs), 1)
+        t_i, t_d = st.associate(w, _t(x), _t(refs), 2)
+        t2_i, t2_d = st.associate(w, _t(x), _t(refs), 2)
+    finally:
+        w.close()
+    np.testing.assert_array_equal(t_i.cpu().numpy(), s_i.cpu().numpy())
+    np.testing.assert_array_equal(t_d.cpu().numpy(), s_d.cpu().numpy())
+    np.testing.assert_array_equal(t2_i.cpu().numpy(), t_i.cpu().numpy())
+    sample = np.concatenate([np.arange(min(n, 2 * pairs)), rng.choice(n, min(n, 256), replace=False)])
+    idx_w, dist_w = oracle.associate(np.ascontiguousarray(x[:, sample]), refs)
+    np.testing.assert_array_equal(t_i.cpu().numpy()[sample], idx_w)
+    np.testing.assert_array_equal(t_d.cpu().numpy()[sample], dist_w)
 
 
 def test_niching_bit_exact(st, ws, oracle):
@@ -231,7 +272,7 @@ def test_niching_bit_exact(st, ws, oracle):
 @pytest.mark.parametrize("seed,M,N,kind", [(0, 3, 92, "dtlz1"), (1, 3, 1024, "dtlz1"),
                                            (2, 3, 2048, "uniform"), (3, 5, 600, "ties"),
                                            (4, 8, 512, "uniform"), (5, 3, 4096, "correlated")])
-@pytest.mark.parametrize("assoc_mode", [0, 1])
+@pytest.mark.parametrize("assoc_mode", [0, 1, 2])
 def test_nsga3_select_bit_exact(st, ws, oracle, seed, M, N, kind, assoc_mode):
     rng = np.random.default_rng(seed)
     objs = _population(rng, M, 2 * N, kind)
