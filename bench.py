@@ -262,7 +262,50 @@ OTHER_WORKLOADS = {
                          algo="RVEA", problem=("DTLZ2", 131072, 8), N=1024, T=100, dirs=None),
     "c1dtlz1-m10": dict(desc="constrained NSGA-III C1-DTLZ1 M=10 D=14 N=16384, 100-generation run",
                         algo="NSGA3", problem=("C1DTLZ1", 14, 10), N=16384, T=100, dirs=None),
+    # many objectives: the default association is the tensor-core search here
+    "dtlz2-m8": dict(desc="NSGA-III DTLZ2 M=8 D=17 N=6436, Das-Dennis H=8 (6435 directions), 100-generation run",
+                     algo="NSGA3", problem=("DTLZ2", 17, 8), N=6436, T=100, dirs=("dd", 8)),
 }
+
+
+# association searches compared on the same runs (all give identical results)
+ASSOC_FORMS = {0: "cone tree", 1: "FP32 scan", 2: "tensor cores (split TF32, exact re-score)"}
+PRECISION_WORKLOADS = [
+    {"desc": "headline: DTLZ1 M=3 D=7 N=32768, 32640 directions", "problem": "DTLZ1", "D": D_VAR, "M": M_OBJ,
+     "N": N_POP, "partitions": PARTITIONS, "modes": (0, 1, 2)},
+    {"desc": "many objectives: DTLZ2 M=8 D=17 N=6436, 6435 directions", "problem": "DTLZ2", "D": 17, "M": 8,
+     "N": 6436, "partitions": 8, "modes": (1, 2)},
+]
+
+
+def precision_form(torch, cm, seed: int, gens: int = 4):
+    """Association stage time of each search on the same seeded run, and
+    whether the runs stay identical.  At M=3 the cone tree visits about 1% of
+    the directions, so the dense tensor-core contraction does not beat it; above
+    five objectives the default search is the tensor-core one."""
+    out = []
+    for w in PRECISION_WORKLOADS:
+        rec = {"workload": w["desc"], "associate_ms": {}, "identical_runs": True}
+        ref = None
+        for mode in w["modes"]:
+            algo = cm.NSGA3(population_size=w["N"], max_generations=gens + 4, problem=getattr(cm, w["problem"])(w["D"], w["M"]),
+                            reference_directions=cm.DasDennisDirections(w["partitions"]), seed=seed,
+                            print_progress=False,
+                            environment_selector=cm.NSGA3EnvironmentSelector(association_mode=mode))
+            algo.initialize()
+            for _ in range(gens):
+                algo.step()
+            times = [dict(algo.profile_step())["select.associate"] for _ in range(3)]
+            x = algo.population.variables.cpu()
+            rec["associate_ms"][ASSOC_FORMS[mode]] = sorted(times)[1]
+            if ref is None:
+                ref = x
+            elif not torch.equal(ref, x):
+                rec["identical_runs"] = False
+            del algo
+            torch.cuda.empty_cache()
+        out.append(rec)
+    return out
 
 
 def other_workload(args, torch, cm):
@@ -296,6 +339,8 @@ def other_workload(args, torch, cm):
            "config": {"workload": w["desc"], "cuda_graph": graph_on, "kernels_per_generation": kernels,
                       "l2": "flushed (256 MiB write) before every timed generation"},
            "clocks": clocks.summary()}
+    if args.workload == "dtlz2-m8":
+        out["stages_ms"] = dict(algo.profile_step())
     if args.workload == "rvea-large-d":
         # streamed bytes of one generation's variation + evaluation: read the two
         # parents of every child and write the child (8 N D), read the child for
@@ -325,6 +370,7 @@ def main() -> None:
     ap.add_argument("--batch-instances", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-precision", action="store_true", help="skip the association-search comparison")
     ap.add_argument("--workload", default="dtlz1-n32768", choices=["dtlz1-n32768", *OTHER_WORKLOADS])
     args = ap.parse_args()
     if args.impl == "reference":
@@ -352,7 +398,7 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     N = args.population
-    gens = args.warmup + args.steps + 1 + args.steps + 1
+    gens = args.warmup + args.steps + 1 + 3 + args.steps + 1
     algo = cm.NSGA3(population_size=N, max_generations=gens, problem=cm.DTLZ1(D_VAR, M_OBJ),
                     reference_directions=cm.DasDennisDirections(PARTITIONS), seed=replica_seed(args.seed, rank),
                     print_progress=False, device=local)
@@ -391,19 +437,26 @@ def main() -> None:
     h_cv = torch.empty(N, dtype=torch.float32, pin_memory=True)
     ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
-    torch.cuda.synchronize()
-    for e0, e1 in ev2:
+
+    def e2e_step(e0=None, e1=None):
         flush.fill_(1)
-        e0.record(stream)
+        if e0 is not None:
+            e0.record(stream)
         p = algo.population_view()
         p.variables.copy_(h_vars, non_blocking=True)
         algo.step()
         p = algo.population_view()
         h_objs.copy_(p.objectives, non_blocking=True)
         h_cv.copy_(p.constraints, non_blocking=True)
-        e1.record(stream)
+        if e1 is not None:
+            e1.record(stream)
         torch.cuda.synchronize()
         h_vars.copy_(p.variables)
+
+    for _ in range(3):  # untimed warm-up of the host-copy path
+        e2e_step()
+    for e0, e1 in ev2:
+        e2e_step(e0, e1)
     e2e_ms = sum(e0.elapsed_time(e1) for e0, e1 in ev2)
     e2e_value = world * args.steps / (over_ranks(e2e_ms, "max", world, "cuda") / 1000.0)
 
@@ -420,6 +473,10 @@ def main() -> None:
     hbm, peak_kind = _peaks()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms == dom_ms else None
     pair_rate = (n_mix * n_mix) / (dom_ms / 1e3) if dom_ms == dom_ms else None
+
+    precision = None
+    if not args.no_precision:
+        precision = precision_form(torch, cm, replica_seed(args.seed, rank))
 
     batched = None
     if not args.no_batch:
@@ -457,6 +514,7 @@ def main() -> None:
                          "traffic": TILES_DRAM_BYTES if N == N_POP else None,
                          "algorithmic_bytes": dom_bytes, "pair_tests_per_s": pair_rate},
             "cpu_baseline": cpu,
+            "precision_form": precision,
             "batched": batched,
         }
         print(json.dumps(out))
