@@ -75,7 +75,9 @@ struct Workspace {
     int* front_list = nullptr;      // members of each peeled front, front by front
     int* counters = nullptr;        // [0] feasible count, [1] list length, [2] max_front,
                                     // [3] assigned, [4] barrier count, [5] barrier generation,
-                                    // [6] device status, [7..] spare
+                                    // [6] device status, [9] front-list length at the barrier,
+                                    // [10] class-2 count, [11] class-3 count, [12] last feasible
+                                    // front, [13] long runs of equal sort keys
     int peel_grid = 0;              // co-resident CTAs of the peel kernel
     int peel_smem = 0;
     bool peel_single_cta = false;   // peel with one ordinary CTA (instances of a batch)

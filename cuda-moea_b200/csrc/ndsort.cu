@@ -5,11 +5,16 @@
 // Same result (front index per point, -1 past the stop rule, index of the last
 // front), different mechanism:
 //
-//  1. Lexicographic sort of the points by (class, f0 | cv, f1, ..., f_{M-1})
-//     with stable LSD radix passes.  Class 0 = feasible, 1 = feasible with a NaN
-//     objective, 2 = infeasible, 3 = infeasible with NaN violation.  In this
-//     order every dominator of a point lies strictly before it, and a feasible
-//     dominator already satisfies f0 <= q0.
+//  1. Sort of the points by (class, f0 | cv, S) with one 64-bit radix sort,
+//     S the top 30 bits of the order key of the FP32 sum f1 + ... + f_{M-1}.
+//     Class 0 = feasible, 1 = feasible with a NaN objective, 2 = infeasible,
+//     3 = infeasible with NaN violation.  FP32 addition rounds monotonically,
+//     so a feasible dominator p of q has f0(p) <= f0(q) and S(p) <= S(q); runs
+//     of equal keys in class 0 are then ordered lexicographically by
+//     (f1, ..., f_{M-1}, index) (nds_tie_fix, nds_tie_fix_long).  In this
+//     order every dominator of a point lies strictly before it, identical
+//     vectors are adjacent, and a feasible dominator already satisfies
+//     f0 <= q0.
 //  2. For every sorted position q, dup[q] is the first position that cannot
 //     dominate q: the start of q's run of identical objective vectors (class 0),
 //     0 (class 1: nothing dominates it), the start of q's run of equal violation
@@ -50,24 +55,33 @@ constexpr uint32_t kInfeasibleBit = 0x80000000u;
 // 1. classification and lexicographic sort
 // ---------------------------------------------------------------------------
 
-__global__ void nds_classify(SplitPop pop, int M, uint64_t* __restrict__ key0,
+// key0[i] = class << 32 | order key of f0 (class 0) or cv (class 2);
+// skey[i] = class << 62 | that key << 30 | S (class 0), the sort key.
+__global__ void nds_classify(SplitPop pop, int M, uint64_t* __restrict__ key0, uint64_t* __restrict__ skey,
                              int* __restrict__ perm, int* __restrict__ feasible_count)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     bool feasible_class = false, infeasible2 = false, infeasible3 = false;
     if (i < pop.n) {
         const float cv = pop.cvv(i);
-        uint32_t cls, val = 0;
+        uint32_t cls, val = 0, s30 = 0;
         if (cv == 0.0f) {
             bool nan = false;
             for (int m = 0; m < M; ++m) nan |= isnan(pop.obj(m, i));
             cls = nan ? 1u : 0u;
-            if (!nan) val = float_order_key(pop.obj(0, i));
+            if (!nan) {
+                val = float_order_key(pop.obj(0, i));
+                // monotone in every f_m; +inf + -inf (NaN) sorts with +inf sums
+                float sum = 0.0f;
+                for (int m = 1; m < M; ++m) sum = __fadd_rn(sum, pop.obj(m, i));
+                s30 = float_order_key(isnan(sum) ? INFINITY : sum) >> 2;
+            }
         } else {
             cls = isnan(cv) ? 3u : 2u;
             if (cls == 2u) val = float_order_key(cv);
         }
         key0[i] = ((uint64_t)cls << 32) | val;
+        skey[i] = ((uint64_t)cls << 62) | ((uint64_t)val << 30) | s30;
         perm[i] = i;
         feasible_class = cls <= 1u;
         infeasible2 = cls == 2u;
@@ -83,21 +97,128 @@ __global__ void nds_classify(SplitPop pop, int M, uint64_t* __restrict__ key0,
     }
 }
 
-// Key of LSD pass m (m >= 1) for the current order.
-__global__ void nds_gather_key(SplitPop pop, int m, const uint64_t* __restrict__ key0,
-                               const int* __restrict__ perm, uint32_t* __restrict__ key)
+// Total order inside a run of equal sort keys of class 0: lexicographic on
+// the order keys of f1 .. f_{M-1}, then the point index.
+__device__ __forceinline__ bool tie_less(const SplitPop& pop, int M, int a, int b)
 {
-    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
-    if (pos >= pop.n) return;
-    const int pt = perm[pos];
-    key[pos] = ((key0[pt] >> 32) == 0) ? float_order_key(pop.obj(m, pt)) : 0u;
+    for (int m = 1; m < M; ++m) {
+        const uint32_t ka = float_order_key(pop.obj(m, a)), kb = float_order_key(pop.obj(m, b));
+        if (ka != kb) return ka < kb;
+    }
+    return a < b;
 }
 
-__global__ void nds_gather_key0(int n, const uint64_t* __restrict__ key0,
-                                const int* __restrict__ perm, uint64_t* __restrict__ key)
+constexpr int kTieShort = 32;         // runs up to this length: one thread, insertion sort
+constexpr int kTieLongThreads = 1024;
+constexpr int kTieLongCtas = 64;        // CTAs of nds_tie_fix_long, each taking runs in turn
+constexpr int kTieSmemSort = 4096;    // longer runs: bitonic in shared memory up to this size
+
+// One thread per run head of class 0: short runs are sorted in place, longer
+// ones are listed for nds_tie_fix_long.  Runs are disjoint, so the in-place
+// sorts do not race.
+__global__ void nds_tie_fix(SplitPop pop, int M, const uint64_t* __restrict__ skey, int* __restrict__ perm,
+                            int* __restrict__ long_runs, int* __restrict__ n_long)
 {
     const int pos = blockIdx.x * blockDim.x + threadIdx.x;
-    if (pos < n) key[pos] = key0[perm[pos]];
+    const int n = pop.n;
+    if (pos >= n) return;
+    const uint64_t k = skey[pos];
+    if ((k >> 62) != 0u || (pos > 0 && skey[pos - 1] == k)) return;
+    int L = 1;
+    while (L <= kTieShort && pos + L < n && skey[pos + L] == k) ++L;
+    if (L == 1) return;
+    if (L > kTieShort) {
+        long_runs[atomicAdd(n_long, 1)] = pos;
+        return;
+    }
+    int* a = perm + pos;
+    for (int x = 1; x < L; ++x) {
+        const int v = a[x];
+        int y = x - 1;
+        while (y >= 0 && tie_less(pop, M, v, a[y])) {
+            a[y + 1] = a[y];
+            --y;
+        }
+        a[y + 1] = v;
+    }
+}
+
+// Ascending bitonic network over a[0, L) with virtual +inf padding to the
+// power of two P >= L (pairs reaching past L are skipped: +inf already sits
+// last).  Every merge opens with the mirrored comparison, so all blocks sort
+// ascending.  Called by every thread of the CTA.
+__device__ void tie_bitonic(const SplitPop& pop, int M, int* a, int L)
+{
+    int P = 1;
+    while (P < L) P <<= 1;
+    for (int k = 2; k <= P; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int q = threadIdx.x; q < P / 2; q += blockDim.x) {
+                int i, p;
+                if (j == k >> 1) {  // mirror inside the block of k
+                    const int half = k >> 1;
+                    i = (q / half) * k + (q % half);
+                    p = (q / half) * k + (k - 1 - (q % half));
+                } else {
+                    i = (q / j) * 2 * j + (q % j);
+                    p = i + j;
+                }
+                if (p < L) {
+                    const int x = a[i], y = a[p];
+                    if (tie_less(pop, M, y, x)) {
+                        a[i] = y;
+                        a[p] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// One CTA per listed run longer than kTieShort: its length, then a bitonic
+// sort unless the run is already in order (runs of identical vectors are).
+__global__ void __launch_bounds__(kTieLongThreads)
+nds_tie_fix_long(SplitPop pop, int M, const uint64_t* __restrict__ skey, int* __restrict__ perm,
+                 const int* __restrict__ long_runs, const int* __restrict__ n_long)
+{
+    __shared__ int s_arr[kTieSmemSort];
+    __shared__ int s_len, s_unsorted;
+    const int n = pop.n;
+    const int count = *n_long;
+    for (int r = blockIdx.x; r < count; r += gridDim.x) {
+        const int start = long_runs[r];
+        const uint64_t k = skey[start];
+        if (threadIdx.x == 0) {
+            s_len = n - start;
+            s_unsorted = 0;
+        }
+        __syncthreads();
+        for (int base = start; base < n; base += blockDim.x) {
+            const int pos = base + threadIdx.x;
+            if (pos < n && skey[pos] != k) atomicMin(&s_len, pos - start);
+            __syncthreads();
+            const bool found = s_len < n - start;
+            __syncthreads();  // every thread has read s_len before the next atomicMin
+            if (found) break;
+        }
+        const int L = s_len;
+        int* a = perm + start;
+        for (int x = threadIdx.x; x + 1 < L; x += blockDim.x)
+            if (tie_less(pop, M, a[x + 1], a[x])) s_unsorted = 1;
+        __syncthreads();
+        if (s_unsorted) {
+            if (L <= kTieSmemSort) {
+                for (int x = threadIdx.x; x < L; x += blockDim.x) s_arr[x] = a[x];
+                __syncthreads();
+                tie_bitonic(pop, M, s_arr, L);
+                for (int x = threadIdx.x; x < L; x += blockDim.x) a[x] = s_arr[x];
+            } else {
+                tie_bitonic(pop, M, a, L);
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // Sorted copy of objectives 1..M-1 and run heads for the dup computation.
@@ -720,7 +841,7 @@ __global__ void nds_reset_counters(int* counters)
 {
     if (threadIdx.x < 4) counters[threadIdx.x] = 0;
     if (threadIdx.x == 4) counters[4] = 0;
-    if (threadIdx.x >= 10 && threadIdx.x <= 12) counters[threadIdx.x] = 0;
+    if (threadIdx.x >= 10 && threadIdx.x <= 13) counters[threadIdx.x] = 0;
 }
 
 template <int M>
@@ -1090,24 +1211,19 @@ int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_f
     const int T = 256, G = ceil_div(n, T);
 
     nds_reset_counters<<<1, 32, 0, stream>>>(ws.counters);
-    nds_classify<<<G, T, 0, stream>>>(pop, M, ws.key0, ws.perm[0], feas);
+    nds_classify<<<G, T, 0, stream>>>(pop, M, ws.key0, ws.key64[0], ws.perm[0], feas);
     MOEA_CUDA_TRY(cudaGetLastError());
     const uint64_t* key0 = ws.key0;
-    int cur = 0;
     size_t tmp = ws.cub_bytes;
-    for (int m = M - 1; m >= 1; --m) {
-        nds_gather_key<<<G, T, 0, stream>>>(pop, m, key0, ws.perm[cur], ws.key32[0]);
-        MOEA_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp, tmp, ws.key32[0], ws.key32[1],
-                                                      ws.perm[cur], ws.perm[cur ^ 1], n, 0, 32,
-                                                      stream));
-        cur ^= 1;
-    }
-    nds_gather_key0<<<G, T, 0, stream>>>(n, key0, ws.perm[cur], ws.key64[0]);
-    MOEA_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp, tmp, ws.key64[0],
-                                                  ws.key64[1], ws.perm[cur],
-                                                  ws.perm[cur ^ 1], n, 0, 34, stream));
-    cur ^= 1;
-    const int* perm = ws.perm[cur];
+    MOEA_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp, tmp, ws.key64[0], ws.key64[1], ws.perm[0],
+                                                  ws.perm[1], n, 0, 64, stream));
+    // runs of equal keys in class 0 into lexicographic order; ws.run_start
+    // holds the list of long runs until the dup scan below overwrites it
+    nds_tie_fix<<<G, T, 0, stream>>>(pop, M, ws.key64[1], ws.perm[1], ws.run_start, ws.counters + 13);
+    nds_tie_fix_long<<<kTieLongCtas, kTieLongThreads, 0, stream>>>(pop, M, ws.key64[1], ws.perm[1], ws.run_start,
+                                                               ws.counters + 13);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    const int* perm = ws.perm[1];
 
     nds_sorted_soa<<<G, T, 0, stream>>>(pop, M, key0, perm, ws.sorted_f, ws.n_max, ws.head);
     MOEA_CUDA_TRY(cub::DeviceScan::InclusiveScan(ws.cub_tmp, tmp, ws.head, ws.run_start,
