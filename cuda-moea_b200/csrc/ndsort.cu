@@ -536,7 +536,7 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
     // rows whose probe did not resolve them: scanned by the whole CTA in
     // chunks of kScanChunk words after the groups of the front
     __shared__ int s_nscan, s_ntask;
-    __shared__ int s_sq[kScanQueue], s_sw[kScanQueue], s_found[kScanQueue], s_cp[kScanQueue];
+    __shared__ int s_sq[kScanQueue], s_sw[kScanQueue], s_found[kScanQueue];
     // points of the next front found by this CTA, appended to the global list
     // with one atomic per CTA and front (directly when the buffer is full)
     __shared__ int s_free[kFreeBuf];
@@ -551,7 +551,9 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
-    const int gwarp = block * wpb + warp;
+    // groups of 32 positions interleaved over the CTAs: every CTA holds low
+    // (short rows) and high (long rows) positions alike
+    const int gwarp = warp * nblocks + block;
     const int twarps = nblocks * wpb;
     const int ngroups = (n + 31) >> 5;
     int len_prev = 0, total = 0, k = 0;
@@ -675,35 +677,33 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
         const int nscan = min(s_nscan, kScanQueue);
         if (nscan > 0) {
             // chunks of the queued rows: row s covers words sw[s]..0 in
-            // chunks of kScanChunk from the top; cp[s] = first chunk of row s
+            // chunks of kScanChunk from the top.  Tasks go level by level (the
+            // top chunk of every row first), and a chunk is skipped once an
+            // unassigned dominator above it has been found: the highest one
+            // found is the same, and most rows end in their top chunk.  A hit
+            // found lower down (a later chunk can finish first) skips nothing.
             if (warp == 0) {
-                int base = 0;
+                int levels = 0;
                 for (int s0 = 0; s0 < nscan; s0 += 32) {
                     const int sidx = s0 + lane;
-                    const int c = (sidx < nscan) ? s_sw[sidx] / kScanChunk + 1 : 0;
-                    int incl = c;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int tv = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-                        if (lane >= o) incl += tv;
-                    }
                     if (sidx < nscan) {
-                        s_cp[sidx] = base + incl - c;
+                        levels = max(levels, s_sw[sidx] / kScanChunk + 1);
                         s_found[sidx] = -1;
                     }
-                    base += __shfl_sync(0xFFFFFFFFu, incl, 31);
                 }
-                if (lane == 0) s_ntask = base;
+#pragma unroll
+                for (int o = 16; o; o >>= 1) levels = max(levels, __shfl_xor_sync(0xFFFFFFFFu, levels, o));
+                if (lane == 0) s_ntask = levels * nscan;
             }
             __syncthreads();
             const int ntask = s_ntask;
             for (int task = warp; task < ntask; task += wpb) {
-                int lo = 0, hi = nscan;  // last row with cp <= task
-                while (hi - lo > 1) {
-                    const int mid = (lo + hi) >> 1;
-                    if (s_cp[mid] <= task) lo = mid; else hi = mid;
-                }
-                const int top = s_sw[lo] - (task - s_cp[lo]) * kScanChunk;
+                const int level = task / nscan, lo = task - level * nscan;
+                if (level > s_sw[lo] / kScanChunk) continue;
+                const int top = s_sw[lo] - level * kScanChunk;
+                // warp-uniform: the chunk scan below is warp-collective
+                const int found_hi = __shfl_sync(0xFFFFFFFFu, *((volatile int*)s_found + lo), 0);
+                if (found_hi > top * 32 + 31) continue;
                 const uint32_t* row = rows + (size_t)s_sq[lo] * W;
                 uint32_t acc[kScanChunk / 32];
 #pragma unroll

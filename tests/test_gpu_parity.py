@@ -95,6 +95,30 @@ def test_ndsort_fronts_bit_exact(st, ws, oracle, M, n, kind, cvmode):
         assert gmf == wmf
 
 
+@pytest.mark.parametrize("M,n,feasible_share", [(3, 65536, 1.0), (5, 40000, 0.7)])
+def test_ndsort_full_size_many_fronts(st, oracle, M, n, feasible_share):
+    """Full-size sorts with dozens of thin fronts: points near the DTLZ1 front
+    (g small), so rows are thousands of words long and every peel front
+    queues hundreds of row scans per CTA.  Three GPU runs against the oracle:
+    the peel's CTAs race only in timing, never in the result."""
+    rng = np.random.default_rng(n + M)
+    x = rng.random((n, M + 4)).astype(np.float32)
+    x[:, M - 1:] = (0.5 + 0.02 * rng.standard_normal((n, 5))).astype(np.float32)
+    objs, _ = oracle.evaluate("DTLZ1", x, M)
+    cv = np.where(rng.random(n) < feasible_share, 0.0, rng.random(n) * 2.0).astype(np.float32)
+    target = n // 2
+    want, wmf = oracle.ndsort(cv, objs, target)
+    assert wmf >= 10  # many fronts, or the test exercises nothing
+    w = st.Workspace(max_points=n, max_objectives=M, max_directions=1)
+    try:
+        for _ in range(3):
+            got, gmf = st.ndsort(w, _t(cv), _t(objs), target)
+            np.testing.assert_array_equal(got.cpu().numpy(), want)
+            assert gmf == wmf
+    finally:
+        w.close()
+
+
 def test_ndsort_all_mutually_nondominated(st, ws, oracle):
     # points on a line f1 = 1 - f0: no dominance pair at all (the reference's
     # CSR queue path leaves every front at -1 in this case; the relation gives front 0)
