@@ -334,6 +334,33 @@ struct TileCfg {
     static constexpr int kMF = (M > 1) ? M - 1 : 1;   // objectives 1..M-1
 };
 
+// Count of the 32 ascending keys at shared address a that are <= v, as the
+// byte offset 4 * count: binary search with steps of 16, 8, 4, 2, 1 keys and
+// a last probe that reaches 32 only from 31.  Each probe is one shared load
+// with an immediate offset, one compare and one predicated add.
+__device__ __forceinline__ uint32_t word_count_bytes(uint32_t a, uint32_t v)
+{
+    const uint32_t a0 = a;
+    asm("{\n\t.reg .pred p;\n\t.reg .u32 t;\n\t"
+        "ld.shared.u32 t, [%0+60];\n\tsetp.le.u32 p, t, %1;\n\t@p add.u32 %0, %0, 64;\n\t"
+        "ld.shared.u32 t, [%0+28];\n\tsetp.le.u32 p, t, %1;\n\t@p add.u32 %0, %0, 32;\n\t"
+        "ld.shared.u32 t, [%0+12];\n\tsetp.le.u32 p, t, %1;\n\t@p add.u32 %0, %0, 16;\n\t"
+        "ld.shared.u32 t, [%0+4];\n\tsetp.le.u32 p, t, %1;\n\t@p add.u32 %0, %0, 8;\n\t"
+        "ld.shared.u32 t, [%0];\n\tsetp.le.u32 p, t, %1;\n\t@p add.u32 %0, %0, 4;\n\t"
+        "ld.shared.u32 t, [%0];\n\tsetp.le.u32 p, t, %1;\n\t@p add.u32 %0, %0, 4;\n\t}"
+        : "+r"(a)
+        : "r"(v)
+        : "memory");
+    return a - a0;
+}
+
+__device__ __forceinline__ uint32_t ld_shared_u32(uint32_t a)
+{
+    uint32_t x;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(x) : "r"(a) : "memory");
+    return x;
+}
+
 // One CTA covers kQB dominatees q (one per lane of warps 0-3, again of warps
 // 4-7) against kPW words of dominator positions p (the first half of the
 // words for warps 0-3, the second half for warps 4-7).  The word tables of
@@ -397,34 +424,47 @@ __device__ __forceinline__ void tile_block(int bx, int by, const float* __restri
 
     constexpr int kHalf = PW / 2;
     const int wb = (warp >> 2) * kHalf;
-    for (int wl = wb; wl < wb + kHalf; ++wl) {
-        uint32_t bits = 0u;
-        if (wl < wcount) {
-            // positions p < dup[q] of this word
-            const int rem = dup - (w0 + wl) * 32;
-            const uint32_t mask = rem >= 32 ? 0xFFFFFFFFu : (rem <= 0 ? 0u : ((1u << rem) - 1u));
-            const bool need = mask != 0u && !inf;
-            if (M > 1 && __any_sync(0xFFFFFFFFu, need)) {
-                uint32_t cmp = 0xFFFFFFFFu;
+    const int wend = min(wb + kHalf, wcount);
+    // words whose 32 positions lie below dup[q] for every lane of the warp
+    // need no dup mask (most of them)
+    uint32_t key_addr[MF], bits_addr[MF];
 #pragma unroll
-                for (int m = 0; m < MF; ++m) {
-                    const uint32_t* sk = &s_key[m][wl * 32];
-                    const uint32_t v = qk[m];
-                    int k = 0;
-                    k += (sk[k + 15] <= v) ? 16 : 0;
-                    k += (sk[k + 7] <= v) ? 8 : 0;
-                    k += (sk[k + 3] <= v) ? 4 : 0;
-                    k += (sk[k + 1] <= v) ? 2 : 0;
-                    k += (sk[k] <= v) ? 1 : 0;
-                    k += (sk[k] <= v) ? 1 : 0;   // reaches 32 only from k == 31
-                    cmp &= s_bits[m][wl * 33 + k];
-                }
-                bits = inf ? mask : (mask & cmp);
-            } else {
-                bits = (inf || M == 1) ? mask : 0u;
+    for (int m = 0; m < MF; ++m) {
+        key_addr[m] = (uint32_t)__cvta_generic_to_shared(&s_key[m][0]);
+        bits_addr[m] = (uint32_t)__cvta_generic_to_shared(&s_bits[m][0]);
+    }
+    const int lane_full = (q < n) ? (dup >> 5) - w0 : 0x7FFFFFFF;
+    const int wfull = min(wend, max(wb, __reduce_min_sync(0xFFFFFFFFu, lane_full)));
+    // Every lane searches (the masks decide).  The prefix set of count c
+    // sits at byte 4 c of the word's bit table.  Running shared addresses
+    // step by one word table per iteration.
+#pragma unroll
+    for (int m = 0; m < MF; ++m) {
+        key_addr[m] += (uint32_t)wb * 128u;
+        bits_addr[m] += (uint32_t)wb * 132u;
+    }
+    uint32_t* so_row = &so[ql][0];
+    const uint32_t infm = inf ? 0xFFFFFFFFu : 0u;
+    auto word_bits = [&]() -> uint32_t {
+        uint32_t cmp = 0xFFFFFFFFu;
+        if (M > 1) {
+#pragma unroll
+            for (int m = 0; m < MF; ++m) {
+                const uint32_t off = word_count_bytes(key_addr[m], qk[m]);
+                cmp &= ld_shared_u32(bits_addr[m] + off);
+                key_addr[m] += 128u;
+                bits_addr[m] += 132u;
             }
         }
-        so[ql][wl] = bits;
+        return cmp | infm;
+    };
+    int wl = wb;
+    for (; wl < wfull; ++wl) so_row[wl] = word_bits();   // all positions below dup[q]
+    for (; wl < wend; ++wl) {
+        // positions p < dup[q] of this word
+        const int rem = dup - (w0 + wl) * 32;
+        const uint32_t mask = rem >= 32 ? 0xFFFFFFFFu : (rem <= 0 ? 0u : ((1u << rem) - 1u));
+        so_row[wl] = mask & word_bits();
     }
     __syncthreads();
     for (int r = warp; r < kQB; r += kTileThreads / 32) {
