@@ -17,11 +17,13 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
 
 #include "internal.cuh"
+#include "snapshot.h"
 
 namespace moea {
 
@@ -202,6 +204,9 @@ struct moea_algorithm {
     bool fused_single = false;
     BatchInst* f_inst[2] = {};
     FusedGroup f_group;
+    // snapshots (data-recorder format) and their metadata
+    std::string save_dir, problem_label;
+    std::unique_ptr<SnapshotWriter> recorder;
 
     int setup_single_fused();
     int describe_single_fused();
@@ -216,6 +221,7 @@ struct moea_algorithm {
 
     void release()
     {
+        recorder.reset();  // waits for queued snapshots
         for (auto& g : graph)
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
         for (auto& d : f_inst)
@@ -363,6 +369,8 @@ struct moea_algorithm {
             cfg.association_mode != MOEA_ASSOC_TENSOR)
             return set_error(MOEA_ERR_INVALID_ARGUMENT, "association_mode must be %d, %d or %d", MOEA_ASSOC_TREE,
                              MOEA_ASSOC_SCAN, MOEA_ASSOC_TENSOR);
+        if (!save_dir.empty() && cfg.save_interval <= 0)
+            return set_error(MOEA_ERR_INVALID_ARGUMENT, "saveData generation interval must be positive");
         if (cfg.mating == MOEA_MATING_CALLBACK && !cfg.mate)
             return set_error(MOEA_ERR_INVALID_ARGUMENT, "callback mating without a function");
         // only the NSGA-III selector provides ranks (mating_selection.cu:80-86)
@@ -453,6 +461,98 @@ struct moea_algorithm {
         MOEA_TRY(start_population());
         initialized = true;
         if (cfg.fused_small && fused_eligible(this)) MOEA_TRY(setup_single_fused());
+        if (!save_dir.empty()) {
+            std::vector<float> lo(D), hi(D);
+            for (int d = 0; d < D; ++d) {
+                lo[d] = hb[2 * d];
+                hi[d] = hb[2 * d + 1];
+            }
+            recorder.reset(new SnapshotWriter());
+            MOEA_TRY(recorder->open(save_dir, cfg.save_interval, snapshot_meta(), lo, hi, refs0, stream));
+            MOEA_TRY(snapshot_now());
+        }
+        return MOEA_OK;
+    }
+
+    SnapshotMeta snapshot_meta() const
+    {
+        static const char* kNames[16] = {nullptr, "DTLZ1", "DTLZ2", "DTLZ3", "DTLZ4", "DTLZ5", "DTLZ6", "DTLZ7",
+                                         "ConvexDTLZ2", "C1DTLZ1", "C1DTLZ3", "C2DTLZ2", "C2ConvexDTLZ2",
+                                         "C3DTLZ1", "C3DTLZ4", "CSDP"};
+        SnapshotMeta m;
+        m.algorithm_name = nsga3() ? "NSGA-III" : "RVEA";  // algorithm_factory.cu:16-17
+        const int k = cfg.problem_kind;
+        m.problem_name = (k >= 1 && k <= 15) ? kNames[k] : problem_label;
+        m.N = N;
+        m.D = D;
+        m.M = M;
+        m.H = H;
+        m.T = T;
+        m.constraint_count = k == 0 ? cfg.constraint_count : (constrained() ? 1 : 0);
+        m.seed = cfg.seed;
+        return m;
+    }
+
+    // Queues the snapshot of the current parents when one is due.
+    int snapshot_now()
+    {
+        if (!recorder) return MOEA_OK;
+        SnapshotSave s;
+        s.generation = generation;
+        s.vars = vars[P];
+        s.objs = objs[P];
+        s.cv = cv[P];
+        s.refs = refs;
+        if (nsga3()) {
+            s.aux = rank[P];
+            s.aux_count = N;
+            s.active = N;
+        } else {
+            s.aux = frontzero;
+            s.aux_count = frontzero_count;
+            s.d_active = d_active;
+        }
+        s.ideal = ideal_last;
+        s.offset = ws.offset_dev;
+        s.epoch = epoch;
+        s.last_prepared_target = last_prepared_target;
+        s.ideal_ready = ideal_ready ? 1 : 0;
+        return recorder->save(s, stream);
+    }
+
+    int load_snapshot(const char* dir)
+    {
+        if (!dir || !*dir) return set_error(MOEA_ERR_INVALID_ARGUMENT, "snapshot: empty directory");
+        if (!initialized) MOEA_TRY(initialize());
+        MOEA_CUDA_TRY(cudaSetDevice(cfg.device));
+        MOEA_CUDA_TRY(cudaStreamSynchronize(stream));
+        SnapshotLoad L;
+        MOEA_TRY(load_snapshot_files(dir, snapshot_meta(), nsga3(), L));
+        auto up = [&](void* dst, const void* src, size_t bytes) {
+            return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream);
+        };
+        MOEA_CUDA_TRY(up(vars[P], L.vars.data(), sizeof(float) * L.vars.size()));
+        MOEA_CUDA_TRY(up(objs[P], L.objs.data(), sizeof(float) * L.objs.size()));
+        MOEA_CUDA_TRY(up(cv[P], L.cv.data(), sizeof(float) * L.cv.size()));
+        if (nsga3()) MOEA_CUDA_TRY(up(rank[P], L.aux.data(), sizeof(int) * L.aux.size()));
+        // adapted directions change during a run; fixed ones were built at initialize
+        if (cfg.directions == MOEA_DIRS_ADAPTIVE && H > 0) {
+            MOEA_CUDA_TRY(up(refs, L.refs.data(), sizeof(float) * L.refs.size()));
+            if (!nsga3()) MOEA_TRY(run_rvea_gamma(refs, M, H, gamma, stream));
+        }
+        const int active = nsga3() ? N : L.active;
+        MOEA_CUDA_TRY(up(d_active, &active, sizeof(int)));
+        MOEA_CUDA_TRY(up(d_gen, &L.generation, sizeof(int)));
+        MOEA_CUDA_TRY(up(ws.offset_dev, &L.niching_offset, sizeof(unsigned long long)));
+        MOEA_CUDA_TRY(up(ideal_last, L.ideal.data(), sizeof(float) * L.ideal.size()));
+        MOEA_CUDA_TRY(cudaStreamSynchronize(stream));
+        generation = L.generation;
+        epoch = L.epoch;
+        last_prepared_target = L.last_prepared_target;
+        ideal_ready = L.ideal_ready != 0;
+        frontzero_count = 0;
+        drop_graphs();  // captured generations hold the seed of their epoch
+        if (fused_single) MOEA_TRY(describe_single_fused());
         return MOEA_OK;
     }
 
@@ -626,7 +726,8 @@ struct moea_algorithm {
             }
         }
         if (!done) MOEA_TRY(generation_body());
-        return post_step();
+        MOEA_TRY(post_step());
+        return snapshot_now();
     }
 
     int active_count_sync()
@@ -659,6 +760,15 @@ struct moea_algorithm {
         return workspace_check_status(ws, stream);
     }
 
+    // finalize plus the snapshot of the current generation (reference result())
+    int finalize_and_save()
+    {
+        MOEA_TRY(finalize());
+        if (!recorder) return MOEA_OK;
+        MOEA_TRY(snapshot_now());
+        return recorder->flush();
+    }
+
     int reset()
     {
         if (!initialized) return MOEA_OK;
@@ -675,7 +785,7 @@ struct moea_algorithm {
         MOEA_TRY(start_population());
         // the draws of the new epoch use another seed
         if (fused_single) MOEA_TRY(describe_single_fused());
-        return MOEA_OK;
+        return snapshot_now();
     }
 };
 
@@ -725,6 +835,9 @@ moea_status moea_algorithm_create(const moea_algorithm_config* cfg, moea_algorit
     if (cfg->h_initial_population && N > 0 && D > 0)
         a->init_pop.assign(cfg->h_initial_population, cfg->h_initial_population + (size_t)N * D);
     a->cfg.h_lower = a->cfg.h_upper = a->cfg.h_user_directions = a->cfg.h_initial_population = nullptr;
+    if (cfg->save_directory) a->save_dir = cfg->save_directory;
+    if (cfg->problem_name) a->problem_label = cfg->problem_name;
+    a->cfg.save_directory = a->cfg.problem_name = nullptr;
     *out = a;
     return MOEA_OK;
 }
@@ -789,7 +902,19 @@ moea_status moea_algorithm_synchronize(moea_algorithm* a)
 moea_status moea_algorithm_finalize(moea_algorithm* a)
 {
     if (!a) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL algorithm");
-    return a->finalize();
+    return a->finalize_and_save();
+}
+
+moea_status moea_algorithm_flush_snapshots(moea_algorithm* a)
+{
+    if (!a) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL algorithm");
+    return a->recorder ? a->recorder->flush() : MOEA_OK;
+}
+
+moea_status moea_algorithm_load_snapshot(moea_algorithm* a, const char* generation_directory)
+{
+    if (!a) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL algorithm");
+    return a->load_snapshot(generation_directory);
 }
 
 moea_status moea_algorithm_view(moea_algorithm* a, moea_population_view* v)
@@ -1202,6 +1327,9 @@ moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void
             return set_error(MOEA_ERR_INVALID_ARGUMENT,
                              "batch: instance %d uses a callback; batched instances need built-in problems "
                              "and mating", i);
+        if (c.save_directory)
+            return set_error(MOEA_ERR_INVALID_ARGUMENT,
+                             "batch: instance %d saves snapshots; run it alone to save them", i);
     }
     MOEA_CUDA_TRY(cudaSetDevice(device));
     moea_batch* b = new (std::nothrow) moea_batch();

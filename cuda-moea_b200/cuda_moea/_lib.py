@@ -53,6 +53,8 @@ class AlgorithmConfig(ctypes.Structure):
         ("cv_log_alpha", c_float), ("feasibility_epsilon", c_float),
         ("association_mode", c_int), ("rvea_alpha", c_float),
         ("h_initial_population", fp), ("use_graphs", c_int), ("fused_small", c_int),
+        ("save_directory", ctypes.c_char_p), ("save_interval", c_int),
+        ("problem_name", ctypes.c_char_p), ("constraint_count", c_int),
     ]
 
 
@@ -116,6 +118,8 @@ _SIGNATURES = [
     ("moea_algorithm_reset", c_int, [vp]),
     ("moea_algorithm_synchronize", c_int, [vp]),
     ("moea_algorithm_finalize", c_int, [vp]),
+    ("moea_algorithm_flush_snapshots", c_int, [vp]),
+    ("moea_algorithm_load_snapshot", c_int, [vp, ctypes.c_char_p]),
     ("moea_algorithm_view", c_int, [vp, ctypes.POINTER(PopulationViewC)]),
     ("moea_algorithm_directions", c_int, [vp, ctypes.POINTER(vp), ip]),
     ("moea_algorithm_profile_step", c_int, [vp, ctypes.c_char_p, c_size_t, fp, c_int, ip]),

@@ -8,6 +8,7 @@ bindings.cpp:100-146 of the reference).
 from __future__ import annotations
 
 import ctypes
+import os
 from dataclasses import dataclass
 from pathlib import Path
 from typing import Any
@@ -138,8 +139,13 @@ class Algorithm:
         self._max_generations = int(max_generations)
         self._progress_interval = progress_interval
         self._print_progress = print_progress
+        # snapshots in the reference's data-recorder layout (algorithm_factory.cu:80-86)
+        if save_data is not None and not str(save_data):
+            raise ValueError("saveData output directory cannot be empty")
+        if save_data is not None and int(save_interval) <= 0:
+            raise ValueError("saveData generation interval must be positive")
         self._save_data = save_data
-        self._save_interval = save_interval
+        self._save_interval = int(save_interval)
         self._device = int(cuda.device_id)
         self._use_graphs = bool(use_graphs)
         self._fuse_small = bool(fuse_small)
@@ -197,6 +203,11 @@ class Algorithm:
             cfg.stream = cur.cuda_stream
         cfg.use_graphs = 1 if self._use_graphs else 0
         cfg.fused_small = 1 if self._fuse_small else 0
+        if self._save_data is not None:
+            directory = os.fsencode(os.fspath(self._save_data))
+            keep.append(directory)
+            cfg.save_directory = directory
+            cfg.save_interval = self._save_interval
         D, M = self._problem_info
         cfg.dimension, cfg.objectives = D, M
         p = self._specs["problem"]
@@ -212,6 +223,10 @@ class Algorithm:
             fn = _lib.EVALUATE_FN(self._make_evaluate(p["object"]))
             keep.append(fn)
             cfg.evaluate = fn
+            name = str(p.get("name") or "").encode()
+            keep.append(name)
+            cfg.problem_name = name or None
+            cfg.constraint_count = int(p.get("constraints", 0))
         m = self._specs["mating"]
         if m["type"] == "TournamentMating":
             cfg.mating = 1
@@ -418,6 +433,19 @@ class Algorithm:
         if self._native is None or not self.initialized:
             return
         self._call(lib().moea_algorithm_reset, self._native.handle)
+
+    def load_snapshot(self, directory: str | Path) -> None:
+        """Resumes from a generation directory written by ``save_data``
+        snapshots (``<save_data>/generation_NNNNNN``): the population and the
+        selection state are replaced, and the following steps equal those of
+        the run that wrote it when the configuration is the same."""
+        h = self._ensure_native()
+        self._call(lib().moea_algorithm_load_snapshot, h, os.fsencode(os.fspath(directory)))
+
+    def flush_snapshots(self) -> None:
+        """Waits until every snapshot queued so far is on disk."""
+        if self._native is not None:
+            self._call(lib().moea_algorithm_flush_snapshots, self._native.handle)
 
     def synchronize(self) -> None:
         if self._native is not None:

@@ -308,6 +308,17 @@ typedef struct moea_algorithm_config {
     int fused_small;          /* run an eligible population with 2N <= 8192 (NSGA-III, built-in
                                  unconstrained DTLZ, fixed directions) as the fused generation:
                                  same results, about 20 launches instead of about 80 */
+    /* Snapshots in the reference's data-recorder format
+     * (nat/src/algorithm/data_recorder.cu:128-292): generation 0, every
+     * save_interval-th generation and the last one, under save_directory
+     * (NULL: no snapshots; save_interval must then be positive).  Written from
+     * pinned host copies by a side stream: the compute stream waits for the
+     * device-to-host copies only.  Each generation directory also holds
+     * resume.bin for moea_algorithm_load_snapshot. */
+    const char* save_directory;
+    int save_interval;
+    const char* problem_name; /* metadata name of a callback problem (NULL: null) */
+    int constraint_count;     /* metadata constraint count of a callback problem */
 } moea_algorithm_config;
 
 /* Fills cfg with the reference defaults (nat/src/factory/algorithm_factory.cu:25-118). */
@@ -322,8 +333,22 @@ moea_status moea_algorithm_step(moea_algorithm* alg);
 moea_status moea_algorithm_run(moea_algorithm* alg, double* h_total_ms);
 moea_status moea_algorithm_reset(moea_algorithm* alg);
 moea_status moea_algorithm_synchronize(moea_algorithm* alg);
-/* Runs finalize (front-0 indices for RVEA) before results are read. */
+/* Runs finalize (front-0 indices for RVEA) before results are read, saves
+ * the current generation's snapshot when one is due and waits for the
+ * snapshot files (the reference saves at result(), algorithm.cu:357-366). */
 moea_status moea_algorithm_finalize(moea_algorithm* alg);
+/* Waits until every snapshot queued so far is on disk and returns the first
+ * file error since the last call.  No counterpart in the reference, whose
+ * recorder writes synchronously (data_recorder.cu:219-292). */
+moea_status moea_algorithm_flush_snapshots(moea_algorithm* alg);
+/* Resume.  Replaces the state of an algorithm (initialized first if needed)
+ * by a generation directory of its snapshots: population, ranks or active
+ * count, adapted directions, running ideal point, niching counter and
+ * generation.  The following steps equal those of the run that wrote it,
+ * bit for bit, when the configuration is the same.  Sizes are checked
+ * against the configuration.  No counterpart in the reference, which only
+ * saves. */
+moea_status moea_algorithm_load_snapshot(moea_algorithm* alg, const char* generation_directory);
 
 typedef struct moea_population_view {
     float* d_variables;       /* (N,D) */
