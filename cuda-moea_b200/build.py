@@ -23,7 +23,8 @@ HOST_CXX = os.environ.get("MOEA_HOST_CXX", "/usr/bin/g++")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off", "-ccbin", HOST_CXX,
-          "-I", str(REPO / "include"), "-I", str(CSRC), "--expt-relaxed-constexpr"]
+          "-I", str(REPO / "include"), "-I", str(CSRC), "-I", str(PKG_ROOT / "sdk" / "include"),
+          "--expt-relaxed-constexpr"]
 
 
 def _sources():
@@ -31,7 +32,8 @@ def _sources():
 
 
 def _headers():
-    return list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list((REPO / "include").glob("*.h"))
+    return (list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list((REPO / "include").glob("*.h")) +
+            list((PKG_ROOT / "sdk" / "include").rglob("*.h*")))
 
 
 def _compile(src: Path, verbose: bool) -> Path:

@@ -246,6 +246,14 @@ struct moea_algorithm {
     }
 
     bool nsga3() const { return cfg.algorithm == MOEA_NSGA3; }
+
+    // A callback returned rc: keep the reason it gave, if any.
+    static int callback_failed(const char* what, int rc)
+    {
+        const std::string reason = last_error();
+        if (reason.empty()) return set_error(MOEA_ERR_CALLBACK, "%s callback failed (%d)", what, rc);
+        return set_error(MOEA_ERR_CALLBACK, "%s callback failed (%d): %s", what, rc, reason.c_str());
+    }
     bool constrained() const { return cfg.problem_kind >= 9 && cfg.problem_kind <= 15; }
 
     // MOEAStdTestEvaluator::is_cv_active (dtlz_kernels.cu:1302-1312)
@@ -266,9 +274,10 @@ struct moea_algorithm {
     int evaluate(int slot, int gen_index)
     {
         if (cfg.problem_kind == 0) {
+            set_error(MOEA_OK, "");  // a failing callback may leave its reason
             const int rc = cfg.evaluate(cfg.evaluate_user, vars[slot], objs[slot], cv[slot], N, D, M,
                                         gen_index, T, (void*)stream);
-            if (rc != 0) return set_error(MOEA_ERR_CALLBACK, "problem evaluate callback failed (%d)", rc);
+            if (rc != 0) return callback_failed("problem evaluate", rc);
             return MOEA_OK;
         }
         MOEA_TRY(run_problem(cfg.problem_kind, vars[slot], N, D, M, objs[slot], cv[slot], stream));
@@ -659,6 +668,14 @@ struct moea_algorithm {
     // prepare_parent, dtlz_kernels.cu:1361-1394).
     int pre_step()
     {
+        if (cfg.problem_kind == 0 && cfg.prepare) {
+            int changed = 0;
+            set_error(MOEA_OK, "");
+            const int rc = cfg.prepare(cfg.evaluate_user, vars[P], objs[P], cv[P], N, D, M, generation, T,
+                                       (void*)stream, &changed);
+            if (rc != 0) return callback_failed("problem prepare", rc);
+            if (changed) MOEA_TRY(prepare());
+        }
         if (constrained() && cfg.problem_kind != 0 && cv_switch_node(generation)) {
             MOEA_TRY(run_problem(cfg.problem_kind, vars[P], N, D, M, objs[P], cv[P], stream));
             last_prepared_target = generation;
@@ -782,6 +799,7 @@ struct moea_algorithm {
         }
         total_ms = 0.0;
         frontzero_count = 0;
+        if (cfg.problem_kind == 0 && cfg.problem_reset) cfg.problem_reset(cfg.evaluate_user);
         MOEA_TRY(start_population());
         // the draws of the new epoch use another seed
         if (fused_single) MOEA_TRY(describe_single_fused());

@@ -29,5 +29,13 @@ __all__ = [
     "AdaptiveRVEADirections", "UserDefinedDirections",
     "NSGA3EnvironmentSelector", "RVEAEnvironmentSelector",
     "PythonProblem", "PythonMating", "PythonCrossover", "PythonMutation",
-    "PythonReferenceDirections", "PythonEnvironmentSelector",
+    "PythonReferenceDirections", "PythonEnvironmentSelector", "NativeProblem",
 ] + _problem.__all__
+
+
+def __getattr__(name):
+    # imported on first use, so `python -m cuda_moea.native` runs the module once
+    if name == "NativeProblem":
+        from .native import NativeProblem
+        return NativeProblem
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")

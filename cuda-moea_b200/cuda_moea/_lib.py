@@ -21,6 +21,8 @@ ip = ctypes.POINTER(ctypes.c_int)
 
 EVALUATE_FN = ctypes.CFUNCTYPE(c_int, vp, vp, vp, vp, c_int, c_int, c_int, c_int, c_int, vp)
 MATING_FN = ctypes.CFUNCTYPE(c_int, vp, vp, vp, vp, vp, c_int, vp, c_int, c_int, c_int, c_int, vp)
+PREPARE_FN = ctypes.CFUNCTYPE(c_int, vp, vp, vp, vp, c_int, c_int, c_int, c_int, c_int, vp, ip)
+RESET_FN = ctypes.CFUNCTYPE(None, vp)
 
 MOEA_OK = 0
 ERROR_NAMES = {1: "invalid argument", 2: "CUDA error", 3: "unsupported", 4: "invalid state",
@@ -55,6 +57,7 @@ class AlgorithmConfig(ctypes.Structure):
         ("h_initial_population", fp), ("use_graphs", c_int), ("fused_small", c_int),
         ("save_directory", ctypes.c_char_p), ("save_interval", c_int),
         ("problem_name", ctypes.c_char_p), ("constraint_count", c_int),
+        ("prepare", PREPARE_FN), ("problem_reset", RESET_FN),
     ]
 
 
@@ -95,6 +98,19 @@ _SIGNATURES = [
     ("moea_nsga3_select", c_int, [vp, vp, vp, c_int, c_int, vp, c_int, c_u64, ctypes.POINTER(c_u64),
                                   vp, vp, vp, vp, c_int, vp]),
     ("moea_quantize_cv", c_int, [vp, vp, c_int, c_float, c_float, c_float, c_int, vp]),
+    ("moea_native_open", c_int, [ctypes.c_char_p, ctypes.POINTER(vp)]),
+    ("moea_native_close", None, [vp]),
+    ("moea_native_schema", c_int, [vp, ctypes.c_char_p, c_size_t, ctypes.POINTER(c_size_t)]),
+    ("moea_native_set_int", c_int, [vp, ctypes.c_char_p, ctypes.c_longlong]),
+    ("moea_native_set_float", c_int, [vp, ctypes.c_char_p, c_double]),
+    ("moea_native_set_bool", c_int, [vp, ctypes.c_char_p, c_int]),
+    ("moea_native_set_string", c_int, [vp, ctypes.c_char_p, ctypes.c_char_p]),
+    ("moea_native_set_floats", c_int, [vp, ctypes.c_char_p, ctypes.POINTER(c_double), c_int]),
+    ("moea_native_create", c_int, [vp, ctypes.c_char_p, c_int, c_int, fp, fp]),
+    ("moea_native_constraint_count", c_int, [vp, ip]),
+    ("moea_native_evaluate", c_int, [vp, vp, vp, vp, c_int, c_int, c_int, c_int, c_int, vp]),
+    ("moea_native_prepare", c_int, [vp, vp, vp, vp, c_int, c_int, c_int, c_int, c_int, vp, ip]),
+    ("moea_native_reset", None, [vp]),
     ("moea_rvea_translate", c_int, [vp, vp, c_int, c_int, vp, vp, vp]),
     ("moea_rvea_partition", c_int, [vp, vp, vp, c_int, c_int, c_int, c_int, c_int, vp, vp, vp]),
     ("moea_rvea_gamma", c_int, [vp, vp, c_int, c_int, vp, vp]),

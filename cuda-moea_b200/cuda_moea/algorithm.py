@@ -167,7 +167,7 @@ class Algorithm:
         t = p["type"]
         if t in ("DTLZProblem",):
             return int(p["dimension"]), int(p["objectives"])
-        if t == "PythonProblem":
+        if t in ("PythonProblem", "NativeProblem"):
             return int(p["dimension"]), int(p["objectives"])
         raise TypeError(f"unsupported problem specification {t}")
 
@@ -214,6 +214,25 @@ class Algorithm:
         if p["type"] == "DTLZProblem":
             cfg.problem_kind = PROBLEM_KINDS[p["kind"]]
             cfg.constraint_activation_ratio = float(p["constraint_activation_ratio"])
+        elif p["type"] == "NativeProblem":
+            # the plugin through the library's own hooks; the instance outlives
+            # the algorithm handle (released after it in _Native)
+            from .native import NativeInstance
+            inst = NativeInstance(p)
+            keep.append(inst)
+            cfg.problem_kind = 0
+            lo_buf, lo = _float_ptr_array(p["lower_bounds"])
+            hi_buf, hi = _float_ptr_array(p["upper_bounds"])
+            keep += [lo_buf, hi_buf]
+            cfg.h_lower, cfg.h_upper = lo, hi
+            cfg.evaluate = _lib.EVALUATE_FN(NativeInstance.hook("moea_native_evaluate"))
+            cfg.prepare = _lib.PREPARE_FN(NativeInstance.hook("moea_native_prepare"))
+            cfg.problem_reset = _lib.RESET_FN(NativeInstance.hook("moea_native_reset"))
+            cfg.evaluate_user = inst.ptr
+            name = p["name"].encode()
+            keep.append(name)
+            cfg.problem_name = name
+            cfg.constraint_count = inst.constraint_count
         else:
             cfg.problem_kind = 0
             lo_buf, lo = _float_ptr_array(p["lower_bounds"])

@@ -262,6 +262,14 @@ typedef int (*moea_evaluate_fn)(void* user, const float* d_vars, float* d_objs, 
 typedef int (*moea_mating_fn)(void* user, const float* d_vars, const float* d_objs,
                               const float* d_cv, const int* d_rank, int active, int* d_out,
                               int N, int D, int M, int generation, void* stream);
+/* Runs before each generation on the parents of a callback problem
+ * (IProblemEvaluator::prepare_parent, nat/src/algorithm/algorithm.cu:230-237);
+ * a nonzero *h_changed makes the algorithm sort the parents again.  Returns 0
+ * on success. */
+typedef int (*moea_prepare_fn)(void* user, float* d_vars, float* d_objs, float* d_cv, int N, int D, int M,
+                               int generation, int max_generations, void* stream, int* h_changed);
+/* Called when the algorithm is reset (IProblemEvaluator::reset, algorithm.cu:413). */
+typedef void (*moea_problem_reset_fn)(void* user);
 
 typedef struct moea_algorithm_config {
     int algorithm;            /* MOEA_NSGA3 / MOEA_RVEA */
@@ -319,6 +327,9 @@ typedef struct moea_algorithm_config {
     int save_interval;
     const char* problem_name; /* metadata name of a callback problem (NULL: null) */
     int constraint_count;     /* metadata constraint count of a callback problem */
+    /* optional hooks of a callback problem, called with evaluate_user */
+    moea_prepare_fn prepare;
+    moea_problem_reset_fn problem_reset;
 } moea_algorithm_config;
 
 /* Fills cfg with the reference defaults (nat/src/factory/algorithm_factory.cu:25-118). */
@@ -414,6 +425,50 @@ moea_status moea_batch_info(moea_batch* b, int* h_count, int* h_generation, int*
                             int* h_fused);
 /* Population view of instance `index` (same contract as moea_algorithm_view). */
 moea_status moea_batch_view(moea_batch* b, int index, moea_population_view* out);
+
+/* ---- problem plugins: C++ IProblemEvaluator libraries ------------------
+ * A plugin is a shared library built against the plugin SDK
+ * (cuda-moea_b200/sdk/include: IProblemEvaluator, PopulationView,
+ * ProblemConfig, CUDA_MOEA_REGISTER_PROBLEM), which repeats the names of the
+ * reference's SDK (nat/include/cuda_moea/native/plugin.cuh:35-58,
+ * problem/problem_evaluator.cuh:10-31), so reference problem sources build
+ * against it unchanged.  Replaces the reference's loader
+ * (python/csrc/native_problem.cpp). */
+typedef struct moea_native_problem moea_native_problem;
+
+/* Loads a problem library and checks its registration (entry point
+ * cuda_moea_problem_v1: ABI 1, this SDK's build id, a name, unique parameter
+ * names). */
+moea_status moea_native_open(const char* library_path, moea_native_problem** out);
+/* Waits for the problem's stream, destroys the problem, unloads the library. */
+void moea_native_close(moea_native_problem* p);
+/* The registration as JSON: {"name", "build_id", "parameters": {name:
+ * {"type", "default", "description"}}}, types int, float, bool, str,
+ * float_list.  *needed receives the size with the terminating zero. */
+moea_status moea_native_schema(const moea_native_problem* p, char* buf, size_t cap, size_t* needed);
+/* A parameter value for moea_native_create.  Its type must be the type of
+ * the registered default (a float parameter also takes an integer); unknown
+ * names are rejected. */
+moea_status moea_native_set_int(moea_native_problem* p, const char* name, long long value);
+moea_status moea_native_set_float(moea_native_problem* p, const char* name, double value);
+moea_status moea_native_set_bool(moea_native_problem* p, const char* name, int value);
+moea_status moea_native_set_string(moea_native_problem* p, const char* name, const char* value);
+moea_status moea_native_set_floats(moea_native_problem* p, const char* name, const double* values, int count);
+/* Constructs the problem (the plugin's constructor) with the values set and
+ * the defaults of the rest.  name must be the registered name; the problem's
+ * ProblemInfo must repeat dimension, objectives and the bounds. */
+moea_status moea_native_create(moea_native_problem* p, const char* name, int dimension, int objectives,
+                               const float* h_lower, const float* h_upper);
+moea_status moea_native_constraint_count(const moea_native_problem* p, int* out);
+/* The problem as callback hooks of moea_algorithm_config (evaluate, prepare,
+ * problem_reset with evaluate_user = the handle).  moea_native_evaluate can
+ * also be called directly: it evaluates d_vars (N,D) into d_objs (M,N) and
+ * d_cv (N) on stream.  The first call runs the plugin's initialize. */
+int moea_native_evaluate(void* p, const float* d_vars, float* d_objs, float* d_cv, int N, int D, int M,
+                         int generation, int max_generations, void* stream);
+int moea_native_prepare(void* p, float* d_vars, float* d_objs, float* d_cv, int N, int D, int M, int generation,
+                        int max_generations, void* stream, int* h_changed);
+void moea_native_reset(void* p);
 
 #ifdef __cplusplus
 }
