@@ -118,15 +118,16 @@ int set_value(moea_native_problem* p, const char* name, cn::Parameter value, int
     const int want = static_cast<int>(spec->default_value.index());
     if (want == 1 && kind == 0) value = static_cast<double>(std::get<std::int64_t>(value));  // int for a float
     else if (want != kind)
-        return moea::set_error(MOEA_ERR_INVALID_ARGUMENT, "Native parameter '%s' must be %s", spec->name,
-                               kTypeNames[want]);
+        return moea::set_error(MOEA_ERR_INVALID_ARGUMENT, "Invalid type/value for native parameter '%s' (%s)",
+                               spec->name, kTypeNames[want]);
     if (value.index() == 1 && !std::isfinite(std::get<double>(value)))
-        return moea::set_error(MOEA_ERR_INVALID_ARGUMENT, "Native parameter '%s' must be finite", spec->name);
+        return moea::set_error(MOEA_ERR_INVALID_ARGUMENT, "Invalid type/value for native parameter '%s' (not finite)",
+                               spec->name);
     if (value.index() == 4)
         for (double x : std::get<std::vector<double>>(value))
             if (!std::isfinite(x))
-                return moea::set_error(MOEA_ERR_INVALID_ARGUMENT, "Native parameter '%s' must be finite",
-                                       spec->name);
+                return moea::set_error(MOEA_ERR_INVALID_ARGUMENT,
+                                       "Invalid type/value for native parameter '%s' (not finite)", spec->name);
     p->values[spec->name] = std::move(value);
     return MOEA_OK;
 }
@@ -176,7 +177,7 @@ moea_status moea_native_open(const char* library_path, moea_native_problem** out
     if (!library_path || !out) return moea::set_error(MOEA_ERR_INVALID_ARGUMENT, "native problem: NULL argument");
     *out = nullptr;
     void* h = dlopen(library_path, RTLD_NOW | RTLD_LOCAL);
-    if (!h) return moea::set_error(MOEA_ERR_INVALID_ARGUMENT, "Cannot load native problem: %s", dlerror());
+    if (!h) return moea::set_error(MOEA_ERR_LOAD, "Cannot load native problem: %s", dlerror());
     auto entry = reinterpret_cast<cn::Entry>(dlsym(h, "cuda_moea_problem_v1"));
     if (!entry) {
         dlclose(h);
@@ -306,12 +307,16 @@ moea_status moea_native_create(moea_native_problem* p, const char* name, int dim
         auto it = p->values.find(spec.name);
         config.parameters.emplace(spec.name, it != p->values.end() ? it->second : spec.default_value);
     }
+    // a constructor that rejects its configuration is an invalid argument
+    // (python/csrc/native_problem.cpp:93-99)
     cuda_moea::IProblemEvaluator* made = nullptr;
-    const int st = guarded("construction", [&]() -> int {
+    try {
         made = p->plugin->create(config);
-        return MOEA_OK;
-    });
-    if (st != MOEA_OK) return st;
+    } catch (const std::exception& e) {
+        return moea::set_error(MOEA_ERR_INVALID_ARGUMENT, "Native problem construction failed: %s", e.what());
+    } catch (...) {
+        return moea::set_error(MOEA_ERR_CALLBACK, "Native problem construction failed with a nonstandard exception");
+    }
     if (!made) return moea::set_error(MOEA_ERR_CALLBACK, "Native problem factory returned null");
     const auto& info = made->info();
     if (info.dimension != dimension || info.objective_count != objectives || info.lower_bounds != config.lower_bounds ||

@@ -26,13 +26,18 @@ RESET_FN = ctypes.CFUNCTYPE(None, vp)
 
 MOEA_OK = 0
 ERROR_NAMES = {1: "invalid argument", 2: "CUDA error", 3: "unsupported", 4: "invalid state",
-               5: "device timeout", 6: "out of memory", 7: "callback failed"}
+               5: "device timeout", 6: "out of memory", 7: "callback failed", 8: "load failed"}
+MOEA_ERR_INVALID_ARGUMENT = 1
 
 
 class MoeaError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"{ERROR_NAMES.get(code, 'error')} ({code}): {message}")
         self.code = code
+
+
+class MoeaValueError(MoeaError, ValueError):
+    """MOEA_ERR_INVALID_ARGUMENT: the reference raises ValueError (std::invalid_argument)."""
 
 
 class AlgorithmConfig(ctypes.Structure):
@@ -175,4 +180,5 @@ def lib():
 def check(status: int) -> None:
     if status != MOEA_OK:
         msg = lib().moea_last_error()
-        raise MoeaError(status, msg.decode() if msg else "")
+        cls = MoeaValueError if status == MOEA_ERR_INVALID_ARGUMENT else MoeaError
+        raise cls(status, msg.decode() if msg else "")

@@ -156,6 +156,13 @@ class Algorithm:
                 raise ValueError("initial_population must have shape (population_size, dimension)")
             self._initial = t
         self._problem_info = self._problem_dims(self._specs["problem"])
+        # a plugin problem is constructed with the algorithm, so a plugin that
+        # rejects its configuration fails here (as the reference's algorithm
+        # constructor does); the instance outlives the algorithm handle
+        self._plugin = None
+        if self._specs["problem"]["type"] == "NativeProblem":
+            from .native import NativeInstance
+            self._plugin = NativeInstance(self._specs["problem"])
         self._validate_unsupported()
         self._native: _Native | None = None
         self._stream = None
@@ -218,7 +225,7 @@ class Algorithm:
             # the plugin through the library's own hooks; the instance outlives
             # the algorithm handle (released after it in _Native)
             from .native import NativeInstance
-            inst = NativeInstance(p)
+            inst = self._plugin
             keep.append(inst)
             cfg.problem_kind = 0
             lo_buf, lo = _float_ptr_array(p["lower_bounds"])

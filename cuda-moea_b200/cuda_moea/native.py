@@ -95,18 +95,23 @@ class NativeProblem:
         self.schema = schema(self.library)
         if self.schema["name"] != name:
             raise ValueError(f"Library registers {self.schema['name']!r}, not {name!r}")
-        self.name = name
-        self.dimension = dimension
-        self.objectives = objectives
-        self.lower_bounds = lower
-        self.upper_bounds = upper
-        self.parameters = copy.deepcopy(dict(parameters or {}))
-        for key, value in self.parameters.items():
+        self._config = {"type": "NativeProblem", "library": str(self.library), "name": name,
+                        "dimension": dimension, "objectives": objectives,
+                        "lower_bounds": lower, "upper_bounds": upper,
+                        "parameters": copy.deepcopy(dict(parameters or {}))}
+        for key, value in self._config["parameters"].items():
             if key not in self.schema["parameters"]:
                 raise ValueError(f"Unknown native problem parameter: {key}")
             kind = self.schema["parameters"][key]["type"]
             if not _VALID[kind](value):
                 raise ValueError(f"Native parameter {key!r} must be {kind}")
+
+    name = property(lambda self: self._config["name"])
+    dimension = property(lambda self: self._config["dimension"])
+    objectives = property(lambda self: self._config["objectives"])
+    lower_bounds = property(lambda self: list(self._config["lower_bounds"]))
+    upper_bounds = property(lambda self: list(self._config["upper_bounds"]))
+    parameters = property(lambda self: copy.deepcopy(self._config["parameters"]))
 
     @staticmethod
     def _bounds(value, dimension):
@@ -117,16 +122,16 @@ class NativeProblem:
         return [struct.unpack("f", struct.pack("f", x))[0] for x in values]
 
     def _spec(self) -> dict:
-        return {"type": "NativeProblem", "library": str(self.library), "name": self.name,
-                "dimension": self.dimension, "objectives": self.objectives,
-                "lower_bounds": list(self.lower_bounds), "upper_bounds": list(self.upper_bounds),
-                "parameters": copy.deepcopy(self.parameters)}
+        return copy.deepcopy(self._config)
 
 
 class NativeInstance:
     """One constructed plugin problem (the library loaded, the evaluator
     created); closed when garbage-collected.  ``ptr`` is the user pointer of
-    the algorithm's evaluate / prepare / reset hooks."""
+    the algorithm's evaluate / prepare / reset hooks.  The specification is
+    checked again against the library's schema here, since it may have been
+    changed after the NativeProblem was made (the reference's bridge does the
+    same, python/csrc/native_problem.cpp:38-44, 86-92)."""
 
     def __init__(self, spec: dict):
         self.handle = _open(spec["library"])
@@ -134,8 +139,12 @@ class NativeInstance:
             kinds = _schema_of(self.handle)["parameters"]
             L = lib()
             for key, value in spec["parameters"].items():
-                k = key.encode()
+                if key not in kinds:
+                    raise ValueError(f"Unknown native problem parameter: {key}")
                 kind = kinds[key]["type"]
+                if not _VALID[kind](value):
+                    raise ValueError(f"Invalid type/value for native parameter '{key}'")
+                k = key.encode()
                 if kind == "int":
                     check(L.moea_native_set_int(self.handle, k, int(value)))
                 elif kind == "float":
@@ -180,9 +189,11 @@ class NativeInstance:
 
 
 def benchmark(problem: NativeProblem, variables, *, repeats: int = 100, warmup: int = 10) -> dict:
-    """Times full evaluations of ``variables`` ((N, D) CUDA float32 tensor):
-    device time from CUDA events on the current stream and host wall time,
-    both per evaluation, excluding loading and construction."""
+    """Times full evaluations of ``variables`` ((N, D) CUDA float32 tensor),
+    excluding loading and construction: ``cuda_ms_per_eval`` from CUDA events
+    on the current stream (launch gaps included), ``wall_ms_per_eval`` host
+    time including the final wait.  Same keys as the reference's
+    benchmark_problem."""
     import torch
     x = variables.to(dtype=torch.float32).contiguous()
     if not x.is_cuda or x.dim() != 2 or x.shape[1] != problem.dimension:
@@ -209,8 +220,8 @@ def benchmark(problem: NativeProblem, variables, *, repeats: int = 100, warmup: 
         e1.record(stream)
         e1.synchronize()
         wall = time.perf_counter() - t0
-    return {"repeats": repeats, "size": N, "cuda_ms": e0.elapsed_time(e1) / repeats,
-            "wall_ms": 1e3 * wall / repeats}
+    return {"repeats": repeats, "size": N, "cuda_ms_per_eval": e0.elapsed_time(e1) / repeats,
+            "wall_ms_per_eval": 1e3 * wall / repeats}
 
 
 def main(argv=None) -> None:

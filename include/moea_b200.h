@@ -38,7 +38,8 @@ enum {
     MOEA_ERR_STATE = 4,            /* reference: std::logic_error */
     MOEA_ERR_DEVICE_TIMEOUT = 5,   /* a bounded device-side wait gave up */
     MOEA_ERR_OUT_OF_MEMORY = 6,
-    MOEA_ERR_CALLBACK = 7          /* a user callback reported failure */
+    MOEA_ERR_CALLBACK = 7,         /* a user callback reported failure */
+    MOEA_ERR_LOAD = 8              /* a plugin library did not load (reference: std::runtime_error) */
 };
 
 /* Version of this ABI (MOEA_ABI_VERSION). */

@@ -102,4 +102,57 @@ def test_plugin_benchmark(spheres_lib):
     x = torch.rand((4096, D), device="cuda") * 3 - 1
     out = native.benchmark(_problem(spheres_lib), x, repeats=20, warmup=3)
     assert out["size"] == 4096 and out["repeats"] == 20
-    assert out["cuda_ms"] > 0 and out["wall_ms"] > 0
+    assert out["cuda_ms_per_eval"] > 0 and out["wall_ms_per_eval"] > 0
+
+
+# The reference's example plugin (examples/native/bi_sphere) compiled unchanged
+# against this SDK by oracle/ref/Makefile; the two cases follow the reference's
+# GPU plugin tests (tests/python/test_native_problem.py:234-270).
+BI_SPHERE = HERE.parent / "oracle" / "_ref" / "bi_sphere" / "problem.so"
+needs_bi_sphere = pytest.mark.skipif(not BI_SPHERE.is_file(), reason="reference example plugin not built")
+
+
+def _bi_sphere(**kwargs):
+    options = dict(library=BI_SPHERE, name="BiSphere", dimension=7, objectives=2,
+                   lower_bounds=-5.0, upper_bounds=5.0)
+    options.update(kwargs)
+    return cm.NativeProblem(**options)
+
+
+@needs_bi_sphere
+def test_reference_plugin_unconstrained_and_benchmark():
+    p = _bi_sphere(parameters={"offset": 2.0})
+    algo = cm.NSGA3(problem=p, population_size=32, max_generations=1, enable_warmup=False, print_progress=False)
+    result = algo.run()
+    torch.testing.assert_close(result.constraints, torch.zeros_like(result.constraints))
+    timing = native.benchmark(p, result.variables, repeats=3, warmup=1)
+    assert timing["wall_ms_per_eval"] > 0
+    assert timing["cuda_ms_per_eval"] > 0
+
+
+@needs_bi_sphere
+@pytest.mark.parametrize("algorithm", [cm.NSGA3, cm.RVEA])
+@pytest.mark.parametrize("dimension", [7, 129])
+def test_reference_plugin_objectives_constraints_streams_reset_and_lifetime(algorithm, dimension):
+    import gc
+    p = _bi_sphere(dimension=dimension, parameters={"offset": 1.5, "radius": 2.0, "constrained": True})
+    with torch.cuda.stream(torch.cuda.Stream()):
+        algo = algorithm(problem=p, population_size=32, max_generations=2, enable_warmup=False,
+                         print_progress=False)
+        algo.initialize()
+        for action in (lambda: None, algo.step, algo.reset):
+            action()
+            population = algo.population
+            valid = torch.isfinite(population.variables).all(1)
+            assert valid.any()
+            x = population.variables[valid]
+            expected = torch.stack((x.square().sum(1), (x - 1.5).square().sum(1)), 1)
+            torch.testing.assert_close(population.objectives[valid], expected, rtol=2e-5, atol=2e-4)
+            torch.testing.assert_close(population.constraints[valid], (expected[:, 0] - 4).clamp_min(0),
+                                       rtol=2e-5, atol=2e-4)
+        del population, x, expected, valid
+        result = algo.run(copy=False)
+        del algo, p
+        gc.collect()
+        assert result.active_count > 0
+        assert torch.isfinite(result.objectives[:result.active_count]).all()

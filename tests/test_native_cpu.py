@@ -101,3 +101,68 @@ def test_never_mode_clean_and_export(spheres_lib, tmp_path_factory):
         native.export_problem(spheres_lib, out)
     with pytest.raises(ValueError):
         native.build_problem(PLUGINS / "weighted_spheres", cache_dir=PLUGINS / "weighted_spheres" / "c")
+
+
+# The reference's example plugin (examples/native/bi_sphere), compiled unchanged
+# against this SDK by oracle/ref/Makefile; present where the reference's sources
+# were available to the build.  The cases follow the reference's own plugin
+# tests (tests/python/test_native_problem.py:159-232).
+BI_SPHERE = HERE.parent / "oracle" / "_ref" / "bi_sphere" / "problem.so"
+needs_bi_sphere = pytest.mark.skipif(not BI_SPHERE.is_file(), reason="reference example plugin not built")
+
+
+def _bi_sphere(**kwargs):
+    options = dict(library=BI_SPHERE, name="BiSphere", dimension=7, objectives=2,
+                   lower_bounds=-5.0, upper_bounds=5.0)
+    options.update(kwargs)
+    return native.NativeProblem(**options)
+
+
+@needs_bi_sphere
+def test_reference_plugin_registration_and_algorithm_construction():
+    import gc
+    import cuda_moea as cm
+    p = _bi_sphere(parameters={"offset": 4.0, "constrained": True})
+    assert p.schema["name"] == "BiSphere"
+    assert p.schema["parameters"]["radius"]["default"] == 3.0
+    assert p.schema["parameters"]["offset"]["default"] == 2.0
+    assert p.schema["parameters"]["constrained"] == {
+        "type": "bool", "default": False, "description": "Enable sum(x*x) <= radius*radius"}
+    assert p._spec()["type"] == "NativeProblem"
+    for algorithm in (cm.NSGA3, cm.RVEA):
+        instance = algorithm(problem=p, population_size=32, max_generations=2, enable_warmup=False)
+        assert not instance.initialized
+        del instance
+    gc.collect()
+
+
+@needs_bi_sphere
+def test_reference_plugin_parameters_do_not_alias():
+    first = _bi_sphere(parameters={"offset": 1.0})
+    second = _bi_sphere(dimension=129, parameters={"offset": 7.0})
+    assert first.library == second.library
+    spec = first._spec()
+    spec["parameters"]["offset"] = 99
+    assert first._spec()["parameters"]["offset"] == 1.0
+
+
+@needs_bi_sphere
+def test_reference_plugin_invalid_parameters_names_and_dimensions():
+    import cuda_moea as cm
+    for params in ({"offest": 2}, {"offset": True}, {"offset": float("nan")}, {"constrained": 1}):
+        with pytest.raises(ValueError):
+            _bi_sphere(parameters=params)
+    with pytest.raises(ValueError):
+        _bi_sphere(name="unknown")
+    with pytest.raises(ValueError):
+        _bi_sphere(lower_bounds=5.0)
+    with pytest.raises(ValueError, match="objectives=2"):
+        cm.NSGA3(problem=_bi_sphere(objectives=3))
+    # the algorithm checks the specification again
+    p = _bi_sphere()
+    p._config["parameters"] = {"offset": True}
+    with pytest.raises(ValueError, match="Invalid type/value"):
+        cm.NSGA3(problem=p)
+    p._config["parameters"] = {"radius": -1.0}
+    with pytest.raises(ValueError, match="nonnegative"):
+        cm.NSGA3(problem=p)
