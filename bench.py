@@ -260,8 +260,9 @@ OTHER_WORKLOADS = {
                         algo="NSGA3", problem=("DTLZ2", 12, 3), N=92, T=100, dirs=("dd", 12)),
     "rvea-large-d": dict(desc="RVEA DTLZ2 M=8 D=131072 N=1024, adaptive two-layer directions, 100-generation run",
                          algo="RVEA", problem=("DTLZ2", 131072, 8), N=1024, T=100, dirs=None),
-    "c1dtlz1-m10": dict(desc="constrained NSGA-III C1-DTLZ1 M=10 D=14 N=16384, 100-generation run",
-                        algo="NSGA3", problem=("C1DTLZ1", 14, 10), N=16384, T=100, dirs=None),
+    "c1dtlz1-m10": dict(desc="constrained NSGA-III C1-DTLZ1 M=10 D=14 N=16384, two-layer (3,2) user "
+                             "directions (275), 100-generation run",
+                        algo="NSGA3", problem=("C1DTLZ1", 14, 10), N=16384, T=100, dirs=("two", 3, 2)),
     # many objectives: the default association is the tensor-core search here
     "dtlz2-m8": dict(desc="NSGA-III DTLZ2 M=8 D=17 N=6436, Das-Dennis H=8 (6435 directions), 100-generation run",
                      algo="NSGA3", problem=("DTLZ2", 17, 8), N=6436, T=100, dirs=("dd", 8)),
@@ -312,8 +313,10 @@ def other_workload(args, torch, cm):
     w = OTHER_WORKLOADS[args.workload]
     kind, D, M = w["problem"]
     kw = {}
-    if w["dirs"]:
+    if w["dirs"] and w["dirs"][0] == "dd":
         kw["reference_directions"] = cm.DasDennisDirections(w["dirs"][1])
+    elif w["dirs"]:
+        kw["reference_directions"] = cm.UserDefinedDirections(cm.two_layer_directions(M, *w["dirs"][1:]))
     algo = cm.Algorithm(w["algo"], population_size=w["N"], max_generations=w["T"],
                         problem=getattr(cm, kind)(D, M), seed=args.seed, print_progress=False, **kw)
     stream = torch.cuda.current_stream()
@@ -339,7 +342,7 @@ def other_workload(args, torch, cm):
            "config": {"workload": w["desc"], "cuda_graph": graph_on, "kernels_per_generation": kernels,
                       "l2": "flushed (256 MiB write) before every timed generation"},
            "clocks": clocks.summary()}
-    if args.workload == "dtlz2-m8":
+    if args.workload in ("dtlz2-m8", "c1dtlz1-m10"):
         out["stages_ms"] = dict(algo.profile_step())
     if args.workload == "rvea-large-d":
         # streamed bytes of one generation's variation + evaluation: read the two
@@ -357,6 +360,84 @@ def other_workload(args, torch, cm):
     print(json.dumps(out))
 
 
+CONSTRAINED_BATCH = ("batched constrained NSGA-III: 64 seeds per launch of C1-DTLZ1 and of C3-DTLZ4, M=10, D=14, "
+                     "N=16384, two-layer (3,2) user directions (275), 100-generation runs")
+
+
+def constrained_batch(args, torch, cm):
+    """The constrained ten-objective configuration: for each problem, 64
+    seeded instances advance together (one graph launch per generation,
+    instances as parallel branches), against the same instances looped
+    through the plain path; afterwards every instance's ranks and objectives
+    are compared.  value = instance-generations/s over both problems."""
+    D, M, N, T, seeds = 14, 10, 16384, 100, 64
+    dirs = cm.two_layer_directions(M, 3, 2)
+    warm, K = max(args.warmup, 3), max(1, min(args.steps, 5))
+
+    def make(kind, seed):
+        return cm.NSGA3(population_size=N, max_generations=T, problem=getattr(cm, kind)(D, M), seed=seed,
+                        reference_directions=cm.UserDefinedDirections(dirs), print_progress=False)
+
+    records, batch_total, plain_total, gens = [], 0.0, 0.0, 0
+    with ClockSampler(0) as clocks:
+        for kind in ("C1DTLZ1", "C3DTLZ4"):
+            batch = cm.Batch([make(kind, s) for s in range(seeds)])
+            batch.run(warm)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(batch.stream)
+            for _ in range(K):
+                batch.step()
+            e1.record(batch.stream)
+            torch.cuda.synchronize()
+            batch_ms = e0.elapsed_time(e1)
+            shared = torch.cuda.Stream()
+            with torch.cuda.stream(shared):
+                plain = [make(kind, s) for s in range(seeds)]
+                for a in plain:
+                    a.initialize()
+                for _ in range(warm):
+                    for a in plain:
+                        a.step()
+                torch.cuda.synchronize()
+                p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                p0.record(shared)
+                for _ in range(K):
+                    for a in plain:
+                        a.step()
+                p1.record(shared)
+                torch.cuda.synchronize()
+            plain_ms = p0.elapsed_time(p1)
+            identical = True
+            feasible = 0
+            for i, a in enumerate(plain):
+                r_b, r_p = batch.result(i), a.result()
+                identical &= bool(torch.equal(r_b.auxiliary_indices, r_p.auxiliary_indices))
+                identical &= bool(torch.equal(r_b.objectives, r_p.objectives))
+                identical &= bool(torch.equal(r_b.constraints, r_p.constraints))
+                feasible += int((r_b.constraints == 0).sum())
+            records.append({"problem": kind, "instances": seeds, "generations_timed": K,
+                            "instance_gen_per_s": seeds * K / (batch_ms / 1e3),
+                            "plain_loop_instance_gen_per_s": seeds * K / (plain_ms / 1e3),
+                            "speedup_vs_plain_loop": plain_ms / batch_ms, "identical_ranks": identical,
+                            "feasible_fraction": feasible / (seeds * N), "fused": batch.fused,
+                            "graph_kernels_per_generation": batch.graph_kernels})
+            batch_total += batch_ms
+            plain_total += plain_ms
+            gens += seeds * K
+            batch.close()
+            del plain, batch
+            torch.cuda.empty_cache()
+    print(json.dumps({
+        "metric": "batched constrained NSGA-III instance-gen/s", "value": gens / (batch_total / 1e3),
+        "unit": "instance-gen/s", "n_gpus": 1, "steps": K, "warmup": warm,
+        "ms_per_step": batch_total / (2 * K), "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": CONSTRAINED_BATCH, "directions": int(dirs.shape[0]),
+                   "l2": "inputs larger than L2 (64 dominance relations of 128 MiB per generation)"},
+        "clocks": clocks.summary(), "plain_loop_value": gens / (plain_total / 1e3),
+        "records": records}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -371,7 +452,8 @@ def main() -> None:
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the association-search comparison")
-    ap.add_argument("--workload", default="dtlz1-n32768", choices=["dtlz1-n32768", *OTHER_WORKLOADS])
+    ap.add_argument("--workload", default="dtlz1-n32768",
+                    choices=["dtlz1-n32768", "constrained-batch", *OTHER_WORKLOADS])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -382,7 +464,10 @@ def main() -> None:
     if args.workload != "dtlz1-n32768":
         import cuda_moea as cm
         torch.cuda.set_stream(torch.cuda.Stream(0))
-        other_workload(args, torch, cm)
+        if args.workload == "constrained-batch":
+            constrained_batch(args, torch, cm)
+        else:
+            other_workload(args, torch, cm)
         return
     import torch.distributed as dist
     import cuda_moea as cm

@@ -17,7 +17,7 @@ from ._specs import (
     NSGA3EnvironmentSelector, NoMutation, PolynomialMutation,
     PythonCrossover, PythonEnvironmentSelector, PythonMating, PythonMutation,
     PythonReferenceDirections, RandomMating, RVEAEnvironmentSelector, SBX,
-    TournamentMating, UserDefinedDirections,
+    TournamentMating, UserDefinedDirections, two_layer_directions,
 )
 
 __version__ = "0.2.0+b200"
@@ -30,6 +30,7 @@ __all__ = [
     "NSGA3EnvironmentSelector", "RVEAEnvironmentSelector",
     "PythonProblem", "PythonMating", "PythonCrossover", "PythonMutation",
     "PythonReferenceDirections", "PythonEnvironmentSelector", "NativeProblem",
+    "two_layer_directions",
 ] + _problem.__all__
 
 

@@ -181,3 +181,35 @@ def specification(value: Any) -> dict[str, Any]:
     if not hasattr(value, "_spec"):
         raise TypeError(f"{value!r} is not a cuda_moea strategy")
     return value._spec()
+
+
+def two_layer_directions(objectives: int, outer: int, inner: int) -> "torch.Tensor":
+    """Two-layer Das-Dennis directions with explicit partitions (Deb & Jain,
+    NSGA-III, 2014): every composition of ``outer`` into ``objectives`` parts
+    divided by ``outer``, then every composition of ``inner`` divided by
+    ``inner`` and moved halfway to the centroid (v + 1/M) / 2.  Returns an
+    (count, objectives) float32 CPU tensor for ``UserDefinedDirections``
+    (which normalises each row to unit length): the reference's providers pick
+    the layers from the population size, so an explicit (outer, inner) pair
+    such as (3, 2) at ten objectives (220 + 55 = 275 directions) is reached
+    through user-defined directions there too."""
+    import itertools
+
+    import numpy as np
+    import torch
+
+    if objectives < 1 or outer < 1 or inner < 0:
+        raise ValueError("objectives and outer must be positive, inner nonnegative")
+
+    def layer(h: int) -> np.ndarray:
+        # compositions of h into M parts by stars and bars, in lexicographic order
+        rows = []
+        for bars in itertools.combinations(range(h + objectives - 1), objectives - 1):
+            edges = (-1,) + bars + (h + objectives - 1,)
+            rows.append([edges[i + 1] - edges[i] - 1 for i in range(objectives)])
+        return np.asarray(rows, np.float64) / h
+
+    parts = [layer(outer)]
+    if inner > 0:
+        parts.append(0.5 * (layer(inner) + 1.0 / objectives))
+    return torch.from_numpy(np.concatenate(parts).astype(np.float32))

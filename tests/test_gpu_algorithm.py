@@ -75,17 +75,36 @@ def test_python_problem_streams_reset_lifetime(algorithm, dimension):
         assert torch.isfinite(result.objectives[:result.active_count]).all()
 
 
-def test_nsga3_trajectory_matches_oracle_selection(oracle):
+TRAJECTORIES = [
+    # (problem, D, M, N, generations, seed, two-layer directions or None)
+    ("DTLZ1", 7, 3, 200, 6, 77, None),
+    # the constrained ten-objective configuration, two-layer (3, 2) = 275
+    # user-defined directions; beyond the reference's eight objectives, so the
+    # oracle alone is the check
+    ("C1DTLZ1", 14, 10, 400, 5, 5, (3, 2)),
+    ("C3DTLZ4", 14, 10, 400, 5, 6, (3, 2)),
+]
+
+
+@pytest.mark.parametrize("kind,D,M,N,T,seed,layers", TRAJECTORIES)
+def test_nsga3_trajectory_matches_oracle_selection(oracle, kind, D, M, N, T, seed, layers):
     """Each generation: offspring from the fused reproduction kernel (same
     Philox streams as the algorithm), objectives from the problem kernel, then
     the oracle's NSGA-III selection must reproduce the algorithm's next
     parents exactly (survivor set, fronts, objectives, niching RNG offset)."""
     from cuda_moea import stages
-    N, D, M, T, seed = 200, 7, 3, 6, 77
-    algo = cm.NSGA3(population_size=N, max_generations=T, problem=cm.DTLZ1(D, M), seed=seed,
-                    print_progress=False, use_graphs=False)
+    from cuda_moea.problem import PROBLEM_KINDS
+    kw = {}
+    if layers is not None:
+        kw["reference_directions"] = cm.UserDefinedDirections(cm.two_layer_directions(M, *layers))
+    algo = cm.NSGA3(population_size=N, max_generations=T, problem=getattr(cm, kind)(D, M), seed=seed,
+                    print_progress=False, use_graphs=False, **kw)
     algo.initialize()
-    refs = oracle.reference_directions(0, N, M)
+    if layers is None:
+        refs = oracle.reference_directions(0, N, M)
+    else:
+        refs = algo.reference_directions.cpu().numpy().copy()
+        assert refs.shape == (M, 275)
     pop = algo.population
     par_x = pop.variables.clone()
     par_f = pop.objectives.t().contiguous().cpu().numpy()
@@ -96,12 +115,14 @@ def test_nsga3_trajectory_matches_oracle_selection(oracle):
     bounds = torch.tile(torch.tensor([0.0, 1.0]), (D,)).cuda()
     dseed = oracle.derive_seed(seed)
     offset = 0
+    constrained = False
     for g in range(T):
         off_x, _ = stages.reproduce(par_x, torch.from_numpy(par_cv).cuda(), rank, N, bounds, N,
                                     seed=dseed, generation=g)
-        off_f, off_cv = stages.problem_evaluate(1, off_x, M)
+        off_f, off_cv = stages.problem_evaluate(PROBLEM_KINDS[kind], off_x, M)
         mix_f = np.concatenate([par_f, off_f.cpu().numpy()], 1)
         mix_cv = np.concatenate([par_cv, off_cv.cpu().numpy()])
+        constrained |= bool((mix_cv > 0).any())
         want = oracle.nsga3_select(mix_cv, mix_f, refs, dseed, offset, ideal)
         offset, ideal = want["offset"], want["ideal"]
         algo.step()
@@ -110,10 +131,13 @@ def test_nsga3_trajectory_matches_oracle_selection(oracle):
         mix_x = torch.cat([par_x, off_x]).cpu().numpy()
         np.testing.assert_array_equal(pop.variables.cpu().numpy(), mix_x[surv])
         np.testing.assert_array_equal(pop.objectives.t().cpu().numpy(), mix_f[:, surv])
+        np.testing.assert_array_equal(pop.constraints.cpu().numpy(), mix_cv[surv])
         par_x = pop.variables.clone()
         par_f = pop.objectives.t().contiguous().cpu().numpy()
         par_cv = pop.constraints.cpu().numpy().copy()
         rank = torch.from_numpy(want["fronts"]).cuda()
+    if kind.startswith("C"):
+        assert constrained  # the violation-first dominance was exercised
 
 
 @pytest.mark.parametrize("kind", ["NSGA3", "RVEA"])
