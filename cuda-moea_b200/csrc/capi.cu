@@ -153,6 +153,8 @@ int workspace_check_status(Workspace& ws, cudaStream_t stream)
             return set_error(MOEA_ERR_DEVICE_TIMEOUT, "front peeling: grid barrier timed out");
         if (st == kDevTensorTimeout)
             return set_error(MOEA_ERR_DEVICE_TIMEOUT, "association: tensor-core wait timed out");
+        if (st == kDevNichingSize)
+            return set_error(MOEA_ERR_UNSUPPORTED, "niching: last front exceeds the cluster's capacity");
         return set_error(MOEA_ERR_CUDA, "front peeling: inconsistent dominance relation (status %d)", st);
     }
     return MOEA_OK;

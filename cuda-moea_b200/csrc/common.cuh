@@ -127,6 +127,7 @@ enum DeviceStatus : int {
     kDevBarrierTimeout = 1,
     kDevPeelInconsistent = 2,
     kDevTensorTimeout = 3,      // a wait of the tensor-core association ran out
+    kDevNichingSize = 4,        // a last front larger than the niching cluster holds
 };
 
 }  // namespace moea

@@ -197,6 +197,13 @@ int prepare_direction_tree(Workspace& ws, const float* d_refs, const float* h_re
                            cudaStream_t stream);
 bool direction_tree_ready(const Workspace& ws, const float* d_refs, int M, int H);
 
+// Niching of the last front on one 16-CTA cluster (niching_cluster.cu):
+// merged populations up to niching_cluster_capacity() members.
+int niching_cluster_capacity();
+bool niching_cluster_ready();
+int launch_niching_cluster(const int* idx, const float* dist, const int* sizes, const int* rho, int H,
+                           uint64_t seed, unsigned long long* offset, const int* nds_gidx, int* selected,
+                           int* status, cudaStream_t stream);
 int run_niching(Workspace& ws, uint64_t seed, const int* nds_gidx, const float* dist,
                 const int* idx, const int* sizes, int H, int N, int* selected,
                 cudaStream_t stream);

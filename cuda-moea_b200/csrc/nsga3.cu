@@ -258,6 +258,24 @@ __device__ __forceinline__ void norm_solve(const float* __restrict__ nds, int nd
         int bad = s_bad;
         if (!bad) {
             for (int sweep = 0; sweep < 60; ++sweep) {
+                // A rotation leaves its two columns with the eigenvalues of their
+                // 2x2 Gram matrix, so the smallest column norm never grows and the
+                // largest never shrinks: once the current norms fail the
+                // conditioning test below, the converged ones fail it too, and
+                // the fallback (which ignores the rotations) is the result.
+                // Degenerate extreme points (repeated rows) stop here instead of
+                // rotating rounding noise for all 60 sweeps.
+                double cmax = 0.0, cmin = INFINITY;
+                for (int i = 0; i < M; ++i) {
+                    const double x = (lane < M) ? sA[lane][i] : 0.0;
+                    const double sg = sqrt(warp_sum_d(x * x));
+                    cmax = fmax(cmax, sg);
+                    cmin = fmin(cmin, sg);
+                }
+                if (cmin < 1e-10 || cmax / cmin > 1e6) {
+                    bad = 1;
+                    break;
+                }
                 int rotated = 0;
                 for (int i = 0; i < M - 1; ++i) {
                     for (int j = i + 1; j < M; ++j) {
@@ -285,7 +303,7 @@ __device__ __forceinline__ void norm_solve(const float* __restrict__ nds, int nd
                 if (!rotated) break;
             }
             double smax = 0.0, smin = INFINITY;
-            for (int i = 0; i < M; ++i) {
+            for (int i = 0; i < M && !bad; ++i) {
                 const double x = (lane < M) ? sA[lane][i] : 0.0;
                 const double sg = sqrt(warp_sum_d(x * x));
                 if (lane == 0) s_sigma[i] = sg;
@@ -1397,6 +1415,12 @@ int run_niching(Workspace& ws, uint64_t seed, const int* nds_gidx, const float* 
     const int T = 256, G = ceil_div(n_cap, T);
     MOEA_CUDA_TRY(cudaMemsetAsync(ws.rho, 0, sizeof(int) * (size_t)H, stream));
     nich_prior<<<G, T, 0, stream>>>(nds_gidx, idx, sizes, H, ws.rho, selected);
+    // the last front in one cluster's shared memory, sorted over its nl members
+    if (n_cap <= niching_cluster_capacity() && niching_cluster_ready()) {
+        MOEA_CUDA_TRY(cudaGetLastError());
+        return launch_niching_cluster(idx, dist, sizes, ws.rho, H, seed, ws.offset_dev, nds_gidx, selected,
+                                      ws.counters + 6, stream);
+    }
     nich_keys1<<<G, T, 0, stream>>>(idx, dist, sizes, n_cap, ws.key64[0], ws.sel_vals[0]);
     size_t tmp = ws.cub_bytes;
     // Bits that order the keys: the high word holds a direction index below

@@ -204,12 +204,25 @@ void orc_ideal_point(const float* objs, int M, int n, float* ideal)
 }
 
 /* One-sided Jacobi SVD of the square matrix a (n x n, row-major, FP64).
- * On return the columns of a hold U*Sigma, v holds V, sigma the column norms. */
-static void jacobi_svd(double* a, double* v, double* sigma, int n)
+ * On return the columns of a hold U*Sigma, v holds V, sigma the column norms.
+ * Returns 1 (ill-conditioned, nothing else set) when the column norms fail
+ * the conditioning test before convergence. */
+static int jacobi_svd(double* a, double* v, double* sigma, int n)
 {
     for (int i = 0; i < n; ++i)
         for (int j = 0; j < n; ++j) v[i * n + j] = (i == j) ? 1.0 : 0.0;
     for (int sweep = 0; sweep < 60; ++sweep) {
+        /* column norms only spread under rotations (each pair ends at the
+         * eigenvalues of its 2x2 Gram matrix): once they fail the
+         * conditioning test the result is the fallback, so stop */
+        double cmax = 0.0, cmin = INFINITY;
+        for (int i = 0; i < n; ++i) {
+            double s = 0.0;
+            for (int k = 0; k < n; ++k) s += a[k * n + i] * a[k * n + i];
+            cmax = fmax(cmax, sqrt(s));
+            cmin = fmin(cmin, sqrt(s));
+        }
+        if (cmin < 1e-10 || cmax / cmin > 1e6) return 1;
         int rotated = 0;
         for (int i = 0; i < n - 1; ++i) {
             for (int j = i + 1; j < n; ++j) {
@@ -241,6 +254,7 @@ static void jacobi_svd(double* a, double* v, double* sigma, int n)
         for (int k = 0; k < n; ++k) s += a[k * n + i] * a[k * n + i];
         sigma[i] = sqrt(s);
     }
+    return 0;
 }
 
 /* Reciprocal intercepts from the extreme points (normalization.cu:739-856,
@@ -255,7 +269,7 @@ static int intercepts_fp64(const float* E /* row-major [m][j] */, int M, double*
             if (!isfinite(e)) return 1;
             a[j * M + m] = (double)e;
         }
-    jacobi_svd(a, v, sg, M);
+    if (jacobi_svd(a, v, sg, M)) return 1;
     double smax = 0.0, smin = INFINITY;
     for (int i = 0; i < M; ++i) {
         if (!isfinite(sg[i])) return 1;

@@ -293,6 +293,37 @@ def test_niching_bit_exact(st, ws, oracle):
         np.testing.assert_array_equal(sel_g.cpu().numpy(), sel_w)
 
 
+@pytest.mark.parametrize("np_,nl,N,H,ties", [
+    (0, 65536, 32768, 32640, False),    # the whole merged population in the last front
+    (31000, 1800, 32768, 32640, False),  # a typical headline generation
+    (20000, 45536, 32768, 500, True),    # large niches, many equal distances
+    (32767, 1, 32768, 91, False),        # one member
+    (0, 4097, 2100, 7, True),            # uneven slices, few directions
+])
+def test_niching_large_last_front(st, oracle, np_, nl, N, H, ties):
+    """The last front's three stable sorts at the merged sizes of the
+    headline workload (up to 65536 members), against the oracle."""
+    rng = np.random.default_rng(nl + H)
+    ws_big = st.Workspace(2 * N, 3, H)
+    try:
+        nds = np_ + nl
+        gidx = rng.permutation(2 * N)[:nds].astype(np.int32)
+        idx = rng.integers(0, H, nds).astype(np.int32)
+        idx[rng.integers(0, nds, 3)] = -1  # members without a direction sort last
+        if ties:
+            dist = (rng.integers(0, 9, nds) / 3.0).astype(np.float32)
+        else:
+            dist = rng.random(nds).astype(np.float32)
+        sizes = np.array([np_, nl, N - np_, nds], np.int32)
+        for offset in (0, 123456789):
+            sel_w, off_w = oracle.niching(2887, offset, gidx, dist, idx, sizes, H, N)
+            sel_g, off_g = st.niching(ws_big, 2887, offset, _t(gidx), _t(dist), _t(idx), _t(sizes), H, N)
+            assert off_g == off_w
+            np.testing.assert_array_equal(sel_g.cpu().numpy(), sel_w)
+    finally:
+        ws_big.close()
+
+
 @pytest.mark.parametrize("seed,M,N,kind", [(0, 3, 92, "dtlz1"), (1, 3, 1024, "dtlz1"),
                                            (2, 3, 2048, "uniform"), (3, 5, 600, "ties"),
                                            (4, 8, 512, "uniform"), (5, 3, 4096, "correlated")])
