@@ -74,7 +74,7 @@ void free_all(Workspace& ws)
                     ws.assoc_idx, ws.assoc_dist, ws.rho, ws.sel_vals[0], ws.sel_vals[1],
                     ws.rank, ws.selected, ws.flags, ws.offset_dev, ws.cub_tmp, ws.tree_dirs,
                     ws.tree_order, ws.tree_center, ws.dir_delta, ws.chunk_keys, ws.chunk_bits,
-                    ws.scalar_d, ws.tc_dirs, ws.tc_rowmax};
+                    ws.scalar_d, ws.tc_dirs, ws.tc_rowmax, ws.peel_fmask};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     ws = Workspace{};
@@ -134,6 +134,7 @@ int workspace_init(Workspace& ws, int device, int n_max, int m_max, int h_max)
         if (e != cudaSuccess) st = set_error(MOEA_ERR_CUDA, "cudaMemset: %s", cudaGetErrorString(e));
     }
     if (st == MOEA_OK) st = configure_peel(ws);
+    if (st == MOEA_OK) st = dalloc(ws, &ws.peel_fmask, 3 * (size_t)ws.words);
     if (st != MOEA_OK) free_all(ws);
     return st;
 }

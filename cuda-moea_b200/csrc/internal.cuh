@@ -73,14 +73,14 @@ struct Workspace {
     int* blocker = nullptr;         // per sorted position: last known unassigned dominator
     int* front_sorted = nullptr;    // per sorted position: front index or -1
     int* front_list = nullptr;      // members of each peeled front, front by front
-    int* counters = nullptr;        // [0] feasible count, [1] list length, [2] max_front,
-                                    // [3] assigned, [4] barrier count, [5] barrier generation,
-                                    // [6] device status, [9] front-list length at the barrier,
-                                    // [10] class-2 count, [11] class-3 count, [12] last feasible
-                                    // front, [13] long runs of equal sort keys
+    int* counters = nullptr;        // [0] feasible count, [1] list length (batched peel),
+                                    // [2] max_front, [3] assigned, [4] grid-barrier arrivals,
+                                    // [6] device status, [10] class-2 count, [11] class-3 count,
+                                    // [12] last feasible front, [13] long runs of equal sort keys
     int peel_grid = 0;              // co-resident CTAs of the peel kernel
     int peel_smem = 0;
     bool peel_single_cta = false;   // peel with one ordinary CTA (instances of a batch)
+    uint32_t* peel_fmask = nullptr; // [3][words] members of the last three fronts (peel)
 
     // --- NSGA-III stages ---
     int* fronts = nullptr;          // fronts of the merged population (point order)

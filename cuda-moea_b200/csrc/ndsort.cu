@@ -48,7 +48,6 @@ constexpr int kTileThreads = 256;
 constexpr int kPeelThreads = 1024;
 constexpr int kScanQueue = 1024;   // rows per CTA and front for the chunked scan
 constexpr int kScanChunk = 256;    // words per chunk (8 per lane)
-constexpr int kFreeBuf = 2048;     // next-front points buffered per CTA
 constexpr uint32_t kInfeasibleBit = 0x80000000u;
 
 // ---------------------------------------------------------------------------
@@ -498,93 +497,82 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 
-// Grid barrier over co-resident CTAs.  Waits at most ~2 s, then records
-// kDevBarrierTimeout in the status word and returns false.  The last CTA to
-// arrive copies the front-list length (counters[1]) into counters[9] before
-// releasing the others, so every CTA reads the same length after the barrier
-// even when a fast CTA has already started appending the next front.
-__device__ bool grid_barrier(int* counters, unsigned nblocks)
+__device__ __forceinline__ int ld_acquire_gpu(const int* p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid barrier over co-resident CTAs.  The arrivals count up during one
+// launch (counters[4] is zeroed before it): barrier number `epoch` is passed
+// when the count reaches epoch * nblocks, so no CTA resets or releases
+// anything and the wait ends one acquire load after the last arrival.
+// Waits at most ~2 s, then records kDevBarrierTimeout in the status word and
+// returns false.  Every thread of the CTA passes the same epoch.
+__device__ bool grid_barrier(int* counters, unsigned nblocks, int epoch)
 {
     __shared__ int s_ok;
     __syncthreads();
     if (nblocks == 1) {  // single-CTA peel: a block barrier suffices
-        if (threadIdx.x == 0) counters[9] = atomicAdd(counters + 1, 0);
         __syncthreads();
         return true;
     }
     if (threadIdx.x == 0) {
-        volatile int* vgen = counters + 5;
-        volatile int* vstatus = counters + 6;
-        const int g = *vgen;
+        const int target = epoch * (int)nblocks;
         __threadfence();
+        atomicAdd(counters + 4, 1);
         int ok = 1;
-        if (atomicAdd(counters + 4, 1) == (int)nblocks - 1) {
-            counters[9] = atomicAdd(counters + 1, 0);
-            atomicExch(counters + 4, 0);
-            __threadfence();
-            atomicAdd(counters + 5, 1);
-        } else {
-            const unsigned long long t0 = global_ns();
-            while (*vgen == g) {
-                if (*vstatus != 0) { ok = 0; break; }
-                if (global_ns() - t0 > 2000000000ull) {
-                    atomicExch(counters + 6, kDevBarrierTimeout);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
+        const unsigned long long t0 = global_ns();
+        while (ld_acquire_gpu(counters + 4) < target) {
+            if (*((volatile int*)counters + 6) != 0) { ok = 0; break; }
+            if (global_ns() - t0 > 2000000000ull) {
+                atomicExch(counters + 6, kDevBarrierTimeout);
+                ok = 0;
+                break;
             }
+            __nanosleep(32);
         }
-        __threadfence();
         s_ok = ok;
     }
     __syncthreads();
     return s_ok != 0;
 }
 
-// Body of the peel, run by CTA `block` of `nblocks` co-resident CTAs; U is the
-// CTA's bitmask of unassigned positions (W words of shared memory).  blocker
-// may point to global or to shared memory.  kInflight groups of 32 points are
-// examined per round by one warp: their blockers and probe words are loaded
-// before any of them is examined.
-// Appends the lanes with is_free to the CTA's buffer of the next front (one
-// shared atomic per warp); lanes beyond the buffer append to the global list.
-__device__ __forceinline__ void peel_append(bool is_free, int q, int k, int lane, int* s_free, int* s_nfree,
-                                            int* list, int* front_sorted, int* counters)
+// Marks the free lanes of a warp, all in the 32-position group of word gw,
+// as members of front k: one atomicOr into the front's mask per warp.
+__device__ __forceinline__ void peel_mark_group(bool is_free, int q, int gw, int k, int lane, uint32_t* G,
+                                                int* front_sorted)
 {
     const unsigned fm = __ballot_sync(0xFFFFFFFFu, is_free);
     if (!fm) return;
-    int base = 0;
-    if (lane == 0) base = atomicAdd(s_nfree, __popc(fm));
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (is_free) {
-        const int pos = base + __popc(fm & ((1u << lane) - 1u));
-        if (pos < kFreeBuf) s_free[pos] = q;
-        else list[atomicAdd(counters + 1, 1)] = q;
-        front_sorted[q] = k;
-    }
+    if (lane == 0) atomicOr(G + gw, fm);
+    if (is_free) front_sorted[q] = k;
 }
 
+// Body of the peel, run by CTA `block` of `nblocks` co-resident CTAs; U is the
+// CTA's bitmask of unassigned positions (W words of shared memory), the same
+// in every CTA.  Per front k:
+//   1. groups: every alive point whose blocker (an unassigned dominator) was
+//      assigned probes the blocker's row word and the one below; a hit is the
+//      new blocker, no dominator at all makes the point free, and the other
+//      rows are queued;
+//   2. the CTA scans its queued rows in chunks of kScanChunk words, level by
+//      level (the top chunk of every row first);
+//   3. free points set their bit in the front's mask (fmask, three in
+//      rotation, so no CTA appends to a shared list); after one grid barrier
+//      every CTA removes the front from U and counts it.
 template <int kInflight>
 __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
                                           const uint32_t* __restrict__ rows, int W, int n, int target,
                                           const int* __restrict__ qinfo, int* __restrict__ blocker,
-                                          int* __restrict__ front_sorted, int* __restrict__ list,
+                                          int* __restrict__ front_sorted, uint32_t* __restrict__ fmask,
                                           int* counters)
 {
-    __shared__ int s_len;
-    // rows whose probe did not resolve them: scanned by the whole CTA in
-    // chunks of kScanChunk words after the groups of the front
     __shared__ int s_nscan, s_ntask;
     __shared__ int s_sq[kScanQueue], s_sw[kScanQueue], s_found[kScanQueue];
-    // points of the next front found by this CTA, appended to the global list
-    // with one atomic per CTA and front (directly when the buffer is full)
-    __shared__ int s_free[kFreeBuf];
-    __shared__ int s_nfree, s_base;
-    if (threadIdx.x == 0) {
-        s_nscan = 0;
-        s_nfree = 0;
-    }
+    __shared__ int s_wsum[32];
+    if (threadIdx.x == 0) s_nscan = 0;
     for (int w = threadIdx.x; w < W; w += blockDim.x) {
         const int lo = w * 32;
         U[w] = (lo + 32 <= n) ? 0xFFFFFFFFu : (lo >= n ? 0u : ((1u << (n - lo)) - 1u));
@@ -596,7 +584,7 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
     const int gwarp = warp * nblocks + block;
     const int twarps = nblocks * wpb;
     const int ngroups = (n + 31) >> 5;
-    int len_prev = 0, total = 0, k = 0;
+    int total = 0, k = 0, epoch = 0;
     // With fewer feasible points than the target, the peel covers the
     // feasible fronts only; the infeasible fronts follow in closed form
     // (nds_infeasible_fronts).  Without feasible points there is nothing to peel.
@@ -612,6 +600,12 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
     }
 
     for (;;) {
+        uint32_t* G = fmask + (size_t)(k % 3) * W;  // members of front k
+        // the mask front k + 1 will write: last read (as front k - 2's) before
+        // the barrier of front k - 1, written again only after this front's
+        const uint32_t nextw = (uint32_t)((k + 1) % 3);
+        for (int w = block * blockDim.x + threadIdx.x; w < W; w += nblocks * blockDim.x)
+            fmask[(size_t)nextw * W + w] = 0u;
         for (int g0 = gwarp; g0 < ngroups; g0 += twarps * kInflight) {
             int qv[kInflight], bv[kInflight];
             uint32_t hiw[kInflight], low[kInflight];
@@ -622,8 +616,9 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
                 const int q = g * 32 + lane;
                 qv[u] = q;
                 alive[u] = g < ngroups && q < n && ((U[q >> 5] >> (q & 31)) & 1u);
-                // blocker[q] is an unassigned dominator of q, or -1 when nothing dominates q
-                bv[u] = alive[u] ? blocker[q] : -1;
+                // blocker[q] is an unassigned dominator of q, or -1 when nothing
+                // dominates q; whichever CTA resolved q's row wrote it: read through L2
+                bv[u] = alive[u] ? __ldcg(blocker + q) : -1;
             }
 #pragma unroll
             for (int u = 0; u < kInflight; ++u) {
@@ -668,9 +663,8 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
                         }
                     }
                 }
-                // rows not resolved by the probe go to the CTA's scan queue;
-                // when it is full the whole warp scans each of them
-                // downwards, 8 coalesced words per lane in flight
+                // rows not resolved by the probe go to the CTA's list; when it
+                // is full the whole warp scans each of them downwards
                 if (need) {
                     const int slot = atomicAdd(&s_nscan, 1);
                     if (slot < kScanQueue) {
@@ -710,7 +704,7 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
                         else is_free = true;
                     }
                 }
-                peel_append(is_free, q, k, lane, s_free, &s_nfree, list, front_sorted, counters);
+                peel_mark_group(is_free, q, g, k, lane, G, front_sorted);
             }
         }
         __syncthreads();
@@ -774,30 +768,32 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
                     if (f >= 0) blocker[q] = f;
                     else is_free = true;
                 }
-                peel_append(is_free, q, k, lane, s_free, &s_nfree, list, front_sorted, counters);
+                if (is_free) {
+                    atomicOr(G + (q >> 5), 1u << (q & 31));
+                    front_sorted[q] = k;
+                }
             }
         }
         __syncthreads();
-        const int nfree = min(s_nfree, kFreeBuf);
-        if (threadIdx.x == 0) s_base = nfree ? atomicAdd(counters + 1, nfree) : 0;
-        __syncthreads();
-        for (int i = threadIdx.x; i < nfree; i += blockDim.x) list[s_base + i] = s_free[i];
-        if (threadIdx.x == 0) {  // read again only after the barrier below
-            s_nscan = 0;
-            s_nfree = 0;
+        if (threadIdx.x == 0) s_nscan = 0;  // read again only after the barrier below
+        if (!grid_barrier(counters, (unsigned)nblocks, ++epoch)) return;
+        // front k is complete: remove it from U and count it
+        int c = 0;
+        for (int w = threadIdx.x; w < W; w += blockDim.x) {
+            const uint32_t g = __ldcg(G + w);
+            if (g) {
+                U[w] &= ~g;
+                c += __popc(g);
+            }
         }
-        if (!grid_barrier(counters, (unsigned)nblocks)) return;
-        if (threadIdx.x == 0) s_len = *((volatile int*)counters + 9);
+#pragma unroll
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+        if (lane == 0) s_wsum[warp] = c;
         __syncthreads();
-        const int len = s_len;
-        const int ck = len - len_prev;
-        for (int i = threadIdx.x; i < ck; i += blockDim.x) {
-            const int q = __ldcg(list + len_prev + i);
-            atomicAnd(&U[q >> 5], ~(1u << (q & 31)));
-        }
-        __syncthreads();
+        int ck = 0;
+        for (int w = 0; w < wpb; ++w) ck += s_wsum[w];
+        __syncthreads();  // s_wsum is reused by the next front
         total += ck;
-        len_prev = len;
         if (total >= target || ck == 0 || (feasible_only && total >= feasible)) {
             if (block == 0 && threadIdx.x == 0) {
                 counters[2] = k;
@@ -814,11 +810,11 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
 
 __global__ void __launch_bounds__(kPeelThreads, 1)
 nds_peel(const uint32_t* __restrict__ rows, int W, int n, int target, const int* __restrict__ qinfo,
-         int* __restrict__ blocker, int* __restrict__ front_sorted, int* __restrict__ list,
+         int* __restrict__ blocker, int* __restrict__ front_sorted, uint32_t* __restrict__ fmask,
          int* counters)
 {
     extern __shared__ uint32_t U[];  // unassigned positions, one bit each
-    peel_body<1>(blockIdx.x, gridDim.x, U, rows, W, n, target, qinfo, blocker, front_sorted, list, counters);
+    peel_body<1>(blockIdx.x, gridDim.x, U, rows, W, n, target, qinfo, blocker, front_sorted, fmask, counters);
 }
 
 // Run heads among the infeasible class-2 positions (sorted by violation).
@@ -1308,11 +1304,13 @@ int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_f
     const int* qi = qinfo;
     int* blk = ws.blocker;
     int* fs = ws.front_sorted;
-    int* list = ws.front_list;
+    uint32_t* fmask = ws.peel_fmask;
     int* ctr = ws.counters;
     (void)W;
+    // the three front masks start empty
+    MOEA_CUDA_TRY(cudaMemsetAsync(fmask, 0, sizeof(uint32_t) * 3 * (size_t)Wp, stream));
     void* args[] = {(void*)&rows, (void*)&Wp, (void*)&nn, (void*)&tt, (void*)&qi,
-                    (void*)&blk, (void*)&fs, (void*)&list, (void*)&ctr};
+                    (void*)&blk, (void*)&fs, (void*)&fmask, (void*)&ctr};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kPeelThreads);
@@ -1326,7 +1324,7 @@ int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_f
     if (grid == 1) {
         // one CTA needs no co-residency guarantee: an ordinary launch, which
         // may run beside other work (batched instances)
-        nds_peel<<<1, kPeelThreads, cfg.dynamicSmemBytes, stream>>>(rows, Wp, nn, tt, qi, blk, fs, list,
+        nds_peel<<<1, kPeelThreads, cfg.dynamicSmemBytes, stream>>>(rows, Wp, nn, tt, qi, blk, fs, fmask,
                                                                     ctr);
     } else {
         MOEA_CUDA_TRY(cudaLaunchKernelExC(&cfg, (const void*)nds_peel, args));
