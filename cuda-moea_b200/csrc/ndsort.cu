@@ -47,6 +47,7 @@ constexpr int kQB = 128;      // sorted positions (dominatees) per tile CTA
 constexpr int kTileThreads = 256;
 constexpr int kPeelThreads = 1024;
 constexpr int kScanQueue = 1024;   // rows per CTA and front for the chunked scan
+constexpr int kProbeWords = 16;    // row words probed below an assigned blocker
 constexpr int kScanChunk = 256;    // words per chunk (8 per lane)
 constexpr uint32_t kInfeasibleBit = 0x80000000u;
 
@@ -608,7 +609,7 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
             fmask[(size_t)nextw * W + w] = 0u;
         for (int g0 = gwarp; g0 < ngroups; g0 += twarps * kInflight) {
             int qv[kInflight], bv[kInflight];
-            uint32_t hiw[kInflight], low[kInflight];
+            uint32_t pw[kInflight][kProbeWords];
             bool alive[kInflight], probe[kInflight];
 #pragma unroll
             for (int u = 0; u < kInflight; ++u) {
@@ -623,16 +624,18 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
 #pragma unroll
             for (int u = 0; u < kInflight; ++u) {
                 const int b = bv[u];
-                // blocker assigned: probe its word and the one below; bits
-                // above it were already free of unassigned dominators
+                // blocker assigned: probe its word and the kProbeWords - 1
+                // below it; bits above it were already free of unassigned
+                // dominators
                 probe[u] = alive[u] && b >= 0 && !((U[b >> 5] >> (b & 31)) & 1u);
-                hiw[u] = 0u;
-                low[u] = 0u;
+#pragma unroll
+                for (int i = 0; i < kProbeWords; ++i) pw[u][i] = 0u;
                 if (probe[u]) {
                     const uint32_t* row = rows + (size_t)qv[u] * W;
                     const int w = b >> 5;
-                    hiw[u] = __ldg(row + w);
-                    if (w > 0) low[u] = __ldg(row + w - 1);
+#pragma unroll
+                    for (int i = 0; i < kProbeWords; ++i)
+                        if (w - i >= 0) pw[u][i] = __ldg(row + w - i);
                 }
             }
 #pragma unroll
@@ -647,19 +650,20 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
                     if (b < 0) {
                         is_free = true;
                     } else if (probe[u]) {
-                        int w = b >> 5;
-                        uint32_t bits = hiw[u] & U[w];
-                        if (!bits && w > 0) {
-                            --w;
-                            bits = low[u] & U[w];
+                        const int w = b >> 5;
+                        int hit = -1;
+#pragma unroll
+                        for (int i = 0; i < kProbeWords; ++i) {
+                            const uint32_t bits = (w - i >= 0) ? (pw[u][i] & U[w - i]) : 0u;
+                            if (hit < 0 && bits) hit = (w - i) * 32 + (31 - __clz(bits));
                         }
-                        if (bits) {
-                            blocker[q] = w * 32 + (31 - __clz(bits));
-                        } else if (w == 0) {
+                        if (hit >= 0) {
+                            blocker[q] = hit;
+                        } else if (w - kProbeWords < 0) {
                             is_free = true;
                         } else {
                             need = true;
-                            start_w = w - 1;
+                            start_w = w - kProbeWords;
                         }
                     }
                 }
