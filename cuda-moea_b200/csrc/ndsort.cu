@@ -1298,8 +1298,10 @@ int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_f
 
     // cooperative peel
     const int W = ceil_div(n, 32);
-    const int wpb = kPeelThreads / 32;
-    int grid = ceil_div(ceil_div(n, 32), wpb);
+    // every co-resident CTA with at least one group of 32 positions: each
+    // CTA scans the rows of its own groups, so more CTAs mean fewer rows per
+    // CTA and front (one CTA per group of 32 warps left half the SMs idle)
+    int grid = ceil_div(n, 32);
     if (grid > ws.peel_grid) grid = ws.peel_grid;
     if (grid < 1 || ws.peel_single_cta) grid = 1;
     const uint32_t* rows = ws.rows;
