@@ -15,8 +15,12 @@
 #include <cmath>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "internal.cuh"
 #include "dirtree.h"
+
+namespace cg = cooperative_groups;
 
 namespace moea {
 namespace {
@@ -127,22 +131,38 @@ int run_compaction(C cls, int n, int* counts, int N, int* out, int* sizes, cudaS
 // ideal point
 // ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(512)
+// Running minimum of each objective (ideal_point.cu:97-165): one 8-CTA
+// cluster per objective, each CTA over a contiguous eighth of the points;
+// CTA 0 combines the eight minima from the cluster's shared memory.
+constexpr int kIdealCtas = 8, kIdealThreads = 256;
+__global__ void __cluster_dims__(kIdealCtas, 1, 1) __launch_bounds__(kIdealThreads)
 ideal_kernel(const float* __restrict__ objs, int stride, int n, const float* prev, float* out)
 {
-    const int m = blockIdx.x;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int r = (int)cluster.block_rank();
+    const int m = blockIdx.x / kIdealCtas;
+    const int per = (n + kIdealCtas - 1) / kIdealCtas;
+    const int lo = r * per, hi = min(n, lo + per);
     float v = INFINITY;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) v = fminf(v, objs[(size_t)m * stride + i]);
-    __shared__ float sh[16];
+    for (int i = lo + threadIdx.x; i < hi; i += kIdealThreads) v = fminf(v, objs[(size_t)m * stride + i]);
+    __shared__ float sh[kIdealThreads / 32];
+    __shared__ float s_min;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_down_sync(0xFFFFFFFFu, v, o));
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
     __syncthreads();
     if (threadIdx.x == 0) {
-        float r = INFINITY;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fminf(r, sh[w]);
-        out[m] = prev ? fminf(prev[m], r) : r;
+        float b = INFINITY;
+        for (int w = 0; w < kIdealThreads / 32; ++w) b = fminf(b, sh[w]);
+        s_min = b;
     }
+    cluster.sync();  // every CTA's minimum is published
+    if (r == 0 && threadIdx.x == 0) {
+        float acc = s_min;
+        for (int c = 1; c < kIdealCtas; ++c) acc = fminf(acc, *cluster.map_shared_rank(&s_min, c));
+        out[m] = prev ? fminf(prev[m], acc) : acc;
+    }
+    cluster.sync();  // CTA 0 has read every CTA's minimum
 }
 
 // ---------------------------------------------------------------------------
@@ -963,7 +983,8 @@ fused_prep(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
         I.sizes[3] = ta + tb;
         s_tot = ta + tb;
     }
-    // ideal point: the reduction order of ideal_kernel (512 threads)
+    // ideal point: fminf orders -0 below +0, so any reduction order gives
+    // the single-instance kernel's result
     for (int m = 0; m < M; ++m) {
         float v = INFINITY;
         if (t < 512)
@@ -1201,7 +1222,7 @@ int run_extract(Workspace& ws, const int* fronts, int n, const int* d_max_front,
 int run_ideal(const float* objs, int stride, int M, int n, const float* prev, float* ideal_out,
               cudaStream_t stream)
 {
-    ideal_kernel<<<M, 512, 0, stream>>>(objs, stride, n, prev, ideal_out);
+    ideal_kernel<<<M * kIdealCtas, kIdealThreads, 0, stream>>>(objs, stride, n, prev, ideal_out);
     MOEA_CUDA_TRY(cudaGetLastError());
     return MOEA_OK;
 }
