@@ -521,8 +521,9 @@ __device__ bool grid_barrier(int* counters, unsigned nblocks, int epoch)
     }
     if (threadIdx.x == 0) {
         const int target = epoch * (int)nblocks;
-        __threadfence();
-        atomicAdd(counters + 4, 1);
+        // release at GPU scope: with the CTA barrier above it orders every
+        // thread's earlier writes before the arrival
+        asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(counters + 4) : "memory");
         int ok = 1;
         const unsigned long long t0 = global_ns();
         while (ld_acquire_gpu(counters + 4) < target) {
@@ -783,11 +784,19 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
         if (!grid_barrier(counters, (unsigned)nblocks, ++epoch)) return;
         // front k is complete: remove it from U and count it
         int c = 0;
-        for (int w = threadIdx.x; w < W; w += blockDim.x) {
-            const uint32_t g = __ldcg(G + w);
-            if (g) {
-                U[w] &= ~g;
-                c += __popc(g);
+        for (int w0 = threadIdx.x; w0 < W; w0 += 4 * blockDim.x) {
+            uint32_t g[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int w = w0 + i * blockDim.x;
+                g[i] = (w < W) ? __ldcg(G + w) : 0u;
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                if (g[i]) {
+                    U[w0 + i * blockDim.x] &= ~g[i];
+                    c += __popc(g[i]);
+                }
             }
         }
 #pragma unroll
