@@ -274,17 +274,25 @@ __device__ __forceinline__ void norm_solve(const float* __restrict__ nds, int nd
         sV[r][m] = (r == m) ? 1.0 : 0.0;
     }
     __syncthreads();
-    if (warp == 0) {
-        int bad = s_bad;
-        if (!bad) {
-            for (int sweep = 0; sweep < 60; ++sweep) {
-                // A rotation leaves its two columns with the eigenvalues of their
-                // 2x2 Gram matrix, so the smallest column norm never grows and the
-                // largest never shrinks: once the current norms fail the
-                // conditioning test below, the converged ones fail it too, and
-                // the fallback (which ignores the rotations) is the result.
-                // Degenerate extreme points (repeated rows) stop here instead of
-                // rotating rounding noise for all 60 sweeps.
+    // Sweeps in round-robin order (circle method over P = M rounded up to
+    // even columns, column P - 1 a bye when M is odd): in round r column
+    // P - 1 meets column r and, for k >= 1, (r + k) mod (P - 1) meets
+    // (r - k) mod (P - 1).  The pairs of a round share no column, so warp k
+    // rotates pair k; every pair comes once per sweep.
+    __shared__ int s_stop, s_rot;
+    constexpr int P = (M + 1) & ~1;
+    constexpr int kPairs = P / 2;
+    int bad = s_bad;
+    if (!bad) {
+        for (int sweep = 0; sweep < 60; ++sweep) {
+            // A rotation leaves its two columns with the eigenvalues of their
+            // 2x2 Gram matrix, so the smallest column norm never grows and the
+            // largest never shrinks: once the current norms fail the
+            // conditioning test below, the converged ones fail it too, and
+            // the fallback (which ignores the rotations) is the result.
+            // Degenerate extreme points (repeated rows) stop here instead of
+            // rotating rounding noise for all 60 sweeps.
+            if (warp == 0) {
                 double cmax = 0.0, cmin = INFINITY;
                 for (int i = 0; i < M; ++i) {
                     const double x = (lane < M) ? sA[lane][i] : 0.0;
@@ -292,36 +300,56 @@ __device__ __forceinline__ void norm_solve(const float* __restrict__ nds, int nd
                     cmax = fmax(cmax, sg);
                     cmin = fmin(cmin, sg);
                 }
-                if (cmin < 1e-10 || cmax / cmin > 1e6) {
-                    bad = 1;
-                    break;
+                if (lane == 0) {
+                    s_stop = (cmin < 1e-10 || cmax / cmin > 1e6) ? 1 : 0;
+                    s_rot = 0;
                 }
-                int rotated = 0;
-                for (int i = 0; i < M - 1; ++i) {
-                    for (int j = i + 1; j < M; ++j) {
+            }
+            __syncthreads();
+            if (s_stop) {  // uniform over the block
+                bad = 1;
+                break;
+            }
+            for (int r = 0; r < P - 1; ++r) {
+                if (warp < kPairs) {
+                    int i = (warp == 0) ? r : (r + warp) % (P - 1);
+                    int j = (warp == 0) ? P - 1 : (r - warp + (P - 1)) % (P - 1);
+                    if (i > j) {
+                        const int tmp = i;
+                        i = j;
+                        j = tmp;
+                    }
+                    if (j < M) {  // j == M is the bye
                         const double x = (lane < M) ? sA[lane][i] : 0.0;
                         const double y = (lane < M) ? sA[lane][j] : 0.0;
                         const double al = warp_sum_d(x * x);
                         const double be = warp_sum_d(y * y);
                         const double ga = warp_sum_d(x * y);
-                        if (ga == 0.0 || fabs(ga) <= 1e-15 * sqrt(al * be)) continue;
-                        rotated = 1;
-                        const double zeta = (be - al) / (2.0 * ga);
-                        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                        const double c = 1.0 / sqrt(1.0 + t * t);
-                        const double s = c * t;
-                        if (lane < M) {
-                            sA[lane][i] = c * x - s * y;
-                            sA[lane][j] = s * x + c * y;
-                            const double vx = sV[lane][i], vy = sV[lane][j];
-                            sV[lane][i] = c * vx - s * vy;
-                            sV[lane][j] = s * vx + c * vy;
+                        if (!(ga == 0.0 || fabs(ga) <= 1e-15 * sqrt(al * be))) {
+                            const double zeta = (be - al) / (2.0 * ga);
+                            const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                            const double c = 1.0 / sqrt(1.0 + t * t);
+                            const double s = c * t;
+                            if (lane < M) {
+                                sA[lane][i] = c * x - s * y;
+                                sA[lane][j] = s * x + c * y;
+                                const double vx = sV[lane][i], vy = sV[lane][j];
+                                sV[lane][i] = c * vx - s * vy;
+                                sV[lane][j] = s * vx + c * vy;
+                            }
+                            if (lane == 0) s_rot = 1;
                         }
-                        __syncwarp();
                     }
                 }
-                if (!rotated) break;
+                __syncthreads();
             }
+            const int rotated = s_rot;
+            __syncthreads();  // every thread read s_rot before warp 0 clears it
+            if (!rotated) break;
+        }
+    }
+    if (warp == 0) {
+        {
             double smax = 0.0, smin = INFINITY;
             for (int i = 0; i < M && !bad; ++i) {
                 const double x = (lane < M) ? sA[lane][i] : 0.0;

@@ -223,12 +223,22 @@ static int jacobi_svd(double* a, double* v, double* sigma, int n)
             cmin = fmin(cmin, sqrt(s));
         }
         if (cmin < 1e-10 || cmax / cmin > 1e6) return 1;
+        /* round-robin order (circle method over P = n rounded up to even
+         * columns, column P - 1 a bye when n is odd): in round r column
+         * P - 1 meets column r and, for k >= 1, (r + k) mod (P - 1) meets
+         * (r - k) mod (P - 1); the pairs of a round share no column, so the
+         * GPU rotates them at once and the order inside a round is free */
         int rotated = 0;
-        for (int i = 0; i < n - 1; ++i) {
-            for (int j = i + 1; j < n; ++j) {
+        const int P = (n + 1) & ~1;
+        for (int r = 0; r < P - 1; ++r) {
+            for (int k = 0; k < P / 2; ++k) {
+                int i = (k == 0) ? r : (r + k) % (P - 1);
+                int j = (k == 0) ? P - 1 : (r - k + (P - 1)) % (P - 1);
+                if (i > j) { const int tmp = i; i = j; j = tmp; }
+                if (j >= n) continue;  /* the bye */
                 double al = 0.0, be = 0.0, ga = 0.0;
-                for (int k = 0; k < n; ++k) {
-                    const double x = a[k * n + i], y = a[k * n + j];
+                for (int q = 0; q < n; ++q) {
+                    const double x = a[q * n + i], y = a[q * n + j];
                     al += x * x; be += y * y; ga += x * y;
                 }
                 if (ga == 0.0 || fabs(ga) <= 1e-15 * sqrt(al * be)) continue;
@@ -237,13 +247,13 @@ static int jacobi_svd(double* a, double* v, double* sigma, int n)
                 const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
                 const double c = 1.0 / sqrt(1.0 + t * t);
                 const double s = c * t;
-                for (int k = 0; k < n; ++k) {
-                    const double x = a[k * n + i], y = a[k * n + j];
-                    a[k * n + i] = c * x - s * y;
-                    a[k * n + j] = s * x + c * y;
-                    const double vx = v[k * n + i], vy = v[k * n + j];
-                    v[k * n + i] = c * vx - s * vy;
-                    v[k * n + j] = s * vx + c * vy;
+                for (int q = 0; q < n; ++q) {
+                    const double x = a[q * n + i], y = a[q * n + j];
+                    a[q * n + i] = c * x - s * y;
+                    a[q * n + j] = s * x + c * y;
+                    const double vx = v[q * n + i], vy = v[q * n + j];
+                    v[q * n + i] = c * vx - s * vy;
+                    v[q * n + j] = s * vx + c * vy;
                 }
             }
         }
