@@ -192,12 +192,29 @@ def batch_specs(count: int, seed: int = 0):
     return out
 
 
-def batched_measure(args, torch, cm):
+def shard_instances(specs, world: int, rank: int):
+    """Indices of the instances `rank` runs: largest first, each to the rank
+    with the least work so far, work = pair tests (2N)^2.  Every instance is
+    on exactly one rank; with one rank, all of them in order."""
+    loads = [0] * world
+    own = []
+    for i in sorted(range(len(specs)), key=lambda i: (-(2 * specs[i][2]) ** 2, i)):
+        r = min(range(world), key=lambda j: (loads[j], j))
+        loads[r] += (2 * specs[i][2]) ** 2
+        if r == rank:
+            own.append(i)
+    return sorted(own)
+
+
+def batched_measure(args, torch, cm, world: int = 1, rank: int = 0):
     """Instance-generations/s of the batch (one graph launch per generation)
     against the same instances looped one after another through the plain
     path on one stream; both advance the same generations, after which every
-    instance's front indices and objectives are compared."""
-    specs = batch_specs(args.batch_instances)
+    instance's front indices and objectives are compared.  With several
+    ranks the instances are sharded (shard_instances) and the job's rate is
+    all instances over the slowest rank's time."""
+    all_specs = batch_specs(args.batch_instances)
+    specs = [all_specs[i] for i in shard_instances(all_specs, world, rank)]
     T = 200
 
     def make(spec):
@@ -239,14 +256,18 @@ def batched_measure(args, torch, cm):
         r_b, r_p = batch.result(i), a.result()
         identical &= bool(torch.equal(r_b.auxiliary_indices, r_p.auxiliary_indices))
         identical &= bool(torch.equal(r_b.objectives, r_p.objectives))
-    n = len(specs)
+    batch_ms = over_ranks(batch_ms, "max", world, "cuda")
+    plain_ms = over_ranks(plain_ms, "max", world, "cuda")
+    identical = over_ranks(0.0 if identical else 1.0, "max", world, "cuda") == 0.0
+    n = len(all_specs)
     out = {"workload": BATCH_WORKLOAD, "instances": n, "generations_timed": K,
            "instance_gen_per_s": n * K / (batch_ms / 1e3),
            "plain_loop_instance_gen_per_s": n * K / (plain_ms / 1e3),
            "speedup_vs_plain_loop": plain_ms / batch_ms,
            "identical_ranks": identical, "fused": batch.fused,
            "graph_kernels_per_generation": batch.graph_kernels,
-           "pair_tests_per_generation": sum((2 * s[2]) ** 2 for s in specs)}
+           "pair_tests_per_generation": sum((2 * s[2]) ** 2 for s in all_specs),
+           "sharding": f"{world} rank(s), instances balanced by pair tests"}
     batch.close()
     del plain
     return out
@@ -569,8 +590,7 @@ def main() -> None:
     if not args.no_batch:
         del algo
         torch.cuda.empty_cache()
-        batched = batched_measure(args, torch, cm)
-        batched["instance_gen_per_s"] = over_ranks(batched["instance_gen_per_s"], "sum", world, "cuda")
+        batched = batched_measure(args, torch, cm, world, rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

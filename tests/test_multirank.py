@@ -41,3 +41,15 @@ def test_two_rank_reductions_and_seeds():
 def test_single_process_passthrough():
     import bench
     assert bench.over_ranks(3.5, "max", 1, "cpu") == 3.5
+
+
+def test_batch_shards_cover_every_instance_once_and_balance():
+    import bench
+    specs = bench.batch_specs(256)
+    for world in (1, 2, 3, 8):
+        shards = [bench.shard_instances(specs, world, r) for r in range(world)]
+        flat = sorted(i for sh in shards for i in sh)
+        assert flat == list(range(len(specs)))
+        loads = [sum((2 * specs[i][2]) ** 2 for i in sh) for sh in shards]
+        assert max(loads) <= min(loads) + max((2 * s[2]) ** 2 for s in specs)
+    assert bench.shard_instances(specs, 1, 0) == list(range(len(specs)))
