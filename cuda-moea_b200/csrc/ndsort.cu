@@ -458,15 +458,23 @@ __device__ __forceinline__ void tile_block(int bx, int by, const float* __restri
         }
         return cmp | infm;
     };
-    int wl = wb;
-    for (; wl < wfull; ++wl) so_row[wl] = word_bits();   // all positions below dup[q]
-    for (; wl < wend; ++wl) {
-        // positions p < dup[q] of this word
-        const int rem = dup - (w0 + wl) * 32;
-        const uint32_t mask = rem >= 32 ? 0xFFFFFFFFu : (rem <= 0 ? 0u : ((1u << rem) - 1u));
-        so_row[wl] = mask & word_bits();
+    // The peel never reaches an infeasible point (each is dominated by every
+    // feasible one, and the peel ends with the feasible fronts), so its row is
+    // never read: a warp of infeasible q (they sort last, so whole warps are)
+    // computes nothing, and a CTA of them stores nothing.  Rows of infeasible
+    // q in a mixed CTA hold unspecified words.
+    const bool all_inf = __all_sync(0xFFFFFFFFu, inf || q >= n);
+    if (!all_inf) {
+        int wl = wb;
+        for (; wl < wfull; ++wl) so_row[wl] = word_bits();   // all positions below dup[q]
+        for (; wl < wend; ++wl) {
+            // positions p < dup[q] of this word
+            const int rem = dup - (w0 + wl) * 32;
+            const uint32_t mask = rem >= 32 ? 0xFFFFFFFFu : (rem <= 0 ? 0u : ((1u << rem) - 1u));
+            so_row[wl] = mask & word_bits();
+        }
     }
-    __syncthreads();
+    if (__syncthreads_and(all_inf)) return;
     for (int r = warp; r < kQB; r += kTileThreads / 32) {
         const int pos = q0 + r;
         if (pos >= n) break;
@@ -575,9 +583,14 @@ __device__ __forceinline__ void peel_body(int block, int nblocks, uint32_t* U,
     __shared__ int s_sq[kScanQueue], s_sw[kScanQueue], s_found[kScanQueue];
     __shared__ int s_wsum[32];
     if (threadIdx.x == 0) s_nscan = 0;
+    // Feasible positions come first in the sorted order.  Infeasible ones are
+    // never assigned here (each is dominated by every feasible point, and the
+    // peel ends with the feasible fronts or the target), so they start out of
+    // the unassigned set: they are never examined and their rows never read.
+    const int nf = min(n, counters[0]);
     for (int w = threadIdx.x; w < W; w += blockDim.x) {
         const int lo = w * 32;
-        U[w] = (lo + 32 <= n) ? 0xFFFFFFFFu : (lo >= n ? 0u : ((1u << (n - lo)) - 1u));
+        U[w] = (lo + 32 <= nf) ? 0xFFFFFFFFu : (lo >= nf ? 0u : ((1u << (nf - lo)) - 1u));
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
