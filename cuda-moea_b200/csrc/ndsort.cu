@@ -972,6 +972,47 @@ fused_lexsort(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
     int vals[kFusedItems];
 #pragma unroll
     for (int j = 0; j < kFusedItems; ++j) vals[j] = t * kFusedItems + j;
+    if (n <= kFusedThreads) {
+        // Small instances: the stable passes below order by (class and f0,
+        // then f1 .. f_{M-1} for class 0, then the index); here each point
+        // counts the points before it under that order directly, instead of
+        // block sorts sized for kFusedMaxPoints.  Same permutation.
+        uint64_t* s_k0 = reinterpret_cast<uint64_t*>(fused_smem);
+        int* s_perm = reinterpret_cast<int*>(s_k0 + kFusedThreads);
+        if (t < n) s_k0[t] = I.key0[t];
+        __syncthreads();
+        if (t < n) {
+            const uint64_t ki = s_k0[t];
+            const bool cls0 = (ki >> 32) == 0;
+            int r = 0;
+            for (int u = 0; u < n; ++u) {
+                const uint64_t ku = s_k0[u];
+                bool less = ku < ki;
+                if (ku == ki) {
+                    less = u < t;
+                    if (cls0) {
+                        for (int m = 1; m < M; ++m) {
+                            const uint32_t a = float_order_key(pop.obj(m, u));
+                            const uint32_t b = float_order_key(pop.obj(m, t));
+                            if (a != b) {
+                                less = a < b;
+                                break;
+                            }
+                        }
+                    }
+                }
+                r += less ? 1 : 0;
+            }
+            s_perm[r] = t;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kFusedItems; ++j) {
+            const int pos = t * kFusedItems + j;
+            vals[j] = (pos < n) ? s_perm[pos] : pos;
+        }
+        __syncthreads();  // the shared storage is reused below
+    } else {
     for (int m = M - 1; m >= 1; --m) {
         uint32_t keys[kFusedItems];
 #pragma unroll
@@ -989,6 +1030,7 @@ fused_lexsort(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
         for (int j = 0; j < kFusedItems; ++j) keys[j] = (vals[j] < n) ? I.key0[vals[j]] : 0x3FFFFFFFFull;
         FusedSort64(tmp.s64).Sort(keys, vals, 0, 34);
         __syncthreads();
+    }
     }
 #pragma unroll
     for (int j = 0; j < kFusedItems; ++j) {

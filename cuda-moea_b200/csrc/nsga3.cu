@@ -1142,6 +1142,69 @@ fused_niching(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
         const int r = I.assoc_idx[i];
         if (r >= 0 && r < H) atomicAdd(I.rho + r, 1);
     }
+    if (nl <= kFusedThreads) {
+        // Small fronts: each stage is a stable sort by (key, position), done by
+        // counting for every member the members before it, instead of block
+        // sorts sized for kFusedMaxPoints.  Same orders, same random words.
+        uint64_t* s_key = reinterpret_cast<uint64_t*>(fused_smem);   // [2][kFusedThreads]
+        int* s_val = reinterpret_cast<int*>(s_key + 2 * kFusedThreads);  // [2][kFusedThreads]
+        int* s_wmax = s_val + 2 * kFusedThreads;                        // [kFusedThreads / 32]
+        int cur = 0;
+        if (t < nl) {
+            s_key[t] = ((uint64_t)(uint32_t)I.assoc_idx[np + t] << 32) | __float_as_uint(I.assoc_dist[np + t]);
+            s_val[t] = t;
+        }
+        __syncthreads();  // rho complete, stage-1 keys in place
+        for (int stage = 1; stage <= 3; ++stage) {
+            const uint64_t* kc = s_key + cur * kFusedThreads;
+            if (t < nl) {
+                const uint64_t k = kc[t];
+                int r = 0;
+                for (int u = 0; u < nl; ++u) {
+                    const uint64_t ku = kc[u];
+                    r += (ku < k || (ku == k && u < t)) ? 1 : 0;
+                }
+                s_key[(cur ^ 1) * kFusedThreads + r] = k;
+                s_val[(cur ^ 1) * kFusedThreads + r] = s_val[cur * kFusedThreads + t];
+            }
+            __syncthreads();
+            cur ^= 1;
+            if (stage == 3) break;
+            // start of each direction's run: max-scan of the run heads
+            const uint64_t* kn = s_key + cur * kFusedThreads;
+            const int lane = t & 31, warp = t >> 5;
+            int head = -1;
+            if (t < nl && (t == 0 || (uint32_t)(kn[t] >> 32) != (uint32_t)(kn[t - 1] >> 32))) head = t;
+            int incl = head;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= o) incl = max(incl, y);
+            }
+            if (lane == 31) s_wmax[warp] = incl;
+            __syncthreads();
+            int rs = incl;
+            for (int w = 0; w < warp; ++w) rs = max(rs, s_wmax[w]);
+            if (t < nl) {
+                const uint32_t ref = (uint32_t)(kn[t] >> 32);
+                const int r_i = (int)ref;
+                const int rho_r = (r_i >= 0 && r_i < H) ? I.rho[r_i] : 0;
+                const int rank = t - rs;
+                uint64_t nk;
+                if (stage == 1) {
+                    const uint32_t rnd = splitmix_u32(off + (uint64_t)t, I.nich_seed);
+                    const uint32_t low = (rho_r == 0 && rank == 0) ? 0u : (rnd | 1u);
+                    nk = ((uint64_t)ref << 32) | low;
+                } else {
+                    const uint32_t rnd = splitmix_u32(off + (uint64_t)nl + (uint64_t)t, I.nich_seed);
+                    nk = ((uint64_t)(uint32_t)(rho_r + rank) << 32) | rnd;
+                }
+                s_key[cur * kFusedThreads + t] = nk;  // own slot only; heads were read above
+            }
+            __syncthreads();
+        }
+        if (t < nrem && t < nl) I.selected[np + t] = I.nds_gidx[np + s_val[cur * kFusedThreads + t]];
+    } else {
     uint64_t keys[kFusedItems];
     int vals[kFusedItems];
 #pragma unroll
@@ -1181,6 +1244,7 @@ fused_niching(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
     for (int j = 0; j < kFusedItems; ++j) {
         const int i = t * kFusedItems + j;
         if (i < nrem && i < nl) I.selected[np + i] = I.nds_gidx[np + vals[j]];
+    }
     }
     if (t == 0) *I.offset = off + 2ull * (unsigned long long)nl;
 }
