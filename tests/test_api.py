@@ -82,3 +82,23 @@ def test_invalid_algorithm_and_device():
         cm.Algorithm("MOEAD")
     with pytest.raises(ValueError):
         cm.NSGA3(device="cpu")
+
+
+def test_two_layer_directions():
+    """Explicit two-layer Das-Dennis sets for UserDefinedDirections: the
+    outer layer's compositions of h1, then the inner layer's compositions of
+    h2 moved halfway to the centroid; rows on the simplex."""
+    from math import comb
+
+    import cuda_moea as cm
+    d = cm.two_layer_directions(10, 3, 2)
+    assert tuple(d.shape) == (comb(12, 9) + comb(11, 9), 10) == (275, 10)
+    assert float((d.sum(1) - 1).abs().max()) < 1e-6
+    outer, inner = d[:220], d[220:]
+    assert float(((outer * 3) - (outer * 3).round()).abs().max()) < 1e-6  # multiples of 1/3
+    assert float(inner.min()) >= 0.5 / 10 - 1e-7                           # shifted off the boundary
+    assert len({tuple(r.tolist()) for r in d}) == 275                     # no repeated direction
+    d3 = cm.two_layer_directions(3, 2, 0)
+    assert tuple(d3.shape) == (6, 3)
+    with pytest.raises(ValueError):
+        cm.two_layer_directions(0, 3, 2)
