@@ -11,8 +11,13 @@ One step = one generation (mating, SBX+PM, DTLZ1 evaluation, environmental
 selection).  Every step is timed with CUDA events on the algorithm's stream;
 between timed steps the L2 cache is flushed by writing a 256 MiB buffer
 (outside the timed intervals).  Multi-GPU: one independent replica per GPU
-(the path does not shard), value = total generations/s,
-max-over-ranks time.
+(a single instance does not shard), value = total generations/s,
+max-over-ranks time; the batched record shards its instances over the ranks.
+
+Other workloads (--workload): dtlz2-small (N=92), rvea-large-d (D=131072),
+c1dtlz1-m10 and constrained-batch (ten objectives, 275 two-layer
+directions, 64 seeds per batched launch), dtlz2-m8 (tensor-core
+association).
 
 `--impl reference` times the CPU restatement of the reference path (oracle/)
 on the host cores, same metric and workload (the reference itself has no CPU
