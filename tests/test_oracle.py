@@ -125,6 +125,36 @@ def test_normalize_hyperplane_and_fallback(oracle):
     assert ill == 1 and list(rcp) == [1.0, 1.0, 1.0]
 
 
+@pytest.mark.parametrize("M", [5, 8, 10])
+def test_normalize_many_objectives(oracle, M):
+    """The Jacobi intercept solve at the many-objective sizes: a non-diagonal
+    extreme matrix gives the hyperplane through its columns (FP64 solve of
+    E^T a = 1), and a rank-deficient objective set takes the row-maximum
+    fallback (normalization.cu:1302-1394)."""
+    rng = np.random.default_rng(M)
+    b = (1.0 + rng.random(M)).astype(np.float32)
+    # extremes: b_j on axis j plus off-axis parts below 0.03, so their
+    # achievement scalarising value (<= 3e4 with the 1e6 weights) stays below
+    # every interior point's (components >= 0.05, value >= 5e4)
+    ext_pts = np.diag(b) + (rng.random((M, M)) * 0.03).astype(np.float32)
+    interior = (0.05 + rng.random((M, 300))).astype(np.float32)
+    pts = np.concatenate([interior[:, :100], ext_pts, interior[:, 100:]], axis=1)
+    ideal = np.zeros(M, np.float32)
+    f, rcp, ext, ill = oracle.normalize(pts, ideal)
+    assert ill == 0
+    assert list(ext) == list(range(100, 100 + M))
+    E = pts[:, ext].astype(np.float64)
+    want = np.linalg.solve(E.T, np.ones(M))
+    np.testing.assert_allclose(rcp, want, rtol=1e-5)
+    np.testing.assert_allclose(f, pts * rcp[:, None], rtol=1e-5)
+    # two equal objectives make every extreme matrix singular
+    dup = interior.copy()
+    dup[M - 1] = dup[M - 2]
+    f, rcp, ext, ill = oracle.normalize(dup, ideal)
+    assert ill == 1
+    np.testing.assert_allclose(rcp, 1.0 / dup.max(axis=1), rtol=1e-6)
+
+
 def test_reference_direction_counts(oracle):
     assert oracle.reference_directions(0, 92, 3).shape == (3, 91)
     assert oracle.reference_directions(0, 32768, 3).shape == (3, 32640)
