@@ -15,7 +15,7 @@
  *     library calls exit() (the reference's CUDA_CHECK does,
  *     nat/include/cuda_moea/core/cuda/cuda_utils.cuh:16-22).
  *
- * Reference paths below are relative to python/csrc/native/ of CUDA-MOEA.
+ * Reference paths below are inside CUDA-MOEA; nat/ stands for python/csrc/native/.
  */
 #ifndef MOEA_B200_H
 #define MOEA_B200_H
@@ -42,7 +42,8 @@ enum {
     MOEA_ERR_LOAD = 8              /* a plugin library did not load (reference: std::runtime_error) */
 };
 
-/* Version of this ABI (MOEA_ABI_VERSION). */
+/* Version of this ABI (MOEA_ABI_VERSION). No reference counterpart: a binding
+ * checks it once before its first call. */
 int moea_abi_version(void);
 /* Message of the last failure on the calling thread ("" if none). */
 const char* moea_last_error(void);
@@ -60,7 +61,8 @@ typedef struct moea_workspace moea_workspace;
 moea_status moea_workspace_create(int device, int max_points, int max_objectives,
                                   int max_directions, moea_workspace** out);
 void moea_workspace_destroy(moea_workspace* ws);
-/* Bytes of device memory held by the workspace. */
+/* Bytes of device memory held by the workspace (the reference's selector scratch
+ * pool, nat/src/selection/nsga3/kernels/dynamic_workspace.cu, reports none). */
 size_t moea_workspace_bytes(const moea_workspace* ws);
 
 /* ========================================================================
@@ -381,18 +383,24 @@ typedef struct moea_population_view {
 } moea_population_view;
 
 /* NSGA-III: index of the last front and {N_prior, N_last, N_rem, N_nds} of the
- * latest selection (synchronises the algorithm's stream). */
+ * latest selection (synchronises the algorithm's stream).  Replaces run_ndsort's
+ * max_front and NumNDSData (nat/src/selection/nsga3/kernels/non_dominated_sort.cu:1407,
+ * :1636). */
 moea_status moea_algorithm_selection_stats(moea_algorithm* alg, int* h_max_front, int* h_sizes);
 
 moea_status moea_algorithm_view(moea_algorithm* alg, moea_population_view* out);
-/* Reference directions in use: d_values (M,count). */
+/* Reference directions in use: d_values (M,count).  Replaces
+ * IReferenceDirectionProvider::view()
+ * (nat/include/cuda_moea/reference/reference_direction_provider.cuh:18). */
 moea_status moea_algorithm_directions(moea_algorithm* alg, const float** d_values, int* count);
 /* Runs one generation with direct launches and CUDA events between its
  * stages: h_ms[i] is the device time of stage i, h_names the '\n'-separated
  * stage names (both up to cap / names_cap). */
 moea_status moea_algorithm_profile_step(moea_algorithm* alg, char* h_names, size_t names_cap,
                                         float* h_ms, int cap, int* h_count);
-/* Device status of the last generation (0 ok); also returned as a status by step. */
+/* Device status of the last generation (0 ok); also returned as a status by step.
+ * Replaces the reference's CUDA error path, which exits the process
+ * (nat/include/cuda_moea/core/cuda/cuda_utils.cuh:16-22). */
 moea_status moea_algorithm_device_status(moea_algorithm* alg, int* h_status);
 
 /* ========================================================================
