@@ -30,6 +30,20 @@ def test_library_exports_every_declared_symbol():
     assert L.moea_abi_version() == 1
 
 
+def test_ctypes_signatures_match_header_arity():
+    """Every declaration's parameter count is the one its ctypes binding passes."""
+    from cuda_moea import _lib
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    arity = {}
+    for name, args in re.findall(r"\b(moea_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        if name.endswith("_fn"):
+            continue
+        args = args.strip()
+        arity[name] = 0 if args in ("", "void") else args.count(",") + 1
+    bound = {name: len(argtypes) for name, _, argtypes in _lib._SIGNATURES}
+    assert arity == bound
+
+
 def test_errors_are_status_codes_not_exits():
     from cuda_moea import _lib
     L = _lib.lib()
