@@ -231,3 +231,36 @@ def test_problem_fp32_against_fp64(oracle):
     x[:, :2] = rng.random((4, 2))
     f, _ = oracle.evaluate("DTLZ2", x, 3, 1)
     np.testing.assert_allclose((f ** 2).sum(0), 1.0, rtol=1e-6)
+
+
+def test_rvea_semantics(oracle):
+    """Hand cases for the RVEA stages: translation floor, partition tie and
+    dead slots, gamma of orthogonal directions, APD edge values, and elitism
+    (objective_translation.cu:125, reference_partition.cu:407,
+    angle_penalized_distance.cu:159,387, elitism_selection.cu:194)."""
+    out, z = oracle.rvea_translate(np.array([[1, 2, 3], [5, 4, 6]], np.float32))
+    np.testing.assert_array_equal(z, [1, 4])
+    np.testing.assert_array_equal(out, np.array([[1e-32, 1, 2], [1, 1e-32, 2]], np.float32))
+
+    refs = np.eye(2, dtype=np.float32)  # directions e0, e1 as columns
+    t = np.array([[2, 1, 1], [1, 1, 3]], np.float32)
+    th, idx = oracle.rvea_partition(t, refs, 2, 3)
+    assert list(idx) == [0, 0, 2]  # (1,1) ties -> smaller direction; slot 2 is dead -> K
+    np.testing.assert_allclose(th[:2], [np.arccos(2 / np.sqrt(5)), np.pi / 4], rtol=1e-6)
+
+    g = oracle.rvea_gamma(refs)
+    np.testing.assert_allclose(g, [np.pi / 2] * 2, rtol=1e-6)
+    assert oracle.rvea_gamma(np.ones((2, 1), np.float32))[0] == np.float32(np.pi)
+
+    t = np.array([[3, 0, 1], [4, 0, 1]], np.float32)
+    apd = oracle.rvea_apd(t, np.zeros(3, np.float32), g, np.array([0, 0, 5], np.int32), 0, 10, 2.0)
+    # generation 0: no angle penalty, APD = |f'|; a zero vector -> 0; a dead direction -> 1e30
+    np.testing.assert_allclose(apd, [5, 0, 1e30], rtol=1e-6)
+
+    idx = np.array([0, 0, 1, 1], np.int32)
+    cv = np.array([0, 0, 0, 0.5], np.float32)
+    apd = np.array([2, 1, 3, 9], np.float32)
+    sel, act = oracle.rvea_elitism(idx, cv, apd, 4, 2)
+    assert act == 2 and sorted(sel) == [1, 2]  # one winner per direction, feasible first
+    sel, act = oracle.rvea_elitism(idx, cv, apd, 1, 2)
+    assert act == 1 and list(sel) == [1]  # more winners than N: the smallest metric
