@@ -264,3 +264,17 @@ def test_rvea_semantics(oracle):
     assert act == 2 and sorted(sel) == [1, 2]  # one winner per direction, feasible first
     sel, act = oracle.rvea_elitism(idx, cv, apd, 1, 2)
     assert act == 1 and list(sel) == [1]  # more winners than N: the smallest metric
+
+
+def test_rvea_adaptation(oracle):
+    """Directions scaled by the objective ranges of the active members only,
+    renormalised; a zero range falls back to the unscaled direction
+    (rvea_reference_adaptation.cu:279)."""
+    s = np.float32(np.sqrt(0.5))
+    v0 = np.array([[1, 0, s], [0, 1, s]], np.float32)
+    objs = np.array([[0, 2, 1, 100], [3, 4, 3.5, -50]], np.float32)  # the last slot is dead
+    v = oracle.rvea_adapt(v0, objs, 3)
+    want = np.array([[1, 0, 2 / np.sqrt(5)], [0, 1, 1 / np.sqrt(5)]])
+    np.testing.assert_allclose(v, want, rtol=1e-6, atol=1e-7)
+    flat = np.ones((2, 4), np.float32)
+    np.testing.assert_allclose(oracle.rvea_adapt(v0, flat, 4), v0, rtol=1e-6)
