@@ -42,6 +42,13 @@ METRIC = "NSGA-III gen/s @N=32768,M=3; batched instance-gen/s vs plain, identica
 WORKLOAD = "NSGA-III DTLZ1 M=3 D=7 N=32768, Das-Dennis H=254 (32640 directions), 1 generation per step"
 N_POP, D_VAR, M_OBJ, PARTITIONS = 32768, 7, 3, 254
 TILES_DRAM_BYTES = 3.00e6 + 210.55e6
+# dram__bytes_read.sum + dram__bytes_write.sum of one nds_peel launch at this
+# workload (ncu --set full, profiles/nds_peel_dtlz1_n65536.md)
+PEEL_DRAM_BYTES = 124.3e6 + 3.7e6
+# warp instructions nds_tiles issues per (warp, 32-position word) step: one
+# step tests 32 x 32 ordered pairs (ncu instruction count,
+# profiles/nds_tiles_dtlz1_n65536.md)
+TILES_WARP_INSTR_PER_STEP = 97
 
 
 def _peaks():
@@ -105,6 +112,41 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def kernel_rooflines(stage_ms: dict, n_mix: int, headline: bool):
+    """Roofline entries of the heavy kernels of one headline generation, the
+    largest stage time first.
+
+    - nds_peel (ndsort.peel): against the measured HBM copy bandwidth; its
+      algorithmic bytes are the lower-triangle relation rows, each read at
+      most once: n(n-1)/2 bits.
+    - nds_tiles (ndsort.dominance_tiles): integer compare work, so against the
+      issue-rate peak of the kernel as written: 148 SMs x 4 schedulers x
+      max SM clock warp instructions/s, TILES_WARP_INSTR_PER_STEP warp
+      instructions per 1024 pair tests; the unit is lower-triangle pair tests/s.
+    """
+    hbm, peak_kind = _peaks()
+    tri_pairs = n_mix * (n_mix - 1) / 2
+    rel_bytes = tri_pairs / 8
+    out = []
+    peel = stage_ms.get("ndsort.peel")
+    if peel:
+        a = rel_bytes / (peel / 1e3) / 1e9
+        out.append({"kernel": "nds_peel (front peeling)", "bound": "hbm", "achieved": a, "peak": hbm,
+                    "unit": "GB/s", "frac": a / hbm, "peak_source": peak_kind, "algorithmic_bytes": rel_bytes,
+                    "traffic": PEEL_DRAM_BYTES if headline else None, "ms": peel})
+    tiles = stage_ms.get("ndsort.dominance_tiles")
+    if tiles:
+        issue_peak = 148 * 4 * 1.965e9 * 1024 / TILES_WARP_INSTR_PER_STEP
+        a = tri_pairs / (tiles / 1e3)
+        out.append({"kernel": "nds_tiles (dominance rows)", "bound": "issue", "achieved": a, "peak": issue_peak,
+                    "unit": "pair tests/s", "frac": a / issue_peak,
+                    "peak_source": "148 SMs x 4 warp instr/clk x 1965 MHz, 97 warp instr per 1024 pairs",
+                    "algorithmic_bytes": rel_bytes, "hbm_frac": rel_bytes / (tiles / 1e3) / 1e9 / hbm,
+                    "traffic": TILES_DRAM_BYTES if headline else None, "ms": tiles})
+    out.sort(key=lambda r: -r["ms"])
+    return out
+
+
 def cpu_generation_time(n: int, threads: int, seed: int = 1):
     """One CPU generation of the restated reference path (oracle, OpenMP)."""
     import numpy as np
@@ -123,16 +165,119 @@ def cpu_generation_time(n: int, threads: int, seed: int = 1):
     mate = O.philox_stream(seed64, 0, 2, n)
     cand = np.stack([mate[:, 0] % n, mate[:, 1] % n], 1).astype(np.int32)
     pidx = O.tournament(cand, fronts, cv)
+    # the product's draw layout: one crossover block per pair element (SBX
+    # draws and both children's mutation tests), a mutation block for the
+    # amplitudes
     cx = O.philox_stream(seed64, 0, 3, (n // 2) * D_VAR)
+    mu = O.philox_stream(seed64, 0, 4, (n // 2) * D_VAR)
     unit = lambda u: (u >> 8).astype(np.float32) * np.float32(1.0 / 16777216.0)
     off = O.sbx(x, pidx, bounds, np.stack([unit(cx[:, 0]), unit(cx[:, 1])], 1),
-                (cx[:, 2] & 1).astype(np.int32), unit(cx[:, 3]), 30.0, 1.0, 0.0, n)
-    mu = O.philox_stream(seed64, 0, 4, n * D_VAR // 2)
-    um = np.stack([unit(mu[:, 0]), unit(mu[:, 1]), unit(mu[:, 2]), unit(mu[:, 3])], 1).reshape(-1, 2)
-    off = O.pm(off, bounds, um[: n * D_VAR], 20.0, 1.0)
+                (cx[:, 0] & 1).astype(np.int32), unit(cx[:, 2]), 30.0, 1.0, 0.0, n)
+    low = ((cx[:, 1] & 0xFF) << 24) | ((cx[:, 2] & 0xFF) << 16) | ((cx[:, 3] & 0xFF) << 8)
+    um = np.stack([unit(cx[:, 3]), unit(mu[:, 0]), unit(low), unit(mu[:, 1])], 1).reshape(n // 2, D_VAR, 2, 2)
+    um = um.transpose(0, 2, 1, 3).reshape(n * D_VAR, 2)
+    off = O.pm(off, bounds, um, 20.0, 1.0)
     of, ocv = O.evaluate("DTLZ1", off, M_OBJ)
     O.nsga3_select(np.concatenate([cv, ocv]), np.concatenate([f, of], 1), refs, seed64, 0, ideal)
     return time.perf_counter() - t0
+
+
+STAGE_SEED = 12345  # the fixed generation-0 population both arms time stages on
+
+
+def stage_population(n: int):
+    """The fixed merged population of the per-stage comparison: 2n points
+    uniform in [0,1]^D_VAR from STAGE_SEED (parents first, then offspring)."""
+    import numpy as np
+    rng = np.random.default_rng(STAGE_SEED)
+    return rng.random((2 * n, D_VAR)).astype(np.float32)
+
+
+class _QuietStdout:
+    """Sends file descriptor 1 to /dev/null for the duration (the reference's
+    library prints progress lines on stdout; the bench prints one JSON line)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(null, 1)
+        os.close(null)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
+def reference_gpu_record(steps: int):
+    with _QuietStdout():
+        return _reference_gpu_record(steps)
+
+
+def _reference_gpu_record(steps: int):
+    """The reference's own GPU path on this GPU, as a second baseline: its
+    complete NSGA-III generation (all of its native sources compiled in place
+    into oracle/_ref/libmoea_ref_algo.so, built through its C++ builder, each
+    step bracketed by device synchronises) on the headline and the small
+    workload, and its stage functions (oracle/_ref/libmoea_ref.so) timed with
+    CUDA events on the fixed generation-0 merged population of
+    stage_population."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device visible to the reference arm"}
+        from oracle.ref import ref as R
+        if not (R.algo_available() and R.available()):
+            return {"unavailable": "oracle/_ref not built (needs the reference sources at build time)"}
+        import numpy as np
+        rec = {"source": "CUDA-MOEA's own kernels and algorithm, compiled for sm_100a from its sources",
+               "timing": "host clock around each device-synchronised step (the reference's step waits on "
+                         "the host for its front sizes); stages: CUDA events over repeated calls",
+               "sparse_ratio": 1.0, "algorithm": []}
+        for desc, kind, D, M, N, parts, gens, warm, k in [
+                (WORKLOAD, 1, D_VAR, M_OBJ, N_POP, PARTITIONS, 50, 5, steps),
+                ("NSGA-III DTLZ2 M=3 D=12 N=92, 91 directions", 2, 12, 3, 92, 0, 100, 5, 50)]:
+            ms = R.algo_time(0, kind, D, M, N, parts, gens, 1.0, 2887, warm, k)
+            rec["algorithm"].append({"workload": desc, "steps": k, "warmup": warm,
+                                     "gen_per_s": k / (sum(ms) / 1e3),
+                                     "ms_per_gen_median": statistics.median(ms)})
+        # stages on the fixed population
+        from oracle import oracle as O
+        x = stage_population(N_POP)
+        rep = 5
+        stages = {}
+        R.set_repeat(rep)
+        objs, _ = R.problem(1, x[N_POP:], M_OBJ)
+        stages["evaluate (DTLZ1, N offspring)"] = R.last_ms()
+        R.set_repeat(0)
+        objs, _ = R.problem(1, x, M_OBJ)
+        cv = np.zeros(2 * N_POP, np.float32)
+        R.set_repeat(rep)
+        fronts, mf = R.ndsort(cv, objs, N_POP)
+        stages["ndsort"] = R.last_ms()
+        R.set_repeat(0)
+        gidx, sizes = O.nds_extract(fronts, mf, N_POP)
+        ideal = objs.min(1).astype(np.float32)
+        f_nds = objs[:, gidx]
+        fn, _ = R.normalize(f_nds, ideal)
+        R.set_repeat(rep)
+        R.normalize(f_nds, ideal)
+        stages["normalize"] = R.last_ms()
+        refs = O.reference_directions(1, PARTITIONS, M_OBJ)
+        idx, dist = R.associate(fn, refs)
+        stages["associate"] = R.last_ms()
+        R.niching(O.derive_seed(2887), 0, gidx, dist, idx, sizes, refs.shape[1], N_POP)
+        stages["niching"] = R.last_ms()
+        R.set_repeat(0)
+        rec["stages_ms_generation0"] = stages
+        rec["stage_population"] = (f"2x{N_POP} points uniform in [0,1]^{D_VAR} (numpy seed {STAGE_SEED}), "
+                                   f"DTLZ1 objectives; max_front {mf}, sizes {[int(v) for v in sizes]}")
+        return rec
+    except Exception as exc:  # the baseline is reported, never fatal
+        return {"unavailable": f"{type(exc).__name__}: {exc}"}
 
 
 def run_reference(args) -> None:
@@ -158,6 +303,7 @@ def run_reference(args) -> None:
         "cpu_baseline": {"value": value, "unit": "gen/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "gen/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": reference_gpu_record(max(5, min(args.steps, 20))),
     }))
 
 
@@ -579,13 +725,21 @@ def main() -> None:
     for name, ms in stages:
         stage_ms[name] = stage_ms.get(name, 0.0) + ms
     n_mix = 2 * N
-    dom_ms = stage_ms.get("ndsort.dominance_tiles", float("nan"))
-    # algorithmic bytes of the dominance stage: the relation of the lower
-    # triangle, one bit per ordered pair (p before q), written once
-    dom_bytes = n_mix * (n_mix - 1) / 2 / 8
-    hbm, peak_kind = _peaks()
-    achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms == dom_ms else None
-    pair_rate = (n_mix * n_mix) / (dom_ms / 1e3) if dom_ms == dom_ms else None
+    rooflines = kernel_rooflines(stage_ms, n_mix, N == N_POP)
+
+    # the same stages at generation 0 from the fixed population that the
+    # reference arm times its own stages on (stage_population): same parents
+    stages0 = None
+    if N == N_POP:
+        del pop
+        algo0 = cm.NSGA3(population_size=N, max_generations=gens, problem=cm.DTLZ1(D_VAR, M_OBJ),
+                         reference_directions=cm.DasDennisDirections(PARTITIONS), seed=args.seed,
+                         initial_population=stage_population(N)[:N], print_progress=False, device=local)
+        algo0.initialize()
+        stages0 = {}
+        for name, ms in algo0.profile_step():
+            stages0[name] = stages0.get(name, 0.0) + ms
+        del algo0
 
     precision = None
     if not args.no_precision:
@@ -619,13 +773,10 @@ def main() -> None:
             # graph kernels of the K device-timed and the K end-to-end generations
             "gpu_launches": kernels * 2 * args.steps,
             "stages_ms": stage_ms,
-            "roofline": {"kernel": "nds_tiles (dominance rows)", "bound": "hbm",
-                         "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": (achieved / hbm) if achieved else None, "peak_source": peak_kind,
-                         # dram__bytes_read.sum + dram__bytes_write.sum of one nds_tiles launch
-                         # at this workload (ncu --set full, profiles/nds_tiles_dtlz1_n65536.md)
-                         "traffic": TILES_DRAM_BYTES if N == N_POP else None,
-                         "algorithmic_bytes": dom_bytes, "pair_tests_per_s": pair_rate},
+            # the dominant kernel of the generation, then every heavy kernel
+            "roofline": rooflines[0],
+            "roofline_kernels": rooflines,
+            "stages_ms_generation0": stages0,
             "cpu_baseline": cpu,
             "precision_form": precision,
             "batched": batched,

@@ -156,8 +156,19 @@ __global__ void mating_philox(const float* __restrict__ cv, const int* __restric
     mating_child(i, cv, rank, active, seed, gen, pidx);
 }
 
-// SBX + PM for pair element e = p*D + d: one Philox block drives the SBX
-// draws (u1, u2, sign, copy), a second one the mutation draws of both children.
+// 24-bit uniform from the low bytes of three draws (bits the SBX draws of
+// the same block leave unused).
+__device__ __forceinline__ float low_bytes_unit(uint32_t a, uint32_t b, uint32_t c)
+{
+    return (float)(((a & 0xFFu) << 16) | ((b & 0xFFu) << 8) | (c & 0xFFu)) * (1.0f / 16777216.0f);
+}
+
+// SBX + PM for pair element e = p*D + d.  One Philox block (tag crossover)
+// gives the SBX draws (u1 and the sign from word 0, u2 from word 1, the copy
+// draw from word 2) and both children's mutation test draws (word 3, and the
+// unused low bytes of words 1-3).  A second block (tag mutation) is computed
+// only where a child mutates, with probability pm_prob/D per child: at large
+// D almost every element costs one block instead of two.
 __device__ __forceinline__ void variation_element(long long e, int p, int d,
                                                   const float* __restrict__ parents,
                                                   const int* __restrict__ pidx,
@@ -169,23 +180,30 @@ __device__ __forceinline__ void variation_element(long long e, int p, int d,
 {
     const float lo = bounds[2 * d], hi = bounds[2 * d + 1];
     const int ca = 2 * p, cb = ca + 1;
+    uint32_t r[4];
+    rng_block(seed, (uint64_t)e, gen, kTagCrossover, r);
     float c1, c2;
     if (p < pairs) {
         const float x1 = parents[(size_t)pidx[ca] * D + d];
         const float x2 = parents[(size_t)pidx[cb] * D + d];
-        uint32_t r[4];
-        rng_block(seed, (uint64_t)e, gen, kTagCrossover, r);
-        sbx_pair(x1, x2, u32_to_unit(r[0]), u32_to_unit(r[1]), (int)(r[2] & 1u),
-                 u32_to_unit(r[3]), eta_c, sbx_prob, copy_prob, lo, hi, c1, c2);
+        sbx_pair(x1, x2, u32_to_unit(r[0]), u32_to_unit(r[1]), (int)(r[0] & 1u),
+                 u32_to_unit(r[2]), eta_c, sbx_prob, copy_prob, lo, hi, c1, c2);
     } else {
         c1 = parents[(size_t)pidx[ca] * D + d];  // odd population: last child copies its parent
         c2 = 0.0f;
     }
     if (mutate) {
-        uint32_t r[4];
-        rng_block(seed, (uint64_t)e, gen, kTagMutation, r);
-        c1 = pm_value(c1, u32_to_unit(r[0]), u32_to_unit(r[1]), eta_m, pm_prob, D, lo, hi);
-        c2 = pm_value(c2, u32_to_unit(r[2]), u32_to_unit(r[3]), eta_m, pm_prob, D, lo, hi);
+        // the reference's test, polynomial_mutation.cu:34
+        const float limit = pm_prob / static_cast<float>(D);
+        const float ta = u32_to_unit(r[3]);
+        const float tb = low_bytes_unit(r[1], r[2], r[3]);
+        const bool ma = ta < limit, mb = p < pairs && tb < limit;
+        if (ma || mb) {
+            uint32_t m[4];
+            rng_block(seed, (uint64_t)e, gen, kTagMutation, m);
+            if (ma) c1 = pm_value(c1, ta, u32_to_unit(m[0]), eta_m, pm_prob, D, lo, hi);
+            if (mb) c2 = pm_value(c2, tb, u32_to_unit(m[1]), eta_m, pm_prob, D, lo, hi);
+        }
     }
     off[(size_t)ca * D + d] = c1;
     if (p < pairs) off[(size_t)cb * D + d] = c2;

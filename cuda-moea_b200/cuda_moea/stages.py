@@ -93,7 +93,21 @@ ASSOC_SCAN = 1    # every direction visited
 ASSOC_TENSOR = 2  # dots on the tensor cores, exact FP32 re-score of the candidates
 
 
+def _check_association(x: torch.Tensor, refs: torch.Tensor) -> None:
+    """Points (M,n) and directions (M,H): both FP32 matrices with the same M
+    on the same device (the kernels read M rows of each)."""
+    if x.dtype != torch.float32 or refs.dtype != torch.float32:
+        raise ValueError("points and directions must be float32")
+    if x.dim() != 2 or refs.dim() != 2:
+        raise ValueError("points (M, n) and directions (M, H) must be matrices")
+    if refs.shape[0] != x.shape[0]:
+        raise ValueError(f"directions have {refs.shape[0]} rows for {x.shape[0]} objectives")
+    if x.device != refs.device:
+        raise ValueError("points and directions must be on the same device")
+
+
 def associate(ws: Workspace, x: torch.Tensor, refs: torch.Tensor, mode: int = ASSOC_TREE):
+    _check_association(x, refs)
     M, n = x.shape
     idx = torch.empty(n, dtype=torch.int32, device=x.device)
     dist = torch.empty(n, dtype=torch.float32, device=x.device)
@@ -104,6 +118,7 @@ def associate(ws: Workspace, x: torch.Tensor, refs: torch.Tensor, mode: int = AS
 
 def associate_static(x: torch.Tensor, refs: torch.Tensor):
     """Full-scan association through the allocation-free entry point."""
+    _check_association(x, refs)
     M, n = x.shape
     idx = torch.empty(n, dtype=torch.int32, device=x.device)
     dist = torch.empty(n, dtype=torch.float32, device=x.device)

@@ -130,8 +130,7 @@ moea_status moea_associate(moea_workspace* ws, const float* d_x, const float* d_
  * overlaps on the device share the scratch and race; the first call on a
  * device resolves the scratch addresses (not stream-ordered), so make it
  * before any stream capture that includes this function.  No counterpart in
- * the reference, whose association always draws scratch from its pool
- * (nat/src/selection/nsga3/kernels/association.cu:586). */
+ * the reference. */
 moea_status moea_associate_static(const float* d_x, const float* d_refs, int M, int n, int H,
                                   int* d_idx, float* d_dist, void* stream);
 

@@ -38,13 +38,55 @@ def lib():
             "ref_rvea_gamma": [vp, c_int, c_int, vp],
             "ref_rvea_apd": [vp, vp, vp, vp, c_int, c_int, c_int, c_int, c_int, c_float, vp],
             "ref_rvea_elitism": [vp, vp, vp, c_int, c_int, c_int, vp, ip],
+            "ref_quantize_cv": [vp, vp, c_int, c_float, c_float, c_float, c_int],
+            "ref_rvea_adapt": [vp, vp, c_int, c_int, c_int, c_int, vp],
+            "ref_sbx": [vp, vp, vp, vp, vp, vp, vp, c_float, c_float, c_float, c_int, c_int],
+            "ref_pm": [vp, vp, vp, c_float, c_float, c_int, c_int],
+            "ref_tournament": [vp, vp, vp, c_int, vp],
+            "ref_rvea_update": [vp, vp, vp, vp, vp, vp, vp, c_int, c_int, c_int, c_int, vp, vp, vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)
             f.restype = c_int
             f.argtypes = args
+        L.ref_set_repeat.restype = None
+        L.ref_set_repeat.argtypes = [c_int]
+        L.ref_last_ms.restype = c_float
+        L.ref_last_ms.argtypes = []
+        L.ref_annealed.restype = c_float
+        L.ref_annealed.argtypes = [c_float, c_float, c_int, c_int]
         _lib = L
     return _lib
+
+
+HOST_LIB_PATH = LIB_PATH.parent / "libmoea_ref_host.so"
+_host = None
+
+
+def host_available() -> bool:
+    return HOST_LIB_PATH.exists()
+
+
+def host_lib():
+    """The reference's host-side direction generators (no CUDA runtime needed)."""
+    global _host
+    if _host is None:
+        L = ctypes.CDLL(str(HOST_LIB_PATH))
+        L.ref_directions.restype = c_int
+        L.ref_directions.argtypes = [c_int, c_int, c_int, vp, ctypes.c_size_t]
+        _host = L
+    return _host
+
+
+def directions(mode, n, M):
+    """Normalised directions (M, count) from the reference's generators: mode 0
+    NSGA-III auto layers, 1 NSGA-III by partitions, 2 RVEA auto layers."""
+    count = host_lib().ref_directions(mode, n, M, None, 0)
+    if count < 0:
+        raise ValueError("reference generator rejected the request")
+    out = np.zeros((M, count), np.float32)
+    host_lib().ref_directions(mode, n, M, out.ctypes.data, out.size)
+    return out
 
 
 _LIVE: list = []
@@ -147,3 +189,113 @@ def rvea_elitism(idx, cv, apd, N, K):
     _chk(lib().ref_rvea_elitism(_d(idx).data_ptr(), _d(cv).data_ptr(), _d(apd).data_ptr(), N, len(idx), K,
                                 sel.data_ptr(), ctypes.byref(act)))
     return np.sort(sel.cpu().numpy()[: act.value]), act.value
+
+
+def quantize_cv(cv, eps, clip, log_alpha, bins):
+    out = torch.empty(len(cv), dtype=torch.float32, device="cuda")
+    _chk(lib().ref_quantize_cv(_d(cv).data_ptr(), out.data_ptr(), len(cv), eps, clip, log_alpha, bins))
+    return out.cpu().numpy()
+
+
+def rvea_adapt(v0, objs, n_active):
+    M, K = v0.shape
+    out = torch.empty((M, K), dtype=torch.float32, device="cuda")
+    _chk(lib().ref_rvea_adapt(_d(v0).data_ptr(), _d(objs).data_ptr(), M, K, n_active, objs.shape[1],
+                              out.data_ptr()))
+    return out.cpu().numpy()
+
+
+def annealed(begin, end, generation, total):
+    return lib().ref_annealed(begin, end, generation, total)
+
+
+def sbx_t(parents, pidx, bounds, u, sign, copy, eta, prob, copy_prob, n_off):
+    """SBX with device tensors in and out (large populations stay on the GPU)."""
+    D = parents.shape[1]
+    off = torch.empty((n_off, D), dtype=torch.float32, device=parents.device)
+    rc = lib().ref_sbx(parents.data_ptr(), pidx.data_ptr(), bounds.data_ptr(), u.data_ptr(), sign.data_ptr(),
+                       copy.data_ptr(), off.data_ptr(), eta, prob, copy_prob, n_off, D)
+    _chk(rc)
+    return off
+
+
+def pm_t(off, bounds, u, eta, prob):
+    """Polynomial mutation of a device tensor in place."""
+    n, D = off.shape
+    _chk(lib().ref_pm(off.data_ptr(), bounds.data_ptr(), u.data_ptr(), eta, prob, n, D))
+    return off
+
+
+def sbx(parents, pidx, bounds, u, sign, copy, eta, prob, copy_prob, n_off):
+    out = sbx_t(_d(parents), _d(pidx), _d(bounds), _d(u), _d(sign), _d(copy), eta, prob, copy_prob, n_off)
+    return out.cpu().numpy()
+
+
+def pm(off, bounds, u, eta, prob):
+    t = _d(off).clone()
+    return pm_t(t, _d(bounds), _d(u), eta, prob).cpu().numpy()
+
+
+def tournament(cand, rank, cv):
+    n = cand.shape[0]
+    w = torch.empty(n, dtype=torch.int32, device="cuda")
+    _chk(lib().ref_tournament(_d(cand).data_ptr(), _d(rank).data_ptr(), _d(cv).data_ptr(), n, w.data_ptr()))
+    return w.cpu().numpy()
+
+
+def problem_t(kind, x, M):
+    """Objectives (M,N) and violation (N) of device variables x (N,D)."""
+    N, D = x.shape
+    objs = torch.empty((M, N), dtype=torch.float32, device=x.device)
+    cv = torch.empty(N, dtype=torch.float32, device=x.device)
+    _chk(lib().ref_problem(kind, x.data_ptr(), N, D, M, objs.data_ptr(), cv.data_ptr()))
+    return objs, cv
+
+
+def rvea_update_t(par_x, off_x, par_f, off_f, par_cv, off_cv, sel, active):
+    """The reference's RVEA merge + survivor update on device tensors: the next
+    population's variables (N,D), objectives (M,N) and violations (N)."""
+    N, D = par_x.shape
+    M = par_f.shape[0]
+    nx = torch.empty_like(par_x)
+    nf = torch.empty_like(par_f)
+    nc = torch.empty_like(par_cv)
+    s = sel.clone()
+    _chk(lib().ref_rvea_update(par_x.data_ptr(), off_x.data_ptr(), par_f.data_ptr(), off_f.data_ptr(),
+                               par_cv.data_ptr(), off_cv.data_ptr(), s.data_ptr(), active, N, D, M,
+                               nx.data_ptr(), nf.data_ptr(), nc.data_ptr()))
+    return nx, nf, nc
+
+
+def set_repeat(repeat: int) -> None:
+    """Timing mode of the stage calls: after the call that produces the
+    outputs, `repeat` more calls between CUDA events (0 = off)."""
+    lib().ref_set_repeat(repeat)
+
+
+def last_ms() -> float:
+    """Mean device time of the repeats of the last stage call (timing mode)."""
+    return float(lib().ref_last_ms())
+
+
+ALGO_LIB_PATH = LIB_PATH.parent / "libmoea_ref_algo.so"
+
+
+def algo_available() -> bool:
+    return ALGO_LIB_PATH.exists()
+
+
+def algo_time(algorithm, problem_kind, D, M, N, partitions, max_gen, sparse_ratio, seed, warmup, steps):
+    """Per-step times (ms) of the reference's own algorithm on the GPU
+    (EvolutionaryAlgorithm::step, each step bracketed by device synchronises)."""
+    L = ctypes.CDLL(str(ALGO_LIB_PATH))
+    L.ref_algo_time.restype = c_int
+    L.ref_algo_time.argtypes = [c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_float, ctypes.c_ulonglong,
+                                c_int, c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_char_p, ctypes.c_size_t]
+    ms = (ctypes.c_double * max(1, steps))()
+    err = ctypes.create_string_buffer(512)
+    rc = L.ref_algo_time(algorithm, problem_kind, D, M, N, partitions, max_gen, sparse_ratio, seed, warmup, steps,
+                         ms, err, 512)
+    if rc != 0:
+        raise RuntimeError(f"reference algorithm failed ({rc}): {err.value.decode(errors='replace')}")
+    return [ms[i] for i in range(steps)]

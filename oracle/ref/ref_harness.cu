@@ -12,6 +12,9 @@
 //   execute_niching                selection/nsga3/kernels/niching.cu:250
 //   compute_fv / compute_cv        problem/dtlz/dtlz_kernels.cu:748, :1094
 //   rvea::translate_fv / execute_partition / compute_apd / compute_gamma / run_elitism_selection
+//   nsga3::quantize_cv             selection/nsga3/kernels/cv_quantization.cu:65-95
+//   rvea::adapt_refvecs            reference/rvea_reference_adaptation.cu:279-317
+//   rvea::merge_* / update_iter_vars selection/rvea/kernels/rvea_population_update.cu:209-300
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -20,6 +23,8 @@
 #include "cuda_moea/core/cuda/cuda_globals.cuh"
 #include "cuda_moea/core/cuda/cuda_manager.cuh"
 #include "cuda_moea/problem/dtlz/evaluation_workspace.cuh"
+#include "cuda_moea/reference/rvea_reference_adaptation.cuh"
+#include "cuda_moea/selection/nsga3/kernels/cv_quantization.cuh"
 #include "cuda_moea/selection/nsga3/kernels/association.cuh"
 #include "cuda_moea/selection/nsga3/kernels/niching.cuh"
 #include "cuda_moea/selection/nsga3/kernels/non_dominated_sort.cuh"
@@ -28,6 +33,8 @@
 #include "cuda_moea/selection/rvea/kernels/elitism_selection.cuh"
 #include "cuda_moea/selection/rvea/kernels/objective_translation.cuh"
 #include "cuda_moea/selection/rvea/kernels/reference_partition.cuh"
+#include "cuda_moea/selection/rvea/kernels/rvea_population_update.cuh"
+#include "cuda_moea/problem/dtlz/population_adapter.cuh"
 
 void compute_fv(float* d_pop, float* d_fit_trans, float* d_fit, int N, int D, int M,
                 cudaStream_t fit_stream, MOPType dtlz_type);
@@ -65,9 +72,40 @@ cudaMemPool_t default_pool()
 
 int status() { return cudaDeviceSynchronize() == cudaSuccess && cudaGetLastError() == cudaSuccess ? 0 : 1; }
 
+// Timing mode (bench.py's reference arm): with a positive repeat count, a
+// stage call is made once for its outputs and then `repeat` more times between
+// two events on the legacy stream, with its scratch already allocated; the
+// mean is kept for ref_last_ms().  Host waits inside the reference's stage
+// (its front loop reads sizes back) count, as they do in its generation.
+int g_repeat = 0;
+float g_ms = 0.0f;
+
+template <class F>
+void run_timed(F&& f)
+{
+    f();
+    g_ms = 0.0f;
+    if (g_repeat <= 0) return;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaDeviceSynchronize();
+    cudaEventRecord(a, nullptr);
+    for (int i = 0; i < g_repeat; ++i) f();
+    cudaEventRecord(b, nullptr);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&g_ms, a, b);
+    g_ms /= (float)g_repeat;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+}
+
 }  // namespace
 
 extern "C" {
+
+void ref_set_repeat(int repeat) { g_repeat = repeat; }
+float ref_last_ms(void) { return g_ms; }
 
 // Non-dominated sort of n_mix = 2N merged points (run_ndsort) or, when
 // n_mix == N, of a parent population (run_ndsort_init).  The pair buffer is
@@ -93,9 +131,11 @@ int ref_ndsort(const float* d_cv, const float* d_objs, int M, int n_mix, int N, 
         const int tiles = (n_mix + 31) / 32;
         uint32_t* mask = s.get<uint32_t>((size_t)n_mix * tiles);
         bool prop_free = false;
-        mf = run_ndsort(const_cast<float*>(d_cv), const_cast<float*>(d_objs), d_fronts, pairs, mask,
-                        dominatee, dom_cnt, asgn, new_front, cap, prop_free, 0, 100, M, N, stream,
-                        default_pool());
+        run_timed([&] {
+            mf = run_ndsort(const_cast<float*>(d_cv), const_cast<float*>(d_objs), d_fronts, pairs, mask,
+                            dominatee, dom_cnt, asgn, new_front, cap, prop_free, 0, 100, M, N, stream,
+                            default_pool());
+        });
     }
     *h_max_front = mf;
     return status();
@@ -109,10 +149,23 @@ int ref_normalize(float* d_f, const float* d_ideal, int M, int n, float* d_rcp)
     std::vector<float> ones(M, 1.0f);
     float* d_ones = s.get<float>(M);
     cudaMemcpy(d_ones, ones.data(), sizeof(float) * M, cudaMemcpyHostToDevice);
-    execute_normalization(d_f, d_ideal, s.get<float>((size_t)blocks * M), s.get<int>((size_t)blocks * M),
-                          s.get<int>(M), s.get<float>(M * M), d_rcp, s.get<int>(1), s.get<float>(M * M),
-                          s.get<float>(M), s.get<float>(M * M), s.get<int>(1), s.get<float>(M), d_ones,
-                          s.get<float>(M), s.get<float>(M), M, n, default_pool(), nullptr);
+    float* b0 = s.get<float>((size_t)blocks * M);
+    int* b1 = s.get<int>((size_t)blocks * M);
+    int* b2 = s.get<int>(M);
+    float* b3 = s.get<float>(M * M);
+    int* b4 = s.get<int>(1);
+    float* b5 = s.get<float>(M * M);
+    float* b6 = s.get<float>(M);
+    float* b7 = s.get<float>(M * M);
+    int* b8 = s.get<int>(1);
+    float* b9 = s.get<float>(M);
+    float* b10 = s.get<float>(M);
+    float* b11 = s.get<float>(M);
+    // in timing mode the repeats normalise the already normalised values again
+    run_timed([&] {
+        execute_normalization(d_f, d_ideal, b0, b1, b2, b3, d_rcp, b4, b5, b6, b7, b8, b9, d_ones, b10, b11, M,
+                              n, default_pool(), nullptr);
+    });
     return status();
 }
 
@@ -120,9 +173,12 @@ int ref_associate(const float* d_x, const float* d_refs, int M, int n, int H, in
 {
     Scratch s;
     const int nbr = (H + 255) / 256;
-    execute_association(const_cast<float*>(d_x), const_cast<float*>(d_refs),
-                        s.get<float>((size_t)nbr * n), s.get<int>((size_t)nbr * n), d_dist, d_idx, H, M,
-                        n, nullptr);
+    float* bmax = s.get<float>((size_t)nbr * n);
+    int* barg = s.get<int>((size_t)nbr * n);
+    run_timed([&] {
+        execute_association(const_cast<float*>(d_x), const_cast<float*>(d_refs), bmax, barg, d_dist, d_idx, H,
+                            M, n, nullptr);
+    });
     return status();
 }
 
@@ -137,10 +193,24 @@ int ref_niching(uint64_t seed, uint64_t* h_offset, const int* d_gidx, const floa
     sz.N_nds = h_sizes[3];
     const size_t nl = sz.N_last > 0 ? sz.N_last : 1;
     ull off = *h_offset;
-    execute_niching(seed, off, d_gidx, d_dist, d_idx, s.get<int>(H), s.get<ull>(nl), s.get<ull>(nl),
-                    s.get<int>(nl), s.get<int>(nl), s.get<int>(nl), s.get<int>(nl), s.get<int>(nl),
-                    s.get<uint>(nl), d_selected, sz, H, N, default_pool(), nullptr, false);
-    *h_offset = off;
+    int* c0 = s.get<int>(H);
+    ull* k0 = s.get<ull>(nl);
+    ull* k1 = s.get<ull>(nl);
+    int* i0 = s.get<int>(nl);
+    int* i1 = s.get<int>(nl);
+    int* i2 = s.get<int>(nl);
+    int* i3 = s.get<int>(nl);
+    int* i4 = s.get<int>(nl);
+    uint* u0 = s.get<uint>(nl);
+    ull first_off = 0;
+    bool first = true;
+    run_timed([&] {
+        execute_niching(seed, off, d_gidx, d_dist, d_idx, c0, k0, k1, i0, i1, i2, i3, i4, u0, d_selected, sz, H,
+                        N, default_pool(), nullptr, false);
+        if (first) first_off = off;
+        first = false;
+    });
+    *h_offset = first_off;
     return status();
 }
 
@@ -150,7 +220,7 @@ int ref_problem(int kind, const float* d_x, int N, int D, int M, float* d_objs, 
     Scratch s;
     float* trans = s.get<float>((size_t)N * M);
     static const int base[16] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 1, 3, 2, 8, 1, 4, 15};
-    compute_fv(const_cast<float*>(d_x), trans, d_objs, N, D, M, nullptr, (MOPType)base[kind]);
+    run_timed([&] { compute_fv(const_cast<float*>(d_x), trans, d_objs, N, D, M, nullptr, (MOPType)base[kind]); });
     cudaMemset(d_cv, 0, sizeof(float) * N);
     if (kind == 15) compute_csdp_cv(d_x, d_cv, N, nullptr);
     else if (kind >= 9) compute_cv(d_objs, d_cv, N, M, nullptr, (MOPType)kind);
@@ -202,6 +272,54 @@ int ref_rvea_elitism(const int* d_idx, const float* d_cv, const float* d_apd, in
                                 s.get<int>(n_mix), s.get<int>(n_mix), s.get<int>(1), d_selected, N, n_mix,
                                 K, active, pool, nullptr);
     *h_active = active;
+    return status();
+}
+
+// RVEA survivor update as RVEAEnvironmentSelector::select does it
+// (rvea_environment_selector.cu:187-290): merge parents and offspring, then
+// gather the `active` selected rows (d_sel, sorted in place) and write the
+// dead-slot sentinels into rows [active, N).
+int ref_rvea_update(const float* d_par_x, const float* d_off_x, const float* d_par_f, const float* d_off_f,
+                    const float* d_par_cv, const float* d_off_cv, int* d_sel, int active, int N, int D, int M,
+                    float* d_next_x, float* d_next_f, float* d_next_cv)
+{
+    Scratch s;
+    PopData par(N, D), off(N, D), mix(2 * N, D), next(N, D);
+    par.d_pop = const_cast<float*>(d_par_x);
+    off.d_pop = const_cast<float*>(d_off_x);
+    mix.d_pop = s.get<float>((size_t)2 * N * D);
+    next.d_pop = d_next_x;
+    float* mix_f = s.get<float>((size_t)2 * N * M);
+    float* mix_cv = s.get<float>((size_t)2 * N);
+    rvea::merge_pop(par, off, mix, D, N, nullptr);
+    rvea::merge_cv(d_par_cv, d_off_cv, mix_cv, N, nullptr);
+    rvea::merge_fv(d_par_f, d_off_f, mix_f, M, N, nullptr);
+    rvea::update_iter_vars(mix, mix_cv, mix_f, d_sel, next, d_next_cv, d_next_f, D, M, active, N, nullptr);
+    const int rc = status();
+    par.d_pop = off.d_pop = mix.d_pop = next.d_pop = nullptr;
+    return rc;
+}
+
+// Optional CV quantisation of n violations (validated parameters only).
+int ref_quantize_cv(const float* d_cv, float* d_out, int n, float eps_feas, float clip_upper,
+                    float log_alpha, int bins)
+{
+    if (!nsga3::validate_cv_quant_params(bins, clip_upper, log_alpha, eps_feas)) return 2;
+    nsga3::quantize_cv(d_cv, d_out, n, eps_feas, clip_upper, log_alpha, bins, nullptr);
+    return status();
+}
+
+// Direction adaptation V = normalise(V0 * (zmax - zmin)) over the first
+// n_active columns of d_objs (M, n_stride), called the way
+// AdaptiveRVEADirections::update calls it (reference_directions.cu:132-162:
+// fr = 1 and a zero trigger, so every call adapts).
+int ref_rvea_adapt(const float* d_v0, const float* d_objs, int M, int K, int n_active, int n_stride,
+                   float* d_v)
+{
+    Scratch s;
+    float trigger = 0.0f;
+    rvea::adapt_refvecs(d_v0, d_objs, d_v, s.get<float>(M), s.get<float>(M), 0, 1, 1.0f, trigger, M, K,
+                        n_active, n_stride, nullptr);
     return status();
 }
 

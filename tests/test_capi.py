@@ -76,3 +76,19 @@ def test_config_struct_matches_header_defaults():
     assert abs(cfg.sparse_ratio - 0.5) < 1e-7 and cfg.rvea_alpha == 2.0 and cfg.use_graphs == 1
     _lib.lib().moea_algorithm_config_defaults(ctypes.byref(cfg), 1)
     assert cfg.mating == 0 and cfg.directions == 1 and abs(cfg.adapt_frequency - 0.1) < 1e-7
+
+
+def test_association_wrappers_reject_mismatched_arguments():
+    """The torch wrappers check dtype, shape and device before any launch: a
+    float64 matrix or a direction matrix with fewer rows than objectives would
+    make the kernels read past their buffers."""
+    import pytest
+    import torch
+    from cuda_moea import stages as st
+    x = torch.zeros((3, 10), dtype=torch.float32)
+    good = torch.ones((3, 4), dtype=torch.float32)
+    for bad_x, bad_r in [(x.double(), good), (x, good.double()), (x, good[:2]), (x[0], good)]:
+        with pytest.raises(ValueError):
+            st.associate_static(bad_x, bad_r)
+        with pytest.raises(ValueError):
+            st.associate(None, bad_x, bad_r)

@@ -135,3 +135,104 @@ def test_rvea_vs_reference(st, ws, oracle):
     gs, ga_ = st.rvea_elitism(ws, _t(ridx), _t(cv), _t(ra), N, refs.shape[1])
     assert ga_ == ra_
     np.testing.assert_array_equal(gs.cpu().numpy(), rs)
+
+
+# ---------------------------------------------------------------- reproduction
+def test_tournament_sbx_pm_bit_exact_vs_reference(st):
+    """The explicit-draw stages against the reference's own kernels
+    (mating_selection.cu:11-35, sbx_crossover.cu:20-70,
+    polynomial_mutation.cu:20-60) on identical draws: same formula, same
+    CUDA powf, so every bit agrees."""
+    rng = np.random.default_rng(81)
+    for n, D, lo, hi in [(257, 33, 0.0, 1.0), (1000, 7, -5.0, 5.0), (64, 1025, -1.0, 3.0)]:
+        parents = (lo + rng.random((n, D)) * (hi - lo)).astype(np.float32)
+        bounds = np.tile([lo, hi], D).astype(np.float32)
+        cv = np.where(rng.random(n) < 0.3, rng.integers(0, 4, n) * 0.5, 0).astype(np.float32)
+        rank = rng.integers(0, 5, n).astype(np.int32)
+        cand = rng.integers(0, n, (n, 2)).astype(np.int32)
+        w_r = R.tournament(cand, rank, cv)
+        np.testing.assert_array_equal(st.tournament(_t(cand), _t(rank), _t(cv)).cpu().numpy(), w_r)
+        pairs = n // 2
+        u = rng.random((pairs * D, 2)).astype(np.float32)
+        u[:7, 0] = [0.0, 0.5, 0.49999997, 0.99999994, 0.25, 0.75, 1e-7]
+        sign = rng.integers(0, 2, pairs * D).astype(np.int32)
+        copy = rng.random(pairs * D).astype(np.float32)
+        for eta, prob, cp in [(30.0, 1.0, 0.0), (30.0, 0.9, 0.5), (2.0, 0.7, 0.2), (100.0, 1.0, 1.0)]:
+            o_r = R.sbx(parents, w_r, bounds, u, sign, copy, eta, prob, cp, n)
+            o_g = st.sbx(_t(parents), _t(w_r), _t(bounds), _t(u), _t(sign), _t(copy), eta, prob, cp, n)
+            np.testing.assert_array_equal(o_g.cpu().numpy().view(np.uint32), o_r.view(np.uint32))
+        um = rng.random((n * D, 2)).astype(np.float32)
+        um[:, 0] *= 0.2 / D * rng.integers(0, 2, n * D)  # about half the values mutate
+        um[:5, 1] = [0.0, 0.5, 0.50000006, 0.99999994, 0.25]
+        for eta, prob in [(20.0, 1.0), (5.0, 0.5)]:
+            m_r = R.pm(o_r, bounds, um, eta, prob)
+            m_g = st.pm(_t(o_r), _t(bounds), _t(um), eta, prob)
+            np.testing.assert_array_equal(m_g.cpu().numpy().view(np.uint32), m_r.view(np.uint32))
+
+
+def test_annealed_index_vs_reference(oracle):
+    """The host-side annealing of the SBX/PM distribution index
+    (sbx_crossover.cu:12-18): the oracle's restatement against the
+    reference's function."""
+    for b, e, g, t in [(30.0, 30.0, 0, 100), (5.0, 40.0, 37, 100), (40.0, 5.0, 99, 100),
+                       (20.0, 3.0, 150, 100), (10.0, 20.0, 3, 0), (7.5, 1.25, 1, 3)]:
+        assert np.float32(oracle.annealed(b, e, g, t)) == np.float32(R.annealed(b, e, g, t))
+
+
+def test_quantize_cv_bit_exact_vs_reference(st, oracle):
+    """Optional CV quantisation (cv_quantization.cu:11-95): product and
+    oracle against the reference's kernel, linear and log mappings."""
+    rng = np.random.default_rng(4)
+    cv = (rng.random(5000) * 3).astype(np.float32)
+    cv[:500] = 0.0
+    cv[500:505] = -0.0
+    cv[505:510] = np.nan
+    cv[510:515] = [1e-4, 2.5, 3.0, 1e30, -1.0]
+    for eps, clip, la, bins in [(0.0, 2.0, 0.0, 16), (1e-3, 2.5, 3.0, 64), (0.0, 10.0, 0.5, 1000)]:
+        want = R.quantize_cv(cv, eps, clip, la, bins)
+        got = st.quantize_cv(_t(cv), eps, clip, la, bins).cpu().numpy()
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+        o = oracle.quantize_cv(cv, eps, clip, la, bins)
+        if la == 0.0:
+            np.testing.assert_array_equal(o.view(np.uint32), want.view(np.uint32))
+        else:  # the host log1pf differs from CUDA's by an ulp near bin edges
+            assert (o != want).mean() < 1e-3
+
+
+def test_rvea_adapt_bit_exact_vs_reference(st, ws, oracle):
+    """Direction adaptation (rvea_reference_adaptation.cu:279-317), called as
+    AdaptiveRVEADirections::update calls it, on populations with dead slots,
+    a degenerate (zero-range) objective and non-finite rows."""
+    rng = np.random.default_rng(17)
+    for M, N, active in [(8, 1024, 900), (3, 92, 92), (5, 500, 1)]:
+        v0 = oracle.reference_directions(2, N, M)
+        objs = (rng.random((M, N)) * rng.random(M)[:, None] * 4).astype(np.float32)
+        objs[:, active:] = 1e15
+        objs[M - 1, :] = 0.25  # zero range in the last objective
+        want = R.rvea_adapt(v0, objs, active)
+        got = st.rvea_adapt(ws, _t(v0), _t(objs), active).cpu().numpy()
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+        np.testing.assert_allclose(oracle.rvea_adapt(v0, objs, active), want, rtol=3e-6, atol=3e-7)
+
+
+def test_fused_reproduction_bit_exact_vs_reference_kernels(st):
+    """The product's fused Philox reproduction (mating, SBX, PM in one pass)
+    against the reference's kernels fed with the same draws, regenerated from
+    the product's Philox stream: tournament and random mating, odd
+    populations, copy probability, every value bit for bit."""
+    import draws
+    rng = np.random.default_rng(5)
+    for n, D, mating, cp, seed, gen in [(300, 13, 1, 0.0, 2024, 5), (301, 7, 1, 0.5, 7, 0),
+                                        (128, 4099, 0, 0.5, 99, 41)]:
+        parents = _t(rng.random((n, D)).astype(np.float32))
+        bounds = _t(np.tile([0.0, 1.0], D).astype(np.float32))
+        cv = _t(np.where(rng.random(n) < 0.2, rng.random(n), 0).astype(np.float32))
+        rank = _t(rng.integers(0, 4, n).astype(np.int32))
+        active = n - 3 if mating == 0 else n
+        off_g, pidx_g = st.reproduce(parents, cv, rank, active, bounds, n, mating=mating, seed=seed,
+                                     generation=gen, sbx_prob=0.9, sbx_copy_prob=cp)
+        off_r, pidx_r = draws.reference_reproduce(st, R, parents, cv, rank, active, bounds, n, mating=mating,
+                                                  seed=seed, generation=gen, sbx_eta=30.0, sbx_prob=0.9,
+                                                  sbx_copy_prob=cp, pm_eta=20.0, pm_prob=1.0)
+        assert torch.equal(pidx_g, pidx_r)
+        assert torch.equal(off_g.view(torch.int32), off_r.view(torch.int32))
