@@ -532,6 +532,56 @@ def other_workload(args, torch, cm):
     print(json.dumps(out))
 
 
+QUALITY = ("DTLZ2 M=3 D=12, N=1024 (RVEA: 990), 500 generations, seeds 0..29: the reference's published "
+           "quality protocol (tests/benchmark/DTLZ/plan.py quality_jobs, adapters/dtlz.py _run_cuda): initial "
+           "population uniform from torch's CPU generator seeded per run, SBX eta 30 pc 1 copy 0.5, PM eta 20, "
+           "NSGA-III on 990 Das-Dennis directions (H=43, clamped >= 1e-6), RVEA adaptive (frequency 0.1, "
+           "alpha 2); IGD in FP64 against 20000 seeded sphere samples (tests/evaluation/pareto_front.py)")
+# tests/benchmark/DTLZ/results/data/quality_summary.csv:14-16, 20-22 (30 runs each, RTX PRO 6000)
+PUBLISHED_QUALITY = {"NSGA3": {"igd_mean": 0.0168882529505434, "igd_std": 2.1336646294516216e-05,
+                               "ms_per_gen_mean": 0.4569740997314453},
+                     "RVEA": {"igd_mean": 0.01699151074727422, "igd_std": 4.04198196642769e-06,
+                              "ms_per_gen_mean": 0.13019642740885418}}
+
+
+def quality_runs(torch, cm, seeds: int = 30, generations: int = 500):
+    """Final IGD and mean ms per generation of NSGA-III and RVEA over seeded
+    runs of the reference's quality protocol, beside its published numbers
+    (Welch's t of the mean IGD difference)."""
+    from cuda_moea import metrics, stages
+    ref = metrics.pareto_front_points("DTLZ2", 3, 20000, 2887).to(torch.float64).cuda()
+    dirs = stages.reference_directions(2, 1024, 3).t().contiguous()   # 990 x 3, clamped
+    out = {}
+    for name in ("NSGA3", "RVEA"):
+        N = 1024 if name == "NSGA3" else 990
+        igds, mss = [], []
+        for seed in range(seeds):
+            gen = torch.Generator(device="cpu").manual_seed(seed)
+            x0 = torch.empty((N, 12), dtype=torch.float32).uniform_(0.0, 1.0, generator=gen)
+            kw = dict(population_size=N, max_generations=generations, problem=cm.DTLZ2(12, 3), seed=seed,
+                      print_progress=False, initial_population=x0,
+                      crossover=cm.SBX(probability=1.0, eta_initial=30.0, eta_final=30.0,
+                                       variable_copy_probability=0.5),
+                      mutation=cm.PolynomialMutation(probability=1.0, eta_initial=20.0, eta_final=20.0))
+            if name == "NSGA3":
+                kw["environment_selector"] = cm.NSGA3EnvironmentSelector(sparse_ratio=1.0)
+                kw["reference_directions"] = cm.UserDefinedDirections(dirs)
+            else:
+                kw["environment_selector"] = cm.RVEAEnvironmentSelector(alpha=2.0)
+                kw["reference_directions"] = cm.AdaptiveRVEADirections(frequency=0.1)
+            r = cm.Algorithm(name, **kw).run()
+            front = r.objectives[: r.active_count]
+            igds.append(metrics.igd(front, ref))
+            mss.append(r.total_ms / generations)
+        pub = PUBLISHED_QUALITY[name]
+        mean, std = statistics.mean(igds), statistics.stdev(igds)
+        welch = (mean - pub["igd_mean"]) / ((std ** 2 + pub["igd_std"] ** 2) / seeds) ** 0.5
+        out[name] = {"runs": seeds, "population": N, "igd_mean": mean, "igd_std": std,
+                     "igd_median": statistics.median(igds), "ms_per_gen_mean": statistics.mean(mss),
+                     "published": pub, "welch_t_vs_published": welch}
+    return out
+
+
 CONSTRAINED_BATCH = ("batched constrained NSGA-III: 64 seeds per launch of C1-DTLZ1 and of C3-DTLZ4, M=10, D=14, "
                      "N=16384, two-layer (3,2) user directions (275), 100-generation runs")
 
@@ -625,7 +675,8 @@ def main() -> None:
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the association-search comparison")
     ap.add_argument("--workload", default="dtlz1-n32768",
-                    choices=["dtlz1-n32768", "constrained-batch", *OTHER_WORKLOADS])
+                    choices=["dtlz1-n32768", "constrained-batch", "quality", *OTHER_WORKLOADS])
+    ap.add_argument("--quality-seeds", type=int, default=30)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -638,6 +689,11 @@ def main() -> None:
         torch.cuda.set_stream(torch.cuda.Stream(0))
         if args.workload == "constrained-batch":
             constrained_batch(args, torch, cm)
+        elif args.workload == "quality":
+            q = quality_runs(torch, cm, seeds=args.quality_seeds)
+            print(json.dumps({"metric": "final IGD (DTLZ2, 500 generations)", "value": q["NSGA3"]["igd_mean"],
+                              "unit": "IGD", "higher_is_better": False, "n_gpus": 1, "dtype": "f32",
+                              "data": "synthetic", "config": {"workload": QUALITY}, "quality": q}))
         else:
             other_workload(args, torch, cm)
         return

@@ -140,6 +140,41 @@ int dmalloc(T** p, size_t count)
 }
 
 }  // namespace
+
+// The next parents from NSGA-III survivors (ascending mixed indices): rows of
+// variables, objectives, violations and, when rank is given, the survivors'
+// fronts (nsga3_population_update.cu:248-300).
+int run_gather_next(const float* vars_a, const float* vars_b, const SplitPop& pop, const int* survivors,
+                    const int* fronts, int N, int D, int M, float* vars, float* objs, float* cv, int* rank,
+                    cudaStream_t stream)
+{
+    gather_next<<<gather_blocks(N, D), 256, 0, stream>>>(vars_a, vars_b, pop, survivors, fronts, N, D, M, vars,
+                                                          objs, cv, rank);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+// Front-0 indices of the first `active` points (RVEAEnvironmentSelector::
+// finalize, front_zero.cu:200-293): *h_count receives their number (the
+// stream is synchronised).
+int run_front_zero(Workspace& ws, const float* objs, const float* cv, int n_stride, int active, int M,
+                   int* out, int* h_count, cudaStream_t stream)
+{
+    *h_count = 0;
+    if (active <= 0) return MOEA_OK;
+    SplitPop pop{objs, objs, cv, cv, n_stride, n_stride, active, active};
+    MOEA_TRY(run_ndsort(ws, pop, M, 1, ws.selected, stream));
+    zero_front_pick<<<ceil_div(active, 256), 256, 0, stream>>>(ws.selected, active, ws.flags);
+    MOEA_TRY(run_flag_compaction(ws, active, out, stream));
+    std::vector<int> flags(active);
+    MOEA_CUDA_TRY(cudaMemcpyAsync(flags.data(), ws.flags, sizeof(int) * active, cudaMemcpyDeviceToHost, stream));
+    MOEA_CUDA_TRY(cudaStreamSynchronize(stream));
+    int c = 0;
+    for (int v : flags) c += v != 0;
+    *h_count = c;
+    return workspace_check_status(ws, stream);
+}
+
 }  // namespace moea
 
 using namespace moea;
@@ -764,17 +799,7 @@ struct moea_algorithm {
         if (nsga3()) return MOEA_OK;
         const int active = active_count_sync();
         frontzero_count = 0;
-        if (active <= 0) return MOEA_OK;
-        MOEA_TRY(run_ndsort(ws, merged_view(objs[P], cv[P], active), M, 1, ws.selected, stream));
-        zero_front_pick<<<ceil_div(active, 256), 256, 0, stream>>>(ws.selected, active, ws.flags);
-        MOEA_TRY(run_flag_compaction(ws, active, frontzero, stream));
-        std::vector<int> flags(active);
-        MOEA_CUDA_TRY(cudaMemcpyAsync(flags.data(), ws.flags, sizeof(int) * active, cudaMemcpyDeviceToHost, stream));
-        MOEA_CUDA_TRY(cudaStreamSynchronize(stream));
-        int c = 0;
-        for (int v : flags) c += v != 0;
-        frontzero_count = c;
-        return workspace_check_status(ws, stream);
+        return run_front_zero(ws, objs[P], cv[P], N, active, M, frontzero, &frontzero_count, stream);
     }
 
     // finalize plus the snapshot of the current generation (reference result())

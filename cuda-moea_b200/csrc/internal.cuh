@@ -136,6 +136,14 @@ struct Workspace {
 // ---- per-TU entry points -------------------------------------------------
 // Non-dominated sort of the split view.  Fronts in point order into ws.fronts
 // (or out_fronts when non-null), max front into ws.counters[2].
+// Passes of the Philox variation: SBX and PM fused, SBX alone, PM alone (in
+// place).  The draws are the same in every form.
+enum VariationPass { kPassBoth = 3, kPassCrossover = 1, kPassMutation = 2 };
+int run_variation_pass(int passes, const float* parents, const int* pidx, const float* bounds, float* off,
+                       int n_off, int D, float sbx_eta0, float sbx_eta1, float sbx_prob, float copy_prob,
+                       int mutate, float pm_eta0, float pm_eta1, float pm_prob, int total,
+                       uint64_t seed, const int* d_gen, uint32_t gen, cudaStream_t stream);
+
 int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_fronts,
                cudaStream_t stream);
 

@@ -169,6 +169,12 @@ __device__ __forceinline__ float low_bytes_unit(uint32_t a, uint32_t b, uint32_t
 // unused low bytes of words 1-3).  A second block (tag mutation) is computed
 // only where a child mutates, with probability pm_prob/D per child: at large
 // D almost every element costs one block instead of two.
+//
+// kCross / kMutate select the passes: both (the fused variation), crossover
+// alone (children written unmutated) or mutation alone (children read from
+// off and mutated in place).  The draws are the same in every form, so
+// crossover followed by mutation equals the fused pass bit for bit.
+template <bool kCross, bool kMutate>
 __device__ __forceinline__ void variation_element(long long e, int p, int d,
                                                   const float* __restrict__ parents,
                                                   const int* __restrict__ pidx,
@@ -182,17 +188,22 @@ __device__ __forceinline__ void variation_element(long long e, int p, int d,
     const int ca = 2 * p, cb = ca + 1;
     uint32_t r[4];
     rng_block(seed, (uint64_t)e, gen, kTagCrossover, r);
-    float c1, c2;
-    if (p < pairs) {
-        const float x1 = parents[(size_t)pidx[ca] * D + d];
-        const float x2 = parents[(size_t)pidx[cb] * D + d];
-        sbx_pair(x1, x2, u32_to_unit(r[0]), u32_to_unit(r[1]), (int)(r[0] & 1u),
-                 u32_to_unit(r[2]), eta_c, sbx_prob, copy_prob, lo, hi, c1, c2);
+    float c1, c2 = 0.0f;
+    if (kCross) {
+        if (p < pairs) {
+            const float x1 = parents[(size_t)pidx[ca] * D + d];
+            const float x2 = parents[(size_t)pidx[cb] * D + d];
+            sbx_pair(x1, x2, u32_to_unit(r[0]), u32_to_unit(r[1]), (int)(r[0] & 1u),
+                     u32_to_unit(r[2]), eta_c, sbx_prob, copy_prob, lo, hi, c1, c2);
+        } else {
+            c1 = parents[(size_t)pidx[ca] * D + d];  // odd population: last child copies its parent
+        }
     } else {
-        c1 = parents[(size_t)pidx[ca] * D + d];  // odd population: last child copies its parent
-        c2 = 0.0f;
+        c1 = off[(size_t)ca * D + d];
+        if (p < pairs) c2 = off[(size_t)cb * D + d];
     }
-    if (mutate) {
+    bool changed = kCross;
+    if (kMutate && mutate) {
         // the reference's test, polynomial_mutation.cu:34
         const float limit = pm_prob / static_cast<float>(D);
         const float ta = u32_to_unit(r[3]);
@@ -203,12 +214,15 @@ __device__ __forceinline__ void variation_element(long long e, int p, int d,
             rng_block(seed, (uint64_t)e, gen, kTagMutation, m);
             if (ma) c1 = pm_value(c1, ta, u32_to_unit(m[0]), eta_m, pm_prob, D, lo, hi);
             if (mb) c2 = pm_value(c2, tb, u32_to_unit(m[1]), eta_m, pm_prob, D, lo, hi);
+            changed = true;
         }
     }
+    if (!changed) return;  // mutation pass: untouched children stay as they are
     off[(size_t)ca * D + d] = c1;
     if (p < pairs) off[(size_t)cb * D + d] = c2;
 }
 
+template <bool kCross, bool kMutate>
 __global__ void variation_philox(const float* __restrict__ parents, const int* __restrict__ pidx,
                                  const float* __restrict__ bounds, float* __restrict__ off,
                                  int n_off, int D, float sbx_eta0, float sbx_eta1, float sbx_prob,
@@ -224,15 +238,15 @@ __global__ void variation_philox(const float* __restrict__ parents, const int* _
     if (count <= 0x7FFFFFFFll) {  // 32-bit row/column split
         for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < (int)count; e += gridDim.x * blockDim.x) {
             const int p = e / D;
-            variation_element(e, p, e - p * D, parents, pidx, bounds, off, pairs, D, eta_c, sbx_prob, copy_prob,
-                              mutate, eta_m, pm_prob, seed, gen);
+            variation_element<kCross, kMutate>(e, p, e - p * D, parents, pidx, bounds, off, pairs, D, eta_c,
+                                               sbx_prob, copy_prob, mutate, eta_m, pm_prob, seed, gen);
         }
         return;
     }
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < count;
          e += (long long)gridDim.x * blockDim.x)
-        variation_element(e, (int)(e / D), (int)(e % D), parents, pidx, bounds, off, pairs, D, eta_c, sbx_prob,
-                          copy_prob, mutate, eta_m, pm_prob, seed, gen);
+        variation_element<kCross, kMutate>(e, (int)(e / D), (int)(e % D), parents, pidx, bounds, off, pairs, D,
+                                           eta_c, sbx_prob, copy_prob, mutate, eta_m, pm_prob, seed, gen);
 }
 
 // ---- fused batch: mating then variation of every instance (blockIdx.y) ----
@@ -254,8 +268,8 @@ __global__ void fused_variation(const BatchInst* __restrict__ insts, const int* 
     const float eta_m = annealed_eta(I.pm_eta0, I.pm_eta1, (int)gen, I.T);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < (int)count; e += gridDim.x * blockDim.x) {
         const int p = e / I.D;  // fused instances hold at most 4096 x 263 elements
-        variation_element(e, p, e - p * I.D, I.varsP, I.pidx, I.bounds, I.varsO, pairs, I.D, eta_c, I.sbx_prob,
-                          I.sbx_copy, I.mutate, eta_m, I.pm_prob, I.seed, gen);
+        variation_element<true, true>(e, p, e - p * I.D, I.varsP, I.pidx, I.bounds, I.varsO, pairs, I.D, eta_c,
+                                      I.sbx_prob, I.sbx_copy, I.mutate, eta_m, I.pm_prob, I.seed, gen);
     }
 }
 
@@ -301,17 +315,36 @@ int run_mating(const float* cv, const int* rank, const int* d_active, int active
     return MOEA_OK;
 }
 
+int run_variation_pass(int passes, const float* parents, const int* pidx, const float* bounds, float* off,
+                       int n_off, int D, float sbx_eta0, float sbx_eta1, float sbx_prob, float copy_prob,
+                       int mutate, float pm_eta0, float pm_eta1, float pm_prob, int total,
+                       uint64_t seed, const int* d_gen, uint32_t gen, cudaStream_t stream)
+{
+    const long long count = (long long)(n_off / 2 + (n_off & 1)) * D;
+    const int grid = grid_for(count, 256);
+    if (passes == kPassBoth)
+        variation_philox<true, true><<<grid, 256, 0, stream>>>(
+            parents, pidx, bounds, off, n_off, D, sbx_eta0, sbx_eta1, sbx_prob, copy_prob, mutate,
+            pm_eta0, pm_eta1, pm_prob, total, seed, d_gen, gen);
+    else if (passes == kPassCrossover)
+        variation_philox<true, false><<<grid, 256, 0, stream>>>(
+            parents, pidx, bounds, off, n_off, D, sbx_eta0, sbx_eta1, sbx_prob, copy_prob, 0,
+            pm_eta0, pm_eta1, pm_prob, total, seed, d_gen, gen);
+    else
+        variation_philox<false, true><<<grid, 256, 0, stream>>>(
+            parents, pidx, bounds, off, n_off, D, sbx_eta0, sbx_eta1, sbx_prob, copy_prob, 1,
+            pm_eta0, pm_eta1, pm_prob, total, seed, d_gen, gen);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
 int run_variation(const float* parents, const int* pidx, const float* bounds, float* off,
                   int n_off, int D, float sbx_eta0, float sbx_eta1, float sbx_prob, float copy_prob,
                   int mutate, float pm_eta0, float pm_eta1, float pm_prob, int total,
                   uint64_t seed, const int* d_gen, uint32_t gen, cudaStream_t stream)
 {
-    const long long count = (long long)(n_off / 2 + (n_off & 1)) * D;
-    variation_philox<<<grid_for(count, 256), 256, 0, stream>>>(
-        parents, pidx, bounds, off, n_off, D, sbx_eta0, sbx_eta1, sbx_prob, copy_prob, mutate,
-        pm_eta0, pm_eta1, pm_prob, total, seed, d_gen, gen);
-    MOEA_CUDA_TRY(cudaGetLastError());
-    return MOEA_OK;
+    return run_variation_pass(kPassBoth, parents, pidx, bounds, off, n_off, D, sbx_eta0, sbx_eta1, sbx_prob,
+                              copy_prob, mutate, pm_eta0, pm_eta1, pm_prob, total, seed, d_gen, gen, stream);
 }
 
 int fused_reproduce(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s)
@@ -398,6 +431,15 @@ moea_status moea_reproduce(const float* d_parents, const float* d_parent_cv, con
     return run_variation(d_parents, d_parent_idx, d_bounds, d_off, n_off, D, sbx_eta, sbx_eta,
                          sbx_prob, sbx_copy_prob, mutate, pm_eta, pm_eta, pm_prob, 0, seed, nullptr,
                          generation, s);
+}
+
+moea_status moea_initialize_population(uint64_t seed, uint32_t epoch, const float* d_bounds, int N, int D,
+                                      float* d_vars, void* stream)
+{
+    if (!d_bounds || !d_vars || N < 1 || D < 1)
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "initialize_population: bad arguments");
+    return run_init_uniform(d_vars, d_bounds, N, D, derive_seed(seed) ^ ((uint64_t)epoch << 48),
+                            (cudaStream_t)stream);
 }
 
 moea_status moea_rng_blocks(uint64_t seed, uint32_t generation, uint32_t tag, int64_t count,

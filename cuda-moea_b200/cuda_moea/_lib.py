@@ -24,6 +24,23 @@ MATING_FN = ctypes.CFUNCTYPE(c_int, vp, vp, vp, vp, vp, c_int, vp, c_int, c_int,
 PREPARE_FN = ctypes.CFUNCTYPE(c_int, vp, vp, vp, vp, c_int, c_int, c_int, c_int, c_int, vp, ip)
 RESET_FN = ctypes.CFUNCTYPE(None, vp)
 
+class PopulationDesc(ctypes.Structure):
+    """moea_population_desc: a borrowed population for the strategy handles."""
+    _fields_ = [("d_variables", vp), ("d_objectives", vp), ("d_constraints", vp), ("d_bounds", vp),
+                ("size", c_int), ("dimension", c_int), ("objectives", c_int)]
+
+
+class GenerationDesc(ctypes.Structure):
+    """moea_generation_desc: the reference's GenerationContext plus the run seed."""
+    _fields_ = [("generation", c_int), ("max_generations", c_int), ("seed", c_u64)]
+
+
+class NSGA3SelectorConfig(ctypes.Structure):
+    """moea_nsga3_selector_config."""
+    _fields_ = [("sparse_ratio", c_float), ("cv_bins", c_int), ("cv_clip_upper", c_float),
+                ("cv_log_alpha", c_float), ("feasibility_epsilon", c_float), ("association_mode", c_int)]
+
+
 MOEA_OK = 0
 ERROR_NAMES = {1: "invalid argument", 2: "CUDA error", 3: "unsupported", 4: "invalid state",
                5: "device timeout", 6: "out of memory", 7: "callback failed", 8: "load failed"}
@@ -128,6 +145,40 @@ _SIGNATURES = [
     ("moea_reproduce", c_int, [vp, vp, vp, c_int, vp, vp, vp, c_int, c_int, c_int, c_int, c_float,
                                c_float, c_float, c_int, c_float, c_float, c_u64, c_u32, vp]),
     ("moea_rng_blocks", c_int, [c_u64, c_u32, c_u32, c_i64, vp, vp]),
+    ("moea_initialize_population", c_int, [c_u64, c_u32, vp, c_int, c_int, vp, vp]),
+    # strategy handles
+    ("moea_create_dasdennis", c_int, [c_int, ctypes.POINTER(vp)]),
+    ("moea_create_adaptive_directions", c_int, [c_float, ctypes.POINTER(vp)]),
+    ("moea_create_user_directions", c_int, [fp, c_int, c_int, c_int, ctypes.POINTER(vp)]),
+    ("moea_directions_initialize", c_int, [vp, c_int, c_int, c_int, vp]),
+    ("moea_directions_view", c_int, [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), ip, ip]),
+    ("moea_directions_update", c_int, [vp, ctypes.POINTER(PopulationDesc), vp, ctypes.POINTER(GenerationDesc), vp]),
+    ("moea_directions_reset", c_int, [vp, vp]),
+    ("moea_directions_destroy", None, [vp]),
+    ("moea_create_tournament", c_int, [ctypes.POINTER(vp)]),
+    ("moea_create_random_mating", c_int, [ctypes.POINTER(vp)]),
+    ("moea_mating_select", c_int, [vp, ctypes.POINTER(PopulationDesc), vp, vp, vp, c_int,
+                                   ctypes.POINTER(GenerationDesc), vp]),
+    ("moea_mating_destroy", None, [vp]),
+    ("moea_create_sbx", c_int, [c_float, c_float, c_float, c_float, ctypes.POINTER(vp)]),
+    ("moea_crossover_apply", c_int, [vp, ctypes.POINTER(PopulationDesc), vp, ctypes.POINTER(PopulationDesc),
+                                     ctypes.POINTER(GenerationDesc), vp]),
+    ("moea_crossover_destroy", None, [vp]),
+    ("moea_create_pm", c_int, [c_float, c_float, c_float, ctypes.POINTER(vp)]),
+    ("moea_mutation_apply", c_int, [vp, ctypes.POINTER(PopulationDesc), ctypes.POINTER(GenerationDesc), vp]),
+    ("moea_mutation_destroy", None, [vp]),
+    ("moea_create_nsga3_selector", c_int, [ctypes.POINTER(NSGA3SelectorConfig), ctypes.POINTER(vp)]),
+    ("moea_create_rvea_selector", c_int, [c_float, ctypes.POINTER(vp)]),
+    ("moea_selector_initialize", c_int, [vp, c_int, c_int, c_int, c_int, vp, c_int, vp]),
+    ("moea_selector_prepare", c_int, [vp, ctypes.POINTER(PopulationDesc), ctypes.POINTER(GenerationDesc), vp]),
+    ("moea_selector_select", c_int, [vp, ctypes.POINTER(PopulationDesc), ctypes.POINTER(PopulationDesc),
+                                     ctypes.POINTER(PopulationDesc), ctypes.POINTER(GenerationDesc), vp]),
+    ("moea_selector_mating_state", c_int, [vp, ctypes.POINTER(vp), ctypes.POINTER(vp)]),
+    ("moea_selector_active_count", c_int, [vp, ip, vp]),
+    ("moea_selector_finalize", c_int, [vp, ctypes.POINTER(PopulationDesc), vp]),
+    ("moea_selector_result_indices", c_int, [vp, ctypes.POINTER(vp), ip]),
+    ("moea_selector_reset", c_int, [vp, vp]),
+    ("moea_selector_destroy", None, [vp]),
     ("moea_problem_evaluate", c_int, [c_int, vp, c_int, c_int, c_int, vp, vp, vp]),
     ("moea_reference_directions", c_int, [c_int, c_int, c_int, fp, c_size_t, ip]),
     ("moea_algorithm_config_defaults", None, [ctypes.POINTER(AlgorithmConfig), c_int]),

@@ -179,14 +179,27 @@ class Algorithm:
         raise TypeError(f"unsupported problem specification {t}")
 
     def _validate_unsupported(self) -> None:
-        for key in ("crossover", "mutation", "environment_selector"):
-            t = self._specs[key]["type"]
-            if t.startswith("Python"):
-                self._deferred_error = NotImplementedError(
-                    f"{t} is not supported by the B200 backend (only PythonProblem, "
-                    "PythonMating and PythonReferenceDirections are)")
-                return
+        """Python crossover, mutation and environmental selection (and a
+        Python direction provider that updates) run through the composed
+        step (composed.py): every generation assembled from strategy handles
+        and Python objects, as the reference's adapters compose them."""
+        from .composed import needs_composition
+        self._compose = needs_composition(self._specs)
+        self._composed = None
         self._deferred_error = None
+        if self._compose and self._save_data is not None:
+            self._deferred_error = NotImplementedError(
+                "snapshots (save_data) are written by the algorithm object; strategies in Python run "
+                "through the composed step, which does not write them")
+
+    def _composed_run(self):
+        """The composed step's run object (created on first use)."""
+        if self._deferred_error is not None:
+            raise self._deferred_error
+        if self._composed is None:
+            from .composed import ComposedRun
+            self._composed = ComposedRun(self)
+        return self._composed
 
     def _build_config(self) -> tuple[AlgorithmConfig, list]:
         keep: list = []
@@ -395,27 +408,43 @@ class Algorithm:
         return self._native.handle
 
     def initialize(self) -> None:
+        if self._compose:
+            self._composed_run().initialize()
+            return
         h = self._ensure_native()
         self._call(lib().moea_algorithm_initialize, h)
 
     def step(self) -> None:
-        h = self._ensure_native()
-        self._call(lib().moea_algorithm_step, h)
+        if self._compose:
+            self._composed_run().step()
+        else:
+            h = self._ensure_native()
+            self._call(lib().moea_algorithm_step, h)
         if self._print_progress:
             g = self.generation
             if g == self._max_generations or (self._progress_interval > 0 and g % self._progress_interval == 0):
                 print(f"Generation {g} / {self._max_generations} completed")
 
     def run(self, *, copy: bool = True) -> Result:
-        h = self._ensure_native()
-        total = ctypes.c_double(0.0)
-        self._call(lib().moea_algorithm_run, h, ctypes.byref(total))
-        self._result_total_ms = float(total.value)
+        if self._compose:
+            self._result_total_ms = self._composed_run().run()
+        else:
+            h = self._ensure_native()
+            total = ctypes.c_double(0.0)
+            self._call(lib().moea_algorithm_run, h, ctypes.byref(total))
+            self._result_total_ms = float(total.value)
         if self._print_progress:
             print(f"Generation {self.generation} / {self._max_generations} completed")
         return self.result(copy=copy)
 
     def result(self, *, copy: bool = True) -> Result:
+        if self._compose:
+            c = self._composed_run()
+            aux, active = c.finalize()
+            x, f, cv = c.P.x, c.P.f.t(), c.P.cv
+            if copy:
+                x, f, cv = x.clone(), f.contiguous(), cv.clone()
+            return Result(x, f, cv, aux, int(active), float(c.total_ms))
         if self._native is None or not self.initialized:
             raise RuntimeError("Algorithm has not been initialized")
         h = self._native.handle
@@ -432,8 +461,14 @@ class Algorithm:
         return Result(pop.variables, pop.objectives, pop.constraints, aux, int(v.active_count),
                       float(v.total_ms))
 
+    def _native_only(self, what: str) -> None:
+        if self._compose:
+            raise NotImplementedError(f"{what} belongs to the algorithm object; this run composes Python "
+                                      "strategies")
+
     def profile_step(self) -> list[tuple[str, float]]:
         """Runs one generation with direct launches; device ms per stage."""
+        self._native_only("profile_step")
         h = self._ensure_native()
         names = ctypes.create_string_buffer(4096)
         ms = (ctypes.c_float * 64)()
@@ -444,6 +479,7 @@ class Algorithm:
 
     def selection_stats(self) -> dict:
         """NSGA-III: last front index and sizes of the latest selection."""
+        self._native_only("selection_stats")
         mf = ctypes.c_int(-1)
         sz = (ctypes.c_int * 4)()
         self._call(lib().moea_algorithm_selection_stats, self._ensure_native(), ctypes.byref(mf), sz)
@@ -452,10 +488,16 @@ class Algorithm:
     @property
     def graph_info(self) -> tuple[bool, int]:
         """(generations replay a CUDA graph, kernel nodes per generation)."""
+        if self._compose:
+            return False, 0
         v = self._view_struct()
         return bool(v.graph_active), int(v.kernels_per_generation)
 
     def reset(self) -> None:
+        if self._compose:
+            if self._composed is not None:
+                self._composed.reset()
+            return
         if self._native is None or not self.initialized:
             return
         self._call(lib().moea_algorithm_reset, self._native.handle)
@@ -465,6 +507,7 @@ class Algorithm:
         snapshots (``<save_data>/generation_NNNNNN``): the population and the
         selection state are replaced, and the following steps equal those of
         the run that wrote it when the configuration is the same."""
+        self._native_only("load_snapshot")
         h = self._ensure_native()
         self._call(lib().moea_algorithm_load_snapshot, h, os.fsencode(os.fspath(directory)))
 
@@ -474,6 +517,10 @@ class Algorithm:
             self._call(lib().moea_algorithm_flush_snapshots, self._native.handle)
 
     def synchronize(self) -> None:
+        if self._compose:
+            if self._composed is not None and self._composed.stream is not None:
+                self._composed.stream.synchronize()
+            return
         if self._native is not None:
             self._call(lib().moea_algorithm_synchronize, self._native.handle)
 
@@ -492,6 +539,12 @@ class Algorithm:
 
     @property
     def population(self) -> Population:
+        if self._compose:
+            c = self._composed
+            if c is None or not c.initialized:
+                raise RuntimeError("Algorithm has not been initialized")
+            c.stream.synchronize()
+            return Population(c.P.x, c.P.f.t(), c.P.cv)
         if self._native is None or not self.initialized:
             raise RuntimeError("Algorithm has not been initialized")
         self.synchronize()
@@ -500,11 +553,16 @@ class Algorithm:
     def population_view(self) -> Population:
         """Zero-copy views of the current parents without synchronising; valid
         for work ordered on the algorithm's stream until the next step."""
+        if self._compose:
+            c = self._composed_run()
+            return Population(c.P.x, c.P.f.t(), c.P.cv)
         return self._population_tensors(self._view_struct(), False)
 
     @property
     def reference_directions(self) -> torch.Tensor:
         """Directions in use, objective-major (M, count) view."""
+        if self._compose:
+            return self._composed_run().reference_directions
         ptr, count = ctypes.c_void_p(), ctypes.c_int()
         self._call(lib().moea_algorithm_directions, self._native.handle, ctypes.byref(ptr),
                    ctypes.byref(count))
@@ -512,18 +570,24 @@ class Algorithm:
 
     @property
     def initialized(self) -> bool:
+        if self._compose:
+            return self._composed is not None and self._composed.initialized
         if self._native is None:
             return False
         return bool(self._view_struct().initialized)
 
     @property
     def finished(self) -> bool:
+        if self._compose:
+            return self._composed is not None and self._composed.generation >= self._max_generations
         if self._native is None:
             return False
         return bool(self._view_struct().finished)
 
     @property
     def generation(self) -> int:
+        if self._compose:
+            return 0 if self._composed is None else self._composed.generation
         if self._native is None:
             return 0
         return int(self._view_struct().generation)

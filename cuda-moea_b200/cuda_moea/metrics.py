@@ -9,6 +9,13 @@ computed in FP64 on the device (moea_igd in libmoea_b200).
 dtlz_reference_front() gives deterministic points of the analytic Pareto
 fronts of DTLZ1-4: Das-Dennis points on the simplex sum(f) = 0.5 (DTLZ1) or
 on the unit sphere (DTLZ2-4).
+
+pareto_front_points() draws the seeded analytic-front samples that the
+reference's published quality numbers are measured against
+(tests/evaluation/pareto_front.py:17-33, 142-175): for DTLZ1 normalised
+exponentials on the simplex sum(f) = 0.5, for DTLZ2-4 uniform points of the
+positive orthant scaled onto the unit sphere, both from torch's CPU
+generator seeded with `seed`, in FP32.
 """
 from __future__ import annotations
 
@@ -68,3 +75,18 @@ def dtlz_reference_front(problem: str, objectives: int, partitions: int) -> torc
     else:
         raise ValueError("analytic fronts are provided for DTLZ1-4")
     return torch.from_numpy(f)
+
+
+def pareto_front_points(problem: str, objectives: int, count: int = 20000, seed: int = 2887) -> torch.Tensor:
+    """(count, M) FP32 samples of the analytic front of DTLZ1-4 (CPU)."""
+    name = problem.upper()
+    if objectives < 2 or count <= 0:
+        raise ValueError("need at least two objectives and a positive count")
+    gen = torch.Generator(device="cpu").manual_seed(seed)
+    u = torch.rand((count, objectives), generator=gen, dtype=torch.float32)
+    if name == "DTLZ1":
+        e = -torch.log(u.clamp_min(torch.finfo(torch.float32).tiny))
+        return 0.5 * e / e.sum(dim=1, keepdim=True)
+    if name in ("DTLZ2", "DTLZ3", "DTLZ4"):
+        return u / u.norm(dim=1, keepdim=True).clamp_min(torch.finfo(torch.float32).eps)
+    raise ValueError("seeded front samples are provided for DTLZ1-4")

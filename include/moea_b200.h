@@ -221,6 +221,13 @@ moea_status moea_reproduce(const float* d_parents, const float* d_parent_cv,
                            int mating, float sbx_eta, float sbx_prob, float sbx_copy_prob,
                            int mutate, float pm_eta, float pm_prob, uint64_t seed,
                            uint32_t generation, void* stream);
+/* Random initial population x = lb + u (ub - lb), u uniform in [0, 1) from
+ * the product's Philox stream of the run seed (CudaConfig.seed, derived as
+ * the algorithm object derives it) and reset epoch (0 for the first run):
+ * the algorithm object's own initial population.  Replaces
+ * Population::initialize_random (nat/src/core/population.cu:97-115). */
+moea_status moea_initialize_population(uint64_t seed, uint32_t epoch, const float* d_bounds, int N, int D,
+                                      float* d_vars, void* stream);
 /* The raw product draws of moea_reproduce, for checking: d_out (count,4). */
 moea_status moea_rng_blocks(uint64_t seed, uint32_t generation, uint32_t tag, int64_t count,
                             uint32_t* d_out, void* stream);
@@ -241,6 +248,136 @@ moea_status moea_problem_evaluate(int kind, const float* d_x, int N, int D, int 
  * written when non-NULL and capacity (floats) suffices. */
 moea_status moea_reference_directions(int mode, int n, int M, float* h_out, size_t capacity,
                                       int* h_count);
+
+/* ========================================================================
+ * Strategy handles: the reference's strategy interfaces as opaque objects, so
+ * a host program can assemble a generation from them the way
+ * EvolutionaryAlgorithm::step does (nat/src/algorithm/algorithm.cu:104-286):
+ * mating -> crossover -> mutation -> evaluation -> environmental selection ->
+ * direction update.  Every call is ordered on `stream` and returns without
+ * waiting for the device; sizes that the reference keeps on the host (the
+ * RVEA active count, the front sizes) stay on the device.  Populations are
+ * borrowed views for the duration of a call, as in the reference.
+ * ====================================================================== */
+
+/* A borrowed population (the reference's PopulationView,
+ * nat/include/cuda_moea/core/types.cuh:21-51): variables (size, dimension)
+ * row-major, objectives (objectives, size) objective-major, constraint
+ * violation (size), bounds interleaved (2 * dimension). */
+typedef struct moea_population_desc {
+    float* d_variables;
+    float* d_objectives;
+    float* d_constraints;
+    const float* d_bounds;
+    int size, dimension, objectives;
+} moea_population_desc;
+
+/* The reference's GenerationContext (nat/include/cuda_moea/core/contexts.cuh):
+ * the generation index, the horizon and the run's seed (CudaConfig.seed; every
+ * handle derives its draws from it the way the algorithm object does, so a
+ * generation assembled from handles equals the algorithm's). */
+typedef struct moea_generation_desc {
+    int generation;
+    int max_generations;
+    uint64_t seed;
+} moea_generation_desc;
+
+/* ---- reference directions (IReferenceDirectionProvider,
+ * nat/include/cuda_moea/reference/reference_direction_provider.cuh:11-26) ---- */
+typedef struct moea_directions moea_directions;
+/* DasDennisDirections{partitions} (0: from the requested count). */
+moea_status moea_create_dasdennis(int partitions, moea_directions** out);
+/* AdaptiveRVEADirections{frequency} (reference_directions.cu:61-162). */
+moea_status moea_create_adaptive_directions(float frequency, moea_directions** out);
+/* UserDefinedDirections: h_values (M, count) objective-major, copied
+ * (reference_directions.cu:180-237). */
+moea_status moea_create_user_directions(const float* h_values, int M, int count, int normalize,
+                                        moea_directions** out);
+moea_status moea_directions_initialize(moea_directions* d, int requested_count, int M, int device,
+                                       void* stream);
+/* view(): directions, initial directions, gamma (NULL unless adaptive), M, count. */
+moea_status moea_directions_view(moea_directions* d, const float** d_values, const float** d_initial,
+                                 const float** d_gamma, int* M, int* count);
+/* update(): adaptive directions adapt on the reference's schedule (every
+ * max(1, lround(frequency * max_generations)) completed generations) to the
+ * first *d_active columns of pop's objectives (d_active NULL: all). */
+moea_status moea_directions_update(moea_directions* d, const moea_population_desc* pop, const int* d_active,
+                                   const moea_generation_desc* ctx, void* stream);
+moea_status moea_directions_reset(moea_directions* d, void* stream);
+void moea_directions_destroy(moea_directions* d);
+
+/* ---- mating (IMatingSelector, nat/include/cuda_moea/reproduction/mating_selector.cuh:9-19) ---- */
+typedef struct moea_mating moea_mating;
+moea_status moea_create_tournament(moea_mating** out);   /* TournamentMating (mating_selection.cu:74) */
+moea_status moea_create_random_mating(moea_mating** out); /* RandomMating (mating_selection.cu:39) */
+/* select(): d_parent_idx (count) from parents; d_rank (tournament: required,
+ * mating_selection.cu:80-86) and d_active (NULL: parents->size) come from the
+ * selector's mating state. */
+moea_status moea_mating_select(moea_mating* m, const moea_population_desc* parents, const int* d_rank,
+                               const int* d_active, int* d_parent_idx, int count,
+                               const moea_generation_desc* ctx, void* stream);
+void moea_mating_destroy(moea_mating* m);
+
+/* ---- crossover (ICrossoverOperator, crossover_operator.cuh:9-19) ---- */
+typedef struct moea_crossover moea_crossover;
+/* SimulatedBinaryCrossover{eta_initial, eta_final, probability,
+ * variable_copy_probability} (sbx_crossover.cu:73-190). */
+moea_status moea_create_sbx(float eta_initial, float eta_final, float probability, float copy_probability,
+                            moea_crossover** out);
+/* apply(): offspring->size children from parents and d_parent_idx (size). */
+moea_status moea_crossover_apply(moea_crossover* c, const moea_population_desc* parents, const int* d_parent_idx,
+                                 moea_population_desc* offspring, const moea_generation_desc* ctx, void* stream);
+void moea_crossover_destroy(moea_crossover* c);
+
+/* ---- mutation (IMutationOperator, mutation_operator.cuh:9-17) ---- */
+typedef struct moea_mutation moea_mutation;
+/* PolynomialMutation{eta_initial, eta_final, probability} (polynomial_mutation.cu:63-124). */
+moea_status moea_create_pm(float eta_initial, float eta_final, float probability, moea_mutation** out);
+/* mutate(): offspring variables in place. */
+moea_status moea_mutation_apply(moea_mutation* m, moea_population_desc* offspring, const moea_generation_desc* ctx,
+                                void* stream);
+void moea_mutation_destroy(moea_mutation* m);
+
+/* ---- environmental selection (IEnvironmentSelector,
+ * nat/include/cuda_moea/selection/environment_selector.cuh:9-33) ---- */
+typedef struct moea_selector moea_selector;
+typedef struct moea_nsga3_selector_config {
+    float sparse_ratio;       /* validated; the bitmask relation needs no pair buffer */
+    int cv_bins;              /* CVQuantizationConfig (0: off) */
+    float cv_clip_upper, cv_log_alpha, feasibility_epsilon;
+    int association_mode;     /* MOEA_ASSOC_* */
+} moea_nsga3_selector_config;
+/* NSGA3EnvironmentSelector (nsga3_environment_selector.cu:50-566); cfg NULL:
+ * the reference defaults. */
+moea_status moea_create_nsga3_selector(const moea_nsga3_selector_config* cfg, moea_selector** out);
+/* RVEAEnvironmentSelector{alpha} (rvea_environment_selector.cu:52-324). */
+moea_status moea_create_rvea_selector(float alpha, moea_selector** out);
+/* initialize(AlgorithmInfo, provider, CudaContext): allocates the selector's
+ * scratch for population_size N (merged 2N) once.  The provider must be
+ * initialized and outlive the selector (the reference keeps a raw pointer). */
+moea_status moea_selector_initialize(moea_selector* s, int population_size, int dimension, int objectives,
+                                     int max_generations, moea_directions* directions, int device, void* stream);
+/* prepare(): NSGA-III sorts the parents (mating ranks, running ideal point on
+ * the first call); RVEA keeps its active count. */
+moea_status moea_selector_prepare(moea_selector* s, const moea_population_desc* parents,
+                                  const moea_generation_desc* ctx, void* stream);
+/* select(): the next population from parents + offspring, written to next. */
+moea_status moea_selector_select(moea_selector* s, const moea_population_desc* parents,
+                                 const moea_population_desc* offspring, moea_population_desc* next,
+                                 const moea_generation_desc* ctx, void* stream);
+/* mating_state(): device pointers of the parents' ranks (NSGA-III; NULL for
+ * RVEA) and of the active count (one int). */
+moea_status moea_selector_mating_state(moea_selector* s, const int** d_rank, const int** d_active);
+/* active_count(): reads the device count back (synchronises the stream). */
+moea_status moea_selector_active_count(moea_selector* s, int* h_active, void* stream);
+/* finalize(): RVEA computes the front-0 indices of the active parents
+ * (front_zero.cu:244-293; synchronises); NSGA-III does nothing. */
+moea_status moea_selector_finalize(moea_selector* s, const moea_population_desc* population, void* stream);
+/* result_indices(): NSGA-III the parents' fronts (count = size), RVEA the
+ * front-0 indices of the last finalize. */
+moea_status moea_selector_result_indices(moea_selector* s, const int** d_indices, int* count);
+moea_status moea_selector_reset(moea_selector* s, void* stream);
+void moea_selector_destroy(moea_selector* s);
 
 /* ========================================================================
  * Algorithm (the NSGA3 / RVEA entry points, Algorithm / AlgorithmBuilder).

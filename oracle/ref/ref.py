@@ -299,3 +299,29 @@ def algo_time(algorithm, problem_kind, D, M, N, partitions, max_gen, sparse_rati
     if rc != 0:
         raise RuntimeError(f"reference algorithm failed ({rc}): {err.value.decode(errors='replace')}")
     return [ms[i] for i in range(steps)]
+
+
+def algo_run(algorithm, problem_kind, D, M, N, max_gen, seed, sbx_eta, copy_prob, init, dirs=None, frequency=0.1):
+    """One run of the reference's own algorithm (see ref_algo_run): final
+    objectives (M, N), active count and its RunResult.total_ms."""
+    L = ctypes.CDLL(str(ALGO_LIB_PATH))
+    fp = ctypes.POINTER(c_float)
+    L.ref_algo_run.restype = c_int
+    L.ref_algo_run.argtypes = [c_int, c_int, c_int, c_int, c_int, c_int, ctypes.c_ulonglong, c_float, c_float, fp,
+                               fp, c_int, c_float, fp, ctypes.POINTER(c_int), ctypes.POINTER(ctypes.c_double),
+                               ctypes.c_char_p, ctypes.c_size_t]
+    init = np.ascontiguousarray(init, np.float32)
+    objs = np.zeros((M, N), np.float32)
+    act, ms = c_int(0), ctypes.c_double(0.0)
+    err = ctypes.create_string_buffer(512)
+    H = 0
+    dptr = None
+    if dirs is not None:
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        H = dirs.shape[1]
+        dptr = dirs.ctypes.data_as(fp)
+    rc = L.ref_algo_run(algorithm, problem_kind, D, M, N, max_gen, seed, sbx_eta, copy_prob, init.ctypes.data_as(fp),
+                        dptr, H, frequency, objs.ctypes.data_as(fp), ctypes.byref(act), ctypes.byref(ms), err, 512)
+    if rc != 0:
+        raise RuntimeError(f"reference algorithm failed ({rc}): {err.value.decode(errors='replace')}")
+    return objs, act.value, ms.value

@@ -22,6 +22,9 @@
 
 #include "cuda_moea/algorithms/nsga3.cuh"
 #include "cuda_moea/algorithms/rvea.cuh"
+#include "cuda_moea/factory/algorithm_factory.cuh"
+#include "cuda_moea/factory/operator_factory.cuh"
+#include "cuda_moea/factory/problem_factory.cuh"
 
 using namespace cuda_moea;
 
@@ -67,6 +70,51 @@ extern "C" int ref_algo_time(int algorithm, int problem_kind, int D, int M, int 
             std::snprintf(err, err_cap, "CUDA: %s", cudaGetErrorString(e));
             return 2;
         }
+        return 0;
+    } catch (const std::exception& ex) {
+        std::snprintf(err, err_cap, "%s", ex.what());
+        return 1;
+    }
+}
+
+// A whole run of the reference's algorithm the way its published quality
+// benchmark configures it (tests/benchmark/adapters/dtlz.py _run_cuda): a given
+// initial population (N, D) row-major, SBX {eta, eta, 1, copy_prob}, PM
+// {20, 20, 1}, NSGA-III with sparse ratio 1 and the given user directions
+// (M, H) objective-major (normalised by the provider), RVEA with alpha 2 and
+// adaptive directions of the given frequency.  After max_gen generations the
+// final objectives (M, N) objective-major, the active count and the run's own
+// device time (RunResult.total_ms) are returned.
+extern "C" int ref_algo_run(int algorithm, int problem_kind, int D, int M, int N, int max_gen,
+                            unsigned long long seed, float sbx_eta, float copy_prob, const float* h_init,
+                            const float* h_dirs, int H, float frequency, float* h_objs, int* h_active,
+                            double* h_total_ms, char* err, size_t err_cap)
+{
+    try {
+        auto st = AlgorithmFactory::defaults(algorithm == 0 ? AlgorithmKind::NSGA3 : AlgorithmKind::RVEA);
+        st.config.population_size = N;
+        st.config.max_generations = max_gen;
+        st.config.print_progress = false;
+        st.config.cuda.seed = seed;
+        st.config.cuda.enable_warmup = false;
+        if (h_init) st.config.initial_population.assign(h_init, h_init + (size_t)N * D);
+        st.strategies.problem = ProblemFactory::create(static_cast<ProblemKind>(problem_kind - 1), D, M, 0.0f);
+        st.strategies.crossover = OperatorFactory::crossover(CrossoverKind::SBX, SBXConfig{sbx_eta, sbx_eta, 1.0f, copy_prob});
+        st.strategies.mutation = OperatorFactory::mutation(MutationKind::Polynomial, PolynomialMutationConfig{20.0f, 20.0f, 1.0f});
+        if (algorithm == 0) {
+            st.strategies.environment_selector = std::make_unique<NSGA3EnvironmentSelector>(NSGA3SelectionConfig{1.0f, {}});
+            if (h_dirs)
+                st.strategies.reference_directions = std::make_unique<UserDefinedDirections>(
+                    std::vector<float>(h_dirs, h_dirs + (size_t)M * H), M, true);
+        } else {
+            st.strategies.environment_selector = std::make_unique<RVEAEnvironmentSelector>(RVEASelectionConfig{2.0f});
+            st.strategies.reference_directions = std::make_unique<AdaptiveRVEADirections>(AdaptiveDirectionConfig{frequency});
+        }
+        Algorithm a = AlgorithmFactory::create(std::move(st));
+        RunResult r = a.run();
+        std::memcpy(h_objs, r.objectives.data(), sizeof(float) * (size_t)M * N);
+        *h_active = r.active_count;
+        *h_total_ms = r.total_ms;
         return 0;
     } catch (const std::exception& ex) {
         std::snprintf(err, err_cap, "%s", ex.what());

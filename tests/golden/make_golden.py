@@ -94,6 +94,49 @@ def main(out: str) -> None:
     g.update({"rvea_objs": objs, "rvea_cv": cv, "rvea_refs": refs, "rvea_t": t, "rvea_z": z,
               "rvea_theta": th, "rvea_idx": idx, "rvea_gamma": gam, "rvea_apd": apd,
               "rvea_sel": sel, "rvea_active": np.int32(act)})
+    # ---- reproduction: tournament, SBX, PM on explicit draws
+    n, D = 65, 9
+    parents = rng.random((n, D)).astype(np.float32)
+    bounds = np.tile([0.0, 1.0], D).astype(np.float32)
+    pcv = np.where(rng.random(n) < 0.3, rng.integers(0, 4, n) * 0.5, 0).astype(np.float32)
+    rank = rng.integers(0, 4, n).astype(np.int32)
+    cand = rng.integers(0, n, (n, 2)).astype(np.int32)
+    win = R.tournament(cand, rank, pcv)
+    pairs = n // 2
+    u = rng.random((pairs * D, 2)).astype(np.float32)
+    sign = rng.integers(0, 2, pairs * D).astype(np.int32)
+    copy = rng.random(pairs * D).astype(np.float32)
+    off = R.sbx(parents, win, bounds, u, sign, copy, 15.0, 0.9, 0.3, n)
+    um = rng.random((n * D, 2)).astype(np.float32)
+    um[:, 0] *= 2.0 / D
+    mut = R.pm(off, bounds, um, 20.0, 1.0)
+    g.update({"rep_parents": parents, "rep_bounds": bounds, "rep_cv": pcv, "rep_rank": rank, "rep_cand": cand,
+              "rep_winners": win, "rep_u": u, "rep_sign": sign, "rep_copy": copy, "rep_sbx": off, "rep_um": um,
+              "rep_pm": mut, "rep_annealed": np.array([R.annealed(5.0, 40.0, 37, 100),
+                                                       R.annealed(20.0, 3.0, 150, 100)], np.float32)})
+    # ---- CV quantisation (linear and log mapping)
+    qcv = (rng.random(400) * 3).astype(np.float32)
+    qcv[:50] = 0.0
+    qcv[50:53] = np.nan
+    g.update({"quant_cv": qcv, "quant_lin": R.quantize_cv(qcv, 0.0, 2.0, 0.0, 16),
+              "quant_log": R.quantize_cv(qcv, 1e-3, 2.5, 3.0, 64)})
+    # ---- RVEA direction adaptation and survivor update with sentinels
+    M, N, active = 5, 120, 100
+    v0 = O.reference_directions(2, N, M)
+    aobjs = (rng.random((M, N)) * rng.random(M)[:, None] * 3).astype(np.float32)
+    aobjs[:, active:] = 1e15
+    g.update({"adapt_v0": v0, "adapt_objs": aobjs, "adapt_active": np.int32(active),
+              "adapt_out": R.rvea_adapt(v0, aobjs, active)})
+    import torch
+    D = 6
+    px, ox = rng.random((N, D)).astype(np.float32), rng.random((N, D)).astype(np.float32)
+    pf, of = rng.random((M, N)).astype(np.float32), rng.random((M, N)).astype(np.float32)
+    pc, oc = rng.random(N).astype(np.float32), rng.random(N).astype(np.float32)
+    usel = rng.permutation(2 * N)[:active].astype(np.int32)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    nx, nf, nc = R.rvea_update_t(t(px), t(ox), t(pf), t(of), t(pc), t(oc), t(usel), active)
+    g.update({"upd_px": px, "upd_ox": ox, "upd_pf": pf, "upd_of": of, "upd_pc": pc, "upd_oc": oc,
+              "upd_sel": usel, "upd_x": nx.cpu().numpy(), "upd_f": nf.cpu().numpy(), "upd_cv": nc.cpu().numpy()})
     np.savez_compressed(out, **g)
     print("wrote", out, len(g), "arrays")
 

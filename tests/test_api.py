@@ -20,9 +20,25 @@ class Mating(cm.PythonMating):
                             dtype=torch.int32)
 
 
+class Crossover(cm.PythonCrossover):
+    def apply(self, parents, parent_indices, context):
+        return parents["variables"][parent_indices.long()]
+
+
+class Mutation(cm.PythonMutation):
+    def mutate(self, offspring, context):
+        return offspring["variables"]
+
+
 class References(cm.PythonReferenceDirections):
     def initialize(self, requested_count, objective_count, context):
         return torch.eye(objective_count)
+
+
+class Selector(cm.PythonEnvironmentSelector):
+    def select(self, parents, offspring, context):
+        size = parents["variables"].shape[0]
+        return {"indices": torch.arange(size, device=parents["variables"].device)}
 
 
 def test_sbx_variable_copy_probability():
@@ -67,7 +83,8 @@ def test_all_builtin_strategies_construct():
 
 def test_custom_strategies_construct():
     algorithm = cm.NSGA3(population_size=16, max_generations=1, problem=Sphere(), mating=Mating(),
-                         reference_directions=References(), enable_warmup=False)
+                         crossover=Crossover(), mutation=Mutation(), reference_directions=References(),
+                         environment_selector=Selector(), enable_warmup=False)
     assert not algorithm.initialized
 
 

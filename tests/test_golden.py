@@ -8,7 +8,11 @@ normalised input (this also pins the fused multiply-add form of the
 reference's distance), niching selection and RNG offset, RVEA translation,
 APD on the same angles, elitism.  Tolerances: intercepts (the reference's
 FP32 cuSOLVER SVD against the oracle's FP64 solve), problem objectives and
-RVEA angles (CUDA cosf/sinf/powf/rsqrtf/acosf against the host libm).
+RVEA angles (CUDA cosf/sinf/powf/rsqrtf/acosf against the host libm), SBX
+and PM values (CUDA powf), the log CV mapping (log1pf) and the adapted
+directions (rsqrtf).  Exact too: tournament winners, the annealed
+distribution index, the linear CV quantisation and the RVEA survivor update
+with its dead-slot sentinels.
 """
 from pathlib import Path
 
@@ -88,3 +92,46 @@ def test_rvea_golden(g, oracle):
     sel, act = oracle.rvea_elitism(g["rvea_idx"], g["rvea_cv"], g["rvea_apd"], 150, g["rvea_refs"].shape[1])
     assert act == int(g["rvea_active"])
     np.testing.assert_array_equal(sel, g["rvea_sel"])
+
+
+def _has(g, key):
+    if key not in g:
+        pytest.skip("golden vectors predate this case")
+
+
+def test_reproduction_golden(g, oracle):
+    _has(g, "rep_winners")
+    np.testing.assert_array_equal(oracle.tournament(g["rep_cand"], g["rep_rank"], g["rep_cv"]), g["rep_winners"])
+    n = g["rep_parents"].shape[0]
+    off = oracle.sbx(g["rep_parents"], g["rep_winners"], g["rep_bounds"], g["rep_u"], g["rep_sign"],
+                     g["rep_copy"], 15.0, 0.9, 0.3, n)
+    np.testing.assert_allclose(off, g["rep_sbx"], rtol=2e-6, atol=2e-7)
+    mut = oracle.pm(g["rep_sbx"], g["rep_bounds"], g["rep_um"], 20.0, 1.0)
+    np.testing.assert_allclose(mut, g["rep_pm"], rtol=5e-6, atol=5e-7)
+    assert np.float32(oracle.annealed(5.0, 40.0, 37, 100)) == g["rep_annealed"][0]
+    assert np.float32(oracle.annealed(20.0, 3.0, 150, 100)) == g["rep_annealed"][1]
+
+
+def test_quantize_golden(g, oracle):
+    _has(g, "quant_cv")
+    np.testing.assert_array_equal(oracle.quantize_cv(g["quant_cv"], 0.0, 2.0, 0.0, 16), g["quant_lin"])
+    assert (oracle.quantize_cv(g["quant_cv"], 1e-3, 2.5, 3.0, 64) != g["quant_log"]).mean() < 1e-2
+
+
+def test_rvea_adapt_and_update_golden(g, oracle):
+    _has(g, "adapt_out")
+    np.testing.assert_allclose(oracle.rvea_adapt(g["adapt_v0"], g["adapt_objs"], int(g["adapt_active"])),
+                               g["adapt_out"], rtol=3e-6, atol=3e-7)
+    # survivor update (rvea_population_update.cu:263-300): the selected rows in
+    # ascending order, then NaN variables and 1e15 objectives/violations
+    sel = np.sort(g["upd_sel"])
+    act, N = len(sel), g["upd_px"].shape[0]
+    x = np.concatenate([g["upd_px"], g["upd_ox"]])[sel]
+    f = np.concatenate([g["upd_pf"], g["upd_of"]], 1)[:, sel]
+    cv = np.concatenate([g["upd_pc"], g["upd_oc"]])[sel]
+    np.testing.assert_array_equal(g["upd_x"][:act], x)
+    assert np.isnan(g["upd_x"][act:]).all()
+    np.testing.assert_array_equal(g["upd_f"][:, :act], f)
+    assert (g["upd_f"][:, act:] == np.float32(1e15)).all()
+    np.testing.assert_array_equal(g["upd_cv"][:act], cv)
+    assert (g["upd_cv"][act:] == np.float32(1e15)).all() and act < N

@@ -49,3 +49,23 @@ def test_igd_rejects_all_nonfinite():
     from cuda_moea._lib import MoeaError
     with pytest.raises(MoeaError):
         metrics.igd(torch.full((5, 3), float("nan")), torch.rand(4, 3, dtype=torch.float64))
+
+
+def test_igd_equals_reference_metric_on_golden_cases():
+    """moea_igd against the reference's own igd() (tests/evaluation/metrics/
+    igd.py:23-47), whose values on seeded approximations are recorded in
+    tests/golden/quality_reference.json: non-finite rows dropped, with and
+    without the non-dominated filter, FP64 (relative tolerance 1e-12)."""
+    import json
+    import sys
+    from pathlib import Path
+    from cuda_moea import metrics
+    golden_dir = Path(__file__).resolve().parent / "golden"
+    sys.path.insert(0, str(golden_dir))
+    from quality_inputs import approximation
+    cases = json.loads((golden_dir / "quality_reference.json").read_text())["igd"]
+    for c in cases:
+        x = torch.from_numpy(approximation(c["seed"], c["n"], c["objectives"])).cuda()
+        ref = metrics.pareto_front_points("DTLZ2", c["objectives"], c["front_count"], 2887).to(torch.float64)
+        got = metrics.igd(x, ref, filter_nondominated=c["filter_nondominated"])
+        assert abs(got - c["igd"]) <= 1e-12 * abs(c["igd"]), (c, got)
