@@ -358,12 +358,14 @@ def shard_instances(specs, world: int, rank: int):
 
 
 def batched_measure(args, torch, cm, world: int = 1, rank: int = 0):
-    """Instance-generations/s of the batch (one graph launch per generation)
-    against the same instances looped one after another through the plain
-    path on one stream; both advance the same generations, after which every
-    instance's front indices and objectives are compared.  With several
-    ranks the instances are sharded (shard_instances) and the job's rate is
-    all instances over the slowest rank's time."""
+    """Instance-generations/s of the batch (one graph launch per generation,
+    schedule chosen by the library's autotuner) against the same instances
+    looped one after another through the plain path on one stream, both over
+    the whole 200-generation run (every generation timed with CUDA events),
+    with the rates of three windows (early, middle, late) beside it.  After
+    the run every instance's front indices and objectives are compared.  With
+    several ranks the instances are sharded (shard_instances) and the job's
+    rate is all instances over the slowest rank's time."""
     all_specs = batch_specs(args.batch_instances)
     specs = [all_specs[i] for i in shard_instances(all_specs, world, rank)]
     T = 200
@@ -373,50 +375,58 @@ def batched_measure(args, torch, cm, world: int = 1, rank: int = 0):
         return cm.NSGA3(population_size=N, max_generations=T, problem=getattr(cm, f"DTLZ{kind}")(D, M),
                         seed=seed, print_progress=False)
 
-    warm, K = 2, args.batch_steps
-    batch = cm.Batch([make(s) for s in specs])
-    batch.run(warm)
+    def timed_run(step, stream):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(T)]
+        for e0, e1 in ev:
+            e0.record(stream)
+            step()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        return [e0.elapsed_time(e1) for e0, e1 in ev]
+
+    t0 = time.perf_counter()
+    batch = cm.Batch([make(s) for s in specs], autotune=True)
+    tune_s = time.perf_counter() - t0
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(batch.stream)
-    for _ in range(K):
-        batch.step()
-    e1.record(batch.stream)
-    torch.cuda.synchronize()
-    batch_ms = e0.elapsed_time(e1)
+    batch_ms = timed_run(batch.step, batch.stream)
 
     shared = torch.cuda.Stream()
     with torch.cuda.stream(shared):
         plain = [make(s) for s in specs]
         for a in plain:
             a.initialize()
-        for _ in range(warm):
+        torch.cuda.synchronize()
+
+        def plain_step():
             for a in plain:
                 a.step()
-        torch.cuda.synchronize()
-        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        p0.record(shared)
-        for _ in range(K):
-            for a in plain:
-                a.step()
-        p1.record(shared)
-        torch.cuda.synchronize()
-    plain_ms = p0.elapsed_time(p1)
+        plain_ms = timed_run(plain_step, shared)
     identical = True
     for i, a in enumerate(plain):
         r_b, r_p = batch.result(i), a.result()
         identical &= bool(torch.equal(r_b.auxiliary_indices, r_p.auxiliary_indices))
         identical &= bool(torch.equal(r_b.objectives, r_p.objectives))
-    batch_ms = over_ranks(batch_ms, "max", world, "cuda")
-    plain_ms = over_ranks(plain_ms, "max", world, "cuda")
     identical = over_ranks(0.0 if identical else 1.0, "max", world, "cuda") == 0.0
     n = len(all_specs)
-    out = {"workload": BATCH_WORKLOAD, "instances": n, "generations_timed": K,
-           "instance_gen_per_s": n * K / (batch_ms / 1e3),
-           "plain_loop_instance_gen_per_s": n * K / (plain_ms / 1e3),
-           "speedup_vs_plain_loop": plain_ms / batch_ms,
+    windows = {}
+    for name, (lo, hi) in (("generations 1-5", (0, 5)), ("generations 96-100", (95, 100)),
+                           ("generations 196-200", (195, 200))):
+        b = over_ranks(sum(batch_ms[lo:hi]), "max", world, "cuda")
+        p = over_ranks(sum(plain_ms[lo:hi]), "max", world, "cuda")
+        windows[name] = {"instance_gen_per_s": n * (hi - lo) / (b / 1e3),
+                         "plain_loop_instance_gen_per_s": n * (hi - lo) / (p / 1e3), "speedup": p / b}
+    b_total = over_ranks(sum(batch_ms), "max", world, "cuda")
+    p_total = over_ranks(sum(plain_ms), "max", world, "cuda")
+    sched = batch.schedule
+    out = {"workload": BATCH_WORKLOAD, "instances": n, "span": f"all {T} generations, each timed",
+           "instance_gen_per_s": n * T / (b_total / 1e3),
+           "plain_loop_instance_gen_per_s": n * T / (p_total / 1e3),
+           "speedup_vs_plain_loop": p_total / b_total, "windows": windows,
            "identical_ranks": identical, "fused": batch.fused,
            "graph_kernels_per_generation": batch.graph_kernels,
+           "schedule": {"groups": sched["groups"], "source": sched["source"], "tuned_ms": sched["tuned_ms"],
+                        "default_ms": sched["default_ms"], "slowest_instance_ms": sched["slowest_instance_ms"],
+                        "instances_serial_ms": sched["instances_serial_ms"], "tuning_and_setup_s": tune_s},
            "pair_tests_per_generation": sum((2 * s[2]) ** 2 for s in all_specs),
            "sharding": f"{world} rank(s), instances balanced by pair tests"}
     batch.close()
@@ -671,7 +681,6 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=40.0)
     ap.add_argument("--batch-instances", type=int, default=256)
-    ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the association-search comparison")
     ap.add_argument("--workload", default="dtlz1-n32768",

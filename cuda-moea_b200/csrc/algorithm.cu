@@ -16,8 +16,11 @@
 //    allocation, dynamic_workspace.cu:3-125).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -1209,6 +1212,13 @@ struct moea_batch {
     bool use_fused = true;
     cudaGraphExec_t graph[2] = {};
     int graph_kernels = 0;
+    // the schedule: group of each instance (fused mode), and how it was chosen
+    std::vector<int> group_of;
+    int schedule_source = 0;    // 0 pair-test LPT, 1 autotuned now, 2 autotuned earlier (cache)
+    float tuned_ms = 0.0f;      // measured generation of the chosen schedule (autotuner)
+    float default_ms = 0.0f;    // measured generation of the default schedule (autotuner)
+    float slowest_ms = 0.0f;    // the slowest instance's generation run alone (autotuner probe)
+    float serial_ms = 0.0f;     // all instances' generations run alone one after another
 
     ~moea_batch()
     {
@@ -1227,12 +1237,16 @@ struct moea_batch {
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 
-    int setup_fused()
+    bool fused_possible() const
     {
         for (moea_algorithm* a : inst)
-            if (!fused_eligible(a)) return MOEA_OK;
-        for (moea_algorithm* a : inst)
-            if (a->P != 0 || a->X != 2) return MOEA_OK;
+            if (!fused_eligible(a) || a->P != 0 || a->X != 2) return false;
+        return true;
+    }
+
+    int setup_fused(const std::vector<int>* schedule = nullptr)
+    {
+        if (!fused_possible()) return MOEA_OK;
         MOEA_TRY(fused_ndsort_configure());
         MOEA_TRY(fused_select_configure());
         const int count = (int)inst.size();
@@ -1242,25 +1256,62 @@ struct moea_batch {
             MOEA_CUDA_TRY(cudaMalloc((void**)&d_inst[parity], sizeof(BatchInst) * count));
             MOEA_CUDA_TRY(cudaMemcpy(d_inst[parity], h.data(), sizeof(BatchInst) * count, cudaMemcpyHostToDevice));
         }
-        // groups: longest-processing-time assignment by the pair tests of one
-        // generation, (2N)^2, so that every group carries a similar share
-        const int G = std::max(1, std::min(fused_groups, count));
-        std::vector<int> order(count);
+        fused = true;
+        if (schedule) return build_groups(*schedule);
+        // default: longest-processing-time assignment by the pair tests of
+        // one generation, (2N)^2, so that every group carries a similar share
+        std::vector<double> cost(count);
+        for (int i = 0; i < count; ++i) cost[i] = (double)inst[i]->N * inst[i]->N;
+        return build_groups(lpt(cost, std::max(1, std::min(fused_groups, count))));
+    }
+
+    // Longest-processing-time assignment of the instances to G groups.
+    static std::vector<int> lpt(const std::vector<double>& cost, int G)
+    {
+        const int count = (int)cost.size();
+        std::vector<int> order(count), group(count, 0);
         for (int i = 0; i < count; ++i) order[i] = i;
         std::sort(order.begin(), order.end(), [&](int x, int y) {
-            const double cx = (double)inst[x]->N * inst[x]->N, cy = (double)inst[y]->N * inst[y]->N;
-            return cx > cy || (cx == cy && x < y);
+            return cost[x] > cost[y] || (cost[x] == cost[y] && x < y);
         });
-        std::vector<std::vector<int>> members(G);
         std::vector<double> load(G, 0.0);
         for (int i : order) {
             const int g = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-            members[g].push_back(i);
-            load[g] += (double)inst[i]->N * inst[i]->N;
+            group[i] = g;
+            load[g] += cost[i];
         }
+        return group;
+    }
+
+    void free_groups()
+    {
+        drop_graphs();
+        for (auto& g : groups) fused_free_group(g);
+        for (cudaStream_t gs : gstream) cudaStreamDestroy(gs);
+        for (cudaEvent_t e : gjoin) cudaEventDestroy(e);
+        groups.clear();
+        gstream.clear();
+        gjoin.clear();
+    }
+
+    void drop_graphs()
+    {
+        for (auto& g : graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+
+    // One fused group per value of group_of (instance -> group); each group's
+    // chain of kernels is one branch of the generation's graph.
+    int build_groups(const std::vector<int>& schedule)
+    {
+        free_groups();
+        group_of = schedule;
+        const int G = schedule.empty() ? 0 : *std::max_element(schedule.begin(), schedule.end()) + 1;
         for (int gi = 0; gi < G; ++gi) {
-            std::vector<int>& ids = members[gi];
-            std::sort(ids.begin(), ids.end());
+            std::vector<int> ids;
+            for (int i = 0; i < (int)schedule.size(); ++i)
+                if (schedule[i] == gi) ids.push_back(i);
+            if (ids.empty()) continue;
             FusedGroup g;
             MOEA_TRY(fused_build_group(inst, ids, g));
             groups.push_back(std::move(g));
@@ -1271,7 +1322,107 @@ struct moea_batch {
             MOEA_CUDA_TRY(cudaEventCreateWithFlags(&ge, cudaEventDisableTiming));
             gjoin.push_back(ge);
         }
-        fused = true;
+        return MOEA_OK;
+    }
+
+    // ---- autotuner (runs on a scratch copy of a batch: it advances and
+    // re-runs that copy's generations freely) ----
+
+    // Device time of each instance's fused generation run alone (one group of
+    // one instance, direct launches), at the current parity.  The outputs go
+    // to the next-population slots and are discarded.
+    int probe_costs(std::vector<double>& cost)
+    {
+        const int count = (int)inst.size();
+        const int parity = (inst[0]->P == 0) ? 0 : 1;
+        cost.assign(count, 0.0);
+        cudaEvent_t e0, e1;
+        MOEA_CUDA_TRY(cudaEventCreate(&e0));
+        MOEA_CUDA_TRY(cudaEventCreate(&e1));
+        int st = MOEA_OK;
+        for (int i = 0; i < count && st == MOEA_OK; ++i) {
+            FusedGroup g;
+            st = fused_build_group(inst, std::vector<int>{i}, g);
+            if (st != MOEA_OK) break;
+            cudaEventRecord(e0, stream);
+            st = fused_reproduce(d_inst[parity], g, stream);
+            if (st == MOEA_OK) st = fused_evaluate(d_inst[parity], g, stream);
+            if (st == MOEA_OK) st = fused_ndsort(d_inst[parity], g, stream);
+            if (st == MOEA_OK) st = fused_select(d_inst[parity], g, stream);
+            cudaEventRecord(e1, stream);
+            cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            cost[i] = ms;
+            fused_free_group(g);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (st == MOEA_OK) MOEA_CUDA_TRY(cudaGetLastError());
+        return st;
+    }
+
+    // Best of `reps` replays of the captured generation of a schedule (the
+    // same parents each time, so each replay is the same generation's work).
+    int time_schedule(const std::vector<int>& schedule, int reps, float* best_ms)
+    {
+        MOEA_TRY(build_groups(schedule));
+        const int parity = (inst[0]->P == 0) ? 0 : 1;
+        cudaGraphExec_t g = nullptr;
+        MOEA_TRY(capture(&g, parity));
+        cudaEvent_t e0, e1;
+        MOEA_CUDA_TRY(cudaEventCreate(&e0));
+        MOEA_CUDA_TRY(cudaEventCreate(&e1));
+        float best = 1e30f;
+        cudaGraphLaunch(g, stream);  // warm
+        for (int r = 0; r < reps; ++r) {
+            cudaEventRecord(e0, stream);
+            cudaGraphLaunch(g, stream);
+            cudaEventRecord(e1, stream);
+            cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            best = std::min(best, ms);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaGraphExecDestroy(g);
+        MOEA_CUDA_TRY(cudaGetLastError());
+        *best_ms = best;
+        return MOEA_OK;
+    }
+
+    // Runs `warm` generations, measures every instance alone, then times the
+    // pair-test LPT schedule of the default group count and measured-cost LPT
+    // schedules of 4..count groups; *chosen receives the fastest.
+    int autotune(int warm, std::vector<int>* chosen, float* chosen_ms, float* dflt_ms, float* slowest,
+                 float* serial)
+    {
+        const int count = (int)inst.size();
+        for (int g = 0; g < warm && generation < T - 1; ++g) MOEA_TRY(step());
+        std::vector<double> measured;
+        MOEA_TRY(probe_costs(measured));
+        *slowest = (float)*std::max_element(measured.begin(), measured.end());
+        double total = 0.0;
+        for (double c : measured) total += c;
+        *serial = (float)total;
+        std::vector<double> pairs(count);
+        for (int i = 0; i < count; ++i) pairs[i] = (double)inst[i]->N * inst[i]->N;
+        std::vector<std::vector<int>> cands;
+        cands.push_back(lpt(pairs, std::max(1, std::min(fused_groups, count))));
+        for (int G = 4; G <= count; G *= 2) cands.push_back(lpt(measured, G));
+        if ((count & (count - 1)) != 0) cands.push_back(lpt(measured, count));
+        float best = 1e30f;
+        for (size_t c = 0; c < cands.size(); ++c) {
+            float ms = 0.0f;
+            MOEA_TRY(time_schedule(cands[c], 3, &ms));
+            if (c == 0) *dflt_ms = ms;
+            if (ms < best) {
+                best = ms;
+                *chosen = cands[c];
+            }
+        }
+        *chosen_ms = best;
         return MOEA_OK;
     }
 
@@ -1353,6 +1504,46 @@ struct moea_batch {
     }
 };
 
+namespace {
+
+struct TunedSchedule {
+    std::vector<int> schedule;
+    float tuned_ms = 0.0f, default_ms = 0.0f, slowest_ms = 0.0f, serial_ms = 0.0f;
+};
+
+std::map<std::string, TunedSchedule>& tuning_cache()
+{
+    static std::map<std::string, TunedSchedule> cache;
+    return cache;
+}
+
+std::mutex& tuning_mutex()
+{
+    static std::mutex m;
+    return m;
+}
+
+// The instance mix a schedule is tuned for: the device and, per instance in
+// order, everything that sets its work (problem, sizes, directions, operators).
+std::string batch_signature(const moea_algorithm_config* cfgs, int count)
+{
+    std::string key;
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, cfgs[0].device) == cudaSuccess) key += prop.name;
+    key += "|" + std::to_string(count) + "|" + std::to_string(cfgs[0].max_generations);
+    for (int i = 0; i < count; ++i) {
+        const moea_algorithm_config& c = cfgs[i];
+        char buf[256];
+        std::snprintf(buf, sizeof(buf), "|%d,%d,%d,%d,%d,%d,%d,%d,%g,%g,%d,%d", c.algorithm, c.problem_kind,
+                      c.population_size, c.dimension, c.objectives, c.directions, c.partitions, c.mating,
+                      (double)c.sbx_probability, (double)c.sbx_copy_probability, c.mutation, c.association_mode);
+        key += buf;
+    }
+    return key;
+}
+
+}  // namespace
+
 extern "C" {
 
 moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void* stream, int flags,
@@ -1417,12 +1608,62 @@ moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void
         cudaGetLastError();
         st = set_error(MOEA_ERR_CUDA, "batch: %s", cudaGetErrorString(ce));
     }
-    if (st == MOEA_OK && b->use_fused) st = b->setup_fused();
+    const bool groups_given = ((flags >> 8) & 0xFF) > 0;
+    if (st == MOEA_OK && b->use_fused && (flags & MOEA_BATCH_AUTOTUNE) && !groups_given && b->fused_possible()) {
+        // the schedule of this instance mix: from the cache, or tuned now on a
+        // scratch copy of the batch (same configurations, so the same work)
+        const std::string key = batch_signature(cfgs, count);
+        std::lock_guard<std::mutex> lock(tuning_mutex());
+        auto it = tuning_cache().find(key);
+        if (it != tuning_cache().end()) {
+            st = b->setup_fused(&it->second.schedule);
+            b->schedule_source = 2;
+            b->tuned_ms = it->second.tuned_ms;
+            b->default_ms = it->second.default_ms;
+            b->slowest_ms = it->second.slowest_ms;
+            b->serial_ms = it->second.serial_ms;
+        } else {
+            moea_batch* scratch = nullptr;
+            st = moea_batch_create(cfgs, count, nullptr, flags & ~MOEA_BATCH_AUTOTUNE, &scratch);
+            TunedSchedule ts;
+            if (st == MOEA_OK) {
+                st = scratch->autotune(std::min(10, T / 4), &ts.schedule, &ts.tuned_ms, &ts.default_ms,
+                                       &ts.slowest_ms, &ts.serial_ms);
+                delete scratch;
+            }
+            if (st == MOEA_OK) {
+                tuning_cache()[key] = ts;
+                st = b->setup_fused(&ts.schedule);
+                b->schedule_source = 1;
+                b->tuned_ms = ts.tuned_ms;
+                b->default_ms = ts.default_ms;
+                b->slowest_ms = ts.slowest_ms;
+                b->serial_ms = ts.serial_ms;
+            }
+        }
+    } else if (st == MOEA_OK && b->use_fused) {
+        st = b->setup_fused();
+    }
     if (st != MOEA_OK) {
         delete b;
         return st;
     }
     *out = b;
+    return MOEA_OK;
+}
+
+moea_status moea_batch_schedule(moea_batch* b, int* h_groups, int* h_source, float* h_tuned_ms,
+                                float* h_default_ms, float* h_slowest_ms, float* h_serial_ms, int* h_group_of)
+{
+    if (!b) return set_error(MOEA_ERR_INVALID_ARGUMENT, "NULL batch");
+    if (h_slowest_ms) *h_slowest_ms = b->slowest_ms;
+    if (h_serial_ms) *h_serial_ms = b->serial_ms;
+    if (h_groups) *h_groups = (int)b->groups.size();
+    if (h_source) *h_source = b->schedule_source;
+    if (h_tuned_ms) *h_tuned_ms = b->tuned_ms;
+    if (h_default_ms) *h_default_ms = b->default_ms;
+    if (h_group_of)
+        for (size_t i = 0; i < b->inst.size(); ++i) h_group_of[i] = i < b->group_of.size() ? b->group_of[i] : -1;
     return MOEA_OK;
 }
 

@@ -21,7 +21,12 @@ class Batch:
     """Advance ``algorithms`` (not yet initialised, built-in problems and
     mating, same device and max_generations) as one batch."""
 
-    def __init__(self, algorithms: Sequence[Algorithm], *, fuse: bool = True, groups: int = 0):
+    def __init__(self, algorithms: Sequence[Algorithm], *, fuse: bool = True, groups: int = 0,
+                 autotune: bool = False):
+        """``groups`` fixes the number of graph branches of the fused
+        generation; ``autotune`` lets the library choose the schedule by
+        timing candidates on a scratch copy of the batch (MOEA_BATCH_AUTOTUNE;
+        cached per instance mix).  Results never depend on either."""
         if not algorithms:
             raise ValueError("Batch needs at least one algorithm")
         n = len(algorithms)
@@ -41,7 +46,7 @@ class Batch:
             self.stream = torch.cuda.Stream(self._device)
         handle = ctypes.c_void_p()
         # MOEA_BATCH_NO_FUSION = 1; MOEA_BATCH_GROUPS(g) = g << 8 (0: library default)
-        flags = (0 if fuse else 1) | ((int(groups) & 0xFF) << 8)
+        flags = (0 if fuse else 1) | ((int(groups) & 0xFF) << 8) | (2 if autotune else 0)
         check(lib().moea_batch_create(cfgs, n, ctypes.c_void_p(self.stream.cuda_stream), flags,
                                       ctypes.byref(handle)))
         self._handle = handle
@@ -97,6 +102,20 @@ class Batch:
     def graph_kernels(self) -> int:
         """Kernel nodes in one generation's graph (all instances)."""
         return self._info()[2]
+
+    @property
+    def schedule(self) -> dict:
+        """Groups of the fused generation and how they were chosen
+        ("default", "autotuned", "autotuned (cached)"), with the autotuner's
+        measured generation times of the chosen and the default schedule."""
+        g, src = ctypes.c_int(), ctypes.c_int()
+        t, d, slow, ser = ctypes.c_float(), ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        group_of = (ctypes.c_int * self._count)()
+        check(lib().moea_batch_schedule(self._handle, ctypes.byref(g), ctypes.byref(src), ctypes.byref(t),
+                                        ctypes.byref(d), ctypes.byref(slow), ctypes.byref(ser), group_of))
+        return {"groups": g.value, "source": ("default", "autotuned", "autotuned (cached)")[src.value],
+                "tuned_ms": t.value, "default_ms": d.value, "slowest_instance_ms": slow.value,
+                "instances_serial_ms": ser.value, "group_of": list(group_of)}
 
     def _view_struct(self, index: int) -> PopulationViewC:
         v = PopulationViewC()

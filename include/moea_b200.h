@@ -558,6 +558,14 @@ moea_status moea_algorithm_device_status(moea_algorithm* alg, int* h_status);
  * ====================================================================== */
 typedef struct moea_batch moea_batch;
 #define MOEA_BATCH_NO_FUSION 1
+/* Autotuned schedule (fused mode, unless MOEA_BATCH_GROUPS is given): a
+ * scratch copy of the batch runs min(10, max_generations/4) generations, times
+ * every instance's fused generation alone, then times the default schedule and
+ * longest-processing-time schedules on those measured costs for 4, 8, ...
+ * groups (graph branches); the fastest is used.  The choice is cached per
+ * device and instance mix for the life of the process.  Results do not depend
+ * on the schedule. */
+#define MOEA_BATCH_AUTOTUNE 2
 #define MOEA_BATCH_GROUPS(g) (((g) & 0xFF) << 8)
 moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void* stream, int flags,
                               moea_batch** out);
@@ -568,6 +576,16 @@ moea_status moea_batch_run(moea_batch* b, int generations, double* h_total_ms);
 moea_status moea_batch_synchronize(moea_batch* b);
 moea_status moea_batch_info(moea_batch* b, int* h_count, int* h_generation, int* h_graph_kernels,
                             int* h_fused);
+/* The batch's schedule: number of groups (graph branches of the fused
+ * generation; 0 when not fused), how it was chosen (0 the default pair-test
+ * assignment, 1 autotuned by this batch, 2 autotuned earlier for the same
+ * mix), the autotuner's measured generation time of the chosen and of the
+ * default schedule, of the slowest instance run alone and of all instances
+ * run alone one after another (ms; 0 when not tuned), and the group of each
+ * instance (h_group_of, count entries, may be NULL).  No counterpart in the
+ * reference. */
+moea_status moea_batch_schedule(moea_batch* b, int* h_groups, int* h_source, float* h_tuned_ms,
+                                float* h_default_ms, float* h_slowest_ms, float* h_serial_ms, int* h_group_of);
 /* Population view of instance `index` (same contract as moea_algorithm_view). */
 moea_status moea_batch_view(moea_batch* b, int index, moea_population_view* out);
 

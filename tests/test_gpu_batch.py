@@ -121,3 +121,27 @@ def test_fused_batch_equals_branch_batch(seed, n_hi):
             a, b = fused.result(i), branch.result(i)
             _same(a, b)
             np.testing.assert_array_equal(a.auxiliary_indices.cpu().numpy(), b.auxiliary_indices.cpu().numpy())
+
+
+def test_autotuned_batch_equals_instances_and_caches_its_schedule():
+    """The autotuned schedule (tuned on a scratch copy of the batch) changes
+    how the generation is launched, never what it computes; a second batch of
+    the same mix takes the cached schedule."""
+    T = 12
+    specs = _specs(40, 11)
+    batch = cm.Batch([_make(s, T) for s in specs], autotune=True)
+    sched = batch.schedule
+    assert batch.fused and sched["source"] == "autotuned"
+    assert sched["groups"] >= 1 and sched["tuned_ms"] > 0 and sched["default_ms"] > 0
+    assert sched["tuned_ms"] <= sched["default_ms"] * 1.0001
+    assert sorted(set(sched["group_of"])) == list(range(sched["groups"]))
+    batch.run()
+    again = cm.Batch([_make(s, T) for s in specs], autotune=True)
+    assert again.schedule["source"] == "autotuned (cached)"
+    assert again.schedule["group_of"] == sched["group_of"]
+    again.close()
+    for i in (0, 7, 19, 39):
+        r = _make(specs[i], T).run()
+        got = batch.result(i)
+        _same(got, r)
+        np.testing.assert_array_equal(got.auxiliary_indices.cpu().numpy(), r.auxiliary_indices.cpu().numpy())
