@@ -109,7 +109,7 @@ int workspace_init(Workspace& ws, int device, int n_max, int m_max, int h_max)
     A(ws.blocker, n); A(ws.front_sorted, n); A(ws.front_list, n);
     A(ws.chunk_keys, (size_t)(m_max > 1 ? m_max - 1 : 1) * ws.words * 32);
     A(ws.chunk_bits, (size_t)(m_max > 1 ? m_max - 1 : 1) * ws.words * 33);
-    A(ws.counters, 16);
+    A(ws.counters, 32);
     A(ws.fronts, n); A(ws.nds_gidx, n); A(ws.sizes, 8);
     A(ws.chunk_counts, 2 * (size_t)ceil_div(n_max, 1024) + 2);
     A(ws.nds_objs, n * (size_t)m_max);
@@ -129,7 +129,7 @@ int workspace_init(Workspace& ws, int device, int n_max, int m_max, int h_max)
         st = dalloc(ws, (char**)&ws.cub_tmp, ws.cub_bytes);
     }
     if (st == MOEA_OK) {
-        cudaError_t e = cudaMemset(ws.counters, 0, 16 * sizeof(int));
+        cudaError_t e = cudaMemset(ws.counters, 0, 32 * sizeof(int));
         if (e == cudaSuccess) e = cudaMemset(ws.offset_dev, 0, sizeof(unsigned long long));
         if (e != cudaSuccess) st = set_error(MOEA_ERR_CUDA, "cudaMemset: %s", cudaGetErrorString(e));
     }

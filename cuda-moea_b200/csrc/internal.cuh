@@ -76,8 +76,10 @@ struct Workspace {
     int* counters = nullptr;        // [0] feasible count, [1] list length (batched peel),
                                     // [2] max_front, [3] assigned, [4] grid-barrier arrivals,
                                     // [6] device status, [10] class-2 count, [11] class-3 count,
-                                    // [12] last feasible front, [13] long runs of equal sort keys
+                                    // [12] last feasible front, [13] long runs of equal sort keys,
+                                    // [16..19] two 64-bit barrier words carrying front sizes
     int peel_grid = 0;              // co-resident CTAs of the peel kernel
+    int peel_owned_grid = 0;        // CTAs of the lane-owned peel (one per SM), 0 if unavailable
     int peel_smem = 0;
     bool peel_single_cta = false;   // peel with one ordinary CTA (instances of a batch)
     uint32_t* peel_fmask = nullptr; // [3][words] members of the last three fronts (peel)

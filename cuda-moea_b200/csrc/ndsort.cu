@@ -843,6 +843,282 @@ nds_peel(const uint32_t* __restrict__ rows, int W, int n, int target, const int*
     peel_body<1>(blockIdx.x, gridDim.x, U, rows, W, n, target, qinfo, blocker, front_sorted, fmask, counters);
 }
 
+// ---- peel with lane-owned points ------------------------------------------
+//
+// When every warp of the grid owns at most one group of 32 positions
+// (n <= 32 * 32 * CTAs), a lane keeps its point's state across the fronts:
+// the blocker in a register and a window of kWin row words (the blocker's
+// word and those below it) in shared memory.  The window is refilled with
+// cp.async whenever the blocker moves to a lower word, so the copy lands
+// while the grid waits at the barrier and the next front's probe reads only
+// shared memory.  Rows the window cannot settle go through the CTA's
+// level-ordered scan as in peel_body.  The barrier carries the front sizes:
+// a CTA adds (1 << 32) + (its free points) to one of two 64-bit words (front
+// parity), so the front's size arrives with the barrier and no block-wide
+// count is needed.  A CTA can run at most one front ahead of the slowest, so
+// the word of front k holds only fronts k, k-2, ... when it is read.
+
+constexpr int kWin = 16;  // row words cached per lane below its blocker
+constexpr unsigned long long kPeelWaitNs = 2000000000ull;  // limit of one barrier wait
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void cp_async4(uint32_t* dst, const uint32_t* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Row words wt, wt-1, ..., wt-kWin+1 of `row` into a lane's window (stride
+// kPeelThreads); words below 0 read as empty.
+__device__ __forceinline__ void window_fill(uint32_t* win, const uint32_t* row, int wt)
+{
+#pragma unroll
+    for (int i = 0; i < kWin; ++i) {
+        const int w = wt - i;
+        if (w >= 0) cp_async4(win + i * kPeelThreads, row + w);
+        else win[i * kPeelThreads] = 0u;
+    }
+}
+
+// Arrival at a front barrier that also sums the fronts' sizes: adds
+// (1 << 32) + count to *word and waits until the high half reaches `need`.
+// Returns the word's value, or ~0 after `limit_ns` (status kDevBarrierTimeout)
+// or when another CTA has failed.  Thread 0 only.
+__device__ unsigned long long counted_arrive(unsigned long long* word, unsigned count, unsigned long long need,
+                                             int* status, unsigned long long limit_ns)
+{
+    const unsigned long long add = (1ull << 32) | count;
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(word), "l"(add) : "memory");
+    const unsigned long long t0 = global_ns();
+    for (;;) {
+        unsigned long long v;
+        asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(word) : "memory");
+        if ((v >> 32) >= need) return v;
+        if (*((volatile int*)status) != 0) return ~0ull;
+        if (global_ns() - t0 > limit_ns) {
+            atomicExch(status, kDevBarrierTimeout);
+            return ~0ull;
+        }
+        __nanosleep(32);
+    }
+}
+
+__global__ void __launch_bounds__(kPeelThreads, 1)
+nds_peel_owned(const uint32_t* __restrict__ rows, int W, int n, int target, const int* __restrict__ blocker0,
+               int* __restrict__ front_sorted, uint32_t* __restrict__ fmask, int* counters)
+{
+    extern __shared__ uint32_t smem[];
+    uint32_t* U = smem;                              // unassigned positions, one bit each
+    uint32_t* s_win = smem + ((W + 3) & ~3);         // [kWin][kPeelThreads] lane windows
+    __shared__ int s_nscan, s_ntask, s_cnt, s_ok, s_ck, s_total;
+    __shared__ int s_sq[kScanQueue], s_sw[kScanQueue], s_found[kScanQueue];
+    static_assert(kScanQueue >= kPeelThreads, "every owned point must fit the scan queue");
+    const int nblocks = gridDim.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    const int nf = min(n, counters[0]);
+    const int feasible = counters[0];
+    const bool feasible_only = feasible < target;
+    // feasible positions come first; infeasible ones never enter U (peel_body)
+    for (int w = threadIdx.x; w < W; w += blockDim.x) {
+        const int lo = w * 32;
+        U[w] = (lo + 32 <= nf) ? 0xFFFFFFFFu : (lo >= nf ? 0u : ((1u << (nf - lo)) - 1u));
+    }
+    if (threadIdx.x == 0) {
+        s_nscan = 0;
+        s_cnt = 0;
+    }
+    // this lane's point: group g = warp * nblocks + blockIdx.x (interleaved,
+    // like peel_body), at most one per warp
+    const int g = warp * nblocks + blockIdx.x;
+    const int q = g * 32 + lane;
+    bool alive = q < nf;
+    int b = -1, wtop = -1;
+    uint32_t* win = s_win + threadIdx.x;
+    const uint32_t* row = rows + (size_t)(alive ? q : 0) * W;
+    if (alive) {
+        b = blocker0[q];
+        if (b >= 0) {
+            wtop = b >> 5;
+            window_fill(win, row, wtop);
+        }
+    }
+    cp_async_commit();
+    __syncthreads();
+    if (feasible_only && feasible == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            counters[2] = -1;
+            counters[12] = -1;
+        }
+        cp_async_wait_all();
+        return;
+    }
+    unsigned long long* sizes = reinterpret_cast<unsigned long long*>(counters + 16);
+    unsigned cum_even = 0u, cum_odd = 0u;  // thread 0: summed sizes of the even and odd fronts
+    int k = 0;
+    for (;;) {
+        uint32_t* G = fmask + (size_t)(k % 3) * W;  // members of front k
+        const uint32_t nextw = (uint32_t)((k + 1) % 3);
+        for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += nblocks * blockDim.x)
+            fmask[(size_t)nextw * W + w] = 0u;
+        cp_async_wait_all();
+        // 1. probe: the window of a point whose blocker was assigned
+        bool is_free = false;
+        int slot = -1;
+        if (alive) {
+            if (b < 0) {
+                is_free = true;
+            } else if (!((U[b >> 5] >> (b & 31)) & 1u)) {
+                const int w = b >> 5;
+                const int lo = max(wtop - (kWin - 1), 0);
+                int hit = -1;
+                for (int i = wtop - w; i < kWin; ++i) {
+                    const int ww = wtop - i;
+                    if (ww < 0) break;
+                    const uint32_t bits = win[i * kPeelThreads] & U[ww];
+                    if (bits) {
+                        hit = ww * 32 + (31 - __clz(bits));
+                        break;
+                    }
+                }
+                if (hit >= 0) {
+                    b = hit;
+                } else if (lo == 0) {
+                    is_free = true;
+                } else {
+                    slot = atomicAdd(&s_nscan, 1);
+                    s_sq[slot] = q;
+                    s_sw[slot] = lo - 1;
+                }
+            }
+        }
+        __syncthreads();
+        // 2. the CTA's level-ordered scans of the queued rows (peel_body)
+        const int nscan = s_nscan;
+        if (nscan > 0) {
+            if (warp == 0) {
+                int levels = 0;
+                for (int s0 = 0; s0 < nscan; s0 += 32) {
+                    const int sidx = s0 + lane;
+                    if (sidx < nscan) {
+                        levels = max(levels, s_sw[sidx] / kScanChunk + 1);
+                        s_found[sidx] = -1;
+                    }
+                }
+#pragma unroll
+                for (int o = 16; o; o >>= 1) levels = max(levels, __shfl_xor_sync(0xFFFFFFFFu, levels, o));
+                if (lane == 0) s_ntask = levels * nscan;
+            }
+            __syncthreads();
+            const int ntask = s_ntask;
+            for (int task = warp; task < ntask; task += wpb) {
+                const int level = task / nscan, lo = task - level * nscan;
+                if (level > s_sw[lo] / kScanChunk) continue;
+                const int top = s_sw[lo] - level * kScanChunk;
+                const int found_hi = __shfl_sync(0xFFFFFFFFu, *((volatile int*)s_found + lo), 0);
+                if (found_hi > top * 32 + 31) continue;
+                const uint32_t* srow = rows + (size_t)s_sq[lo] * W;
+                uint32_t acc[kScanChunk / 32];
+#pragma unroll
+                for (int i = 0; i < kScanChunk / 32; ++i) {
+                    const int w = top - lane - 32 * i;
+                    acc[i] = (w >= 0 && w > top - kScanChunk) ? (__ldg(srow + w) & U[w]) : 0u;
+                }
+#pragma unroll
+                for (int i = 0; i < kScanChunk / 32; ++i) {
+                    const unsigned nz = __ballot_sync(0xFFFFFFFFu, acc[i] != 0u);
+                    if (nz) {
+                        const int src = __ffs(nz) - 1;
+                        const uint32_t bb = __shfl_sync(0xFFFFFFFFu, acc[i], src);
+                        if (lane == 0) atomicMax(s_found + lo, (top - src - 32 * i) * 32 + (31 - __clz(bb)));
+                        break;
+                    }
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) s_nscan = 0;  // next written after two more CTA barriers
+        }
+        if (slot >= 0) {
+            const int f = s_found[slot];
+            if (f >= 0) b = f;
+            else is_free = true;
+        }
+        // a blocker in a lower word: refill the window for the next front
+        if (alive && !is_free && b >= 0 && (b >> 5) != wtop) {
+            wtop = b >> 5;
+            window_fill(win, row, wtop);
+        }
+        cp_async_commit();
+        // 3. members of front k: the front's mask and the CTA's count
+        const unsigned fm = __ballot_sync(0xFFFFFFFFu, is_free);
+        if (fm) {
+            if (lane == 0) {
+                atomicOr(G + g, fm);
+                atomicAdd(&s_cnt, __popc(fm));
+            }
+            if (is_free) {
+                front_sorted[q] = k;
+                alive = false;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned long long v = counted_arrive(sizes + (k & 1), (unsigned)s_cnt,
+                                                        (unsigned long long)(k / 2 + 1) * (unsigned)nblocks,
+                                                        counters + 6, kPeelWaitNs);
+            s_cnt = 0;
+            s_ok = v != ~0ull;
+            if (s_ok) {
+                const unsigned c = (unsigned)v;
+                if (k & 1) {
+                    s_ck = (int)(c - cum_odd);
+                    cum_odd = c;
+                } else {
+                    s_ck = (int)(c - cum_even);
+                    cum_even = c;
+                }
+                s_total = (int)(cum_even + cum_odd);
+            }
+        }
+        __syncthreads();
+        if (!s_ok) {
+            cp_async_wait_all();
+            return;
+        }
+        // front k is complete: remove it from U
+        for (int w = threadIdx.x; w < W; w += blockDim.x) {
+            const uint32_t gv = __ldcg(G + w);
+            if (gv) U[w] &= ~gv;
+        }
+        __syncthreads();
+        const int ck = s_ck, total = s_total;
+        if (total >= target || ck == 0 || (feasible_only && total >= feasible)) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                counters[2] = k;
+                counters[3] = total;
+                counters[12] = k;
+                if (ck == 0 && total < (feasible_only ? feasible : target))
+                    atomicExch(counters + 6, kDevPeelInconsistent);
+            }
+            cp_async_wait_all();
+            return;
+        }
+        ++k;
+    }
+}
+
+// Shared memory of nds_peel_owned beyond its static arrays.
+size_t peel_owned_smem(int W)
+{
+    return (size_t)(((W + 3) & ~3) + kWin * kPeelThreads) * sizeof(uint32_t);
+}
+
 // Run heads among the infeasible class-2 positions (sorted by violation).
 __global__ void nds_infeasible_heads(int n, const int* __restrict__ qinfo, const int* __restrict__ counters,
                                      int target, int* __restrict__ flags)
@@ -904,6 +1180,7 @@ __global__ void nds_reset_counters(int* counters)
     if (threadIdx.x < 4) counters[threadIdx.x] = 0;
     if (threadIdx.x == 4) counters[4] = 0;
     if (threadIdx.x >= 10 && threadIdx.x <= 13) counters[threadIdx.x] = 0;
+    if (threadIdx.x >= 16 && threadIdx.x <= 19) counters[threadIdx.x] = 0;  // front sizes (nds_peel_owned)
 }
 
 template <int M>
@@ -1391,7 +1668,24 @@ int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_f
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (grid == 1) {
+    // lane-owned points when every warp of the grid holds at most one group
+    // of 32 positions and the rows are 16-byte aligned
+    const bool owned = ws.peel_owned_grid > 0 && ceil_div(n, 32) <= 32 * min(grid, ws.peel_owned_grid) &&
+                       Wp >= kWin;
+    if (owned) {
+        if (grid > ws.peel_owned_grid) grid = ws.peel_owned_grid;
+        const int* b0 = ws.blocker;
+        void* oargs[] = {(void*)&rows, (void*)&Wp, (void*)&nn, (void*)&tt, (void*)&b0,
+                         (void*)&fs, (void*)&fmask, (void*)&ctr};
+        cfg.gridDim = dim3(grid);
+        cfg.dynamicSmemBytes = peel_owned_smem(Wp);
+        if (grid == 1) {
+            nds_peel_owned<<<1, kPeelThreads, cfg.dynamicSmemBytes, stream>>>(rows, Wp, nn, tt, b0, fs, fmask,
+                                                                              ctr);
+        } else {
+            MOEA_CUDA_TRY(cudaLaunchKernelExC(&cfg, (const void*)nds_peel_owned, oargs));
+        }
+    } else if (grid == 1) {
         // one CTA needs no co-residency guarantee: an ordinary launch, which
         // may run beside other work (batched instances)
         nds_peel<<<1, kPeelThreads, cfg.dynamicSmemBytes, stream>>>(rows, Wp, nn, tt, qi, blk, fs, fmask,
@@ -1410,13 +1704,23 @@ int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_f
     return MOEA_OK;
 }
 
+// Raises a kernel's dynamic shared-memory limit to at least `bytes`.  The
+// limit belongs to the function, not to a workspace, so it is never lowered:
+// a smaller workspace created later must not shrink the launch of a larger one.
+static int raise_dynamic_smem(const void* func, size_t bytes)
+{
+    cudaFuncAttributes fa = {};
+    MOEA_CUDA_TRY(cudaFuncGetAttributes(&fa, func));
+    if ((size_t)fa.maxDynamicSharedSizeBytes < bytes)
+        MOEA_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return MOEA_OK;
+}
+
 // Configure the co-resident grid of the peel kernel for this device.
 int configure_peel(Workspace& ws)
 {
     const size_t smem = (size_t)ws.words * sizeof(uint32_t);
-    if (smem > 48 * 1024)
-        MOEA_CUDA_TRY(cudaFuncSetAttribute(nds_peel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem));
+    if (smem > 48 * 1024) MOEA_TRY(raise_dynamic_smem((const void*)nds_peel, smem));
     int per_sm = 0;
     MOEA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nds_peel, kPeelThreads,
                                                                 smem));
@@ -1426,6 +1730,15 @@ int configure_peel(Workspace& ws)
         return set_error(MOEA_ERR_UNSUPPORTED, "peel kernel does not fit on an SM (smem %zu)", smem);
     ws.peel_grid = sms * (per_sm > 2 ? 2 : per_sm);
     ws.peel_smem = (int)smem;
+    // the lane-owned peel: one CTA per SM
+    ws.peel_owned_grid = 0;
+    const size_t osmem = peel_owned_smem(ws.words);
+    if (ws.words >= kWin) {
+        MOEA_TRY(raise_dynamic_smem((const void*)nds_peel_owned, osmem));
+        int oper = 0;
+        MOEA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oper, nds_peel_owned, kPeelThreads, osmem));
+        if (oper >= 1) ws.peel_owned_grid = sms;
+    }
     return MOEA_OK;
 }
 
