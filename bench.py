@@ -747,12 +747,14 @@ def main() -> None:
         p.variables.copy_(h_vars, non_blocking=True)
         algo.step()
         p = algo.population_view()
+        # the whole next population back to the host: objectives, violations
+        # and the decision vectors (the next step's input)
         h_objs.copy_(p.objectives, non_blocking=True)
         h_cv.copy_(p.constraints, non_blocking=True)
+        h_vars.copy_(p.variables, non_blocking=True)
         if e1 is not None:
             e1.record(stream)
         torch.cuda.synchronize()
-        h_vars.copy_(p.variables)
 
     for _ in range(3):  # untimed warm-up of the host-copy path
         e2e_step()
@@ -834,7 +836,7 @@ def main() -> None:
                        "parallelism": f"replicas x{world}", "cuda_graph": graph_on},
             "clocks": clocks.summary(),
             "e2e": {"value": e2e_value, "unit": "gen/s",
-                    "h2d_bytes_per_step": N * D_VAR * 4, "d2h_bytes_per_step": N * (M_OBJ + 1) * 4},
+                    "h2d_bytes_per_step": N * D_VAR * 4, "d2h_bytes_per_step": N * (D_VAR + M_OBJ + 1) * 4},
             # graph kernels of the K device-timed and the K end-to-end generations
             "gpu_launches": kernels * 2 * args.steps,
             "stages_ms": stage_ms,

@@ -139,13 +139,14 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
-// Wait for the phase of this parity to complete; false after about 1 s.
-__device__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+// Wait for the phase of this parity to complete; false after limit_ns
+// (about 1 s in the association kernel).
+__device__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long limit_ns = 1000000000ull)
 {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = tc_now_ns();
     while (!mbar_try(bar, parity))
-        if (tc_now_ns() - t0 > 1000000000ull) return false;
+        if (tc_now_ns() - t0 > limit_ns) return false;
     return true;
 }
 
@@ -153,6 +154,11 @@ __device__ bool mbar_wait(uint64_t* bar, uint32_t parity)
 __device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity)
 {
     return __all_sync(0xFFFFFFFFu, mbar_wait(bar, parity));
+}
+
+__device__ __forceinline__ bool mbar_wait_warp_limit(uint64_t* bar, uint32_t parity, unsigned long long limit_ns)
+{
+    return __all_sync(0xFFFFFFFFu, mbar_wait(bar, parity, limit_ns));
 }
 
 // One contiguous global -> shared copy by the bulk-copy engine, completing
@@ -590,6 +596,22 @@ void launch_tensor(const float* x, int x_stride, const float* scale, int H, cons
                                                                  splits, d_n, pass, row_max, best, status);
 }
 
+// Self-test of the association's mbarrier wait with a short limit: the
+// barrier expects one arrival that never comes, so every warp's wait runs
+// out and the kernel records kDevTensorTimeout, as the association kernel
+// does before it drains.
+__global__ void selftest_mbar_wait(int* status, unsigned long long limit_ns)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_warp_limit(&bar, 0u, limit_ns);
+    if (!ok && threadIdx.x == 0) atomicExch(status, kDevTensorTimeout);
+}
+
 }  // namespace
 
 bool tensor_directions_ready(const Workspace& ws, const float* d_refs, int M, int H)
@@ -653,6 +675,13 @@ int run_associate_tensor(Workspace& ws, const float* x, int x_stride, const floa
     }
     MOEA_CUDA_TRY(cudaGetLastError());
     return run_assoc_finish(ws.assoc_best, d_n, n_cap, idx, dist, stream);
+}
+
+int selftest_mbar_timeout(Workspace& ws, unsigned long long limit_ns, cudaStream_t stream)
+{
+    selftest_mbar_wait<<<1, 64, 0, stream>>>(ws.counters + 6, limit_ns);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
 }
 
 }  // namespace moea

@@ -8,6 +8,8 @@
 namespace moea {
 
 int configure_peel(Workspace& ws);
+int selftest_barrier_timeout(Workspace& ws, int which, unsigned long long limit_ns, cudaStream_t stream);
+int selftest_mbar_timeout(Workspace& ws, unsigned long long limit_ns, cudaStream_t stream);
 int run_normalize_inplace(Workspace& ws, float* objs, const float* ideal, int M, int n,
                           float* rcp_out, int* extreme_out, cudaStream_t stream);
 int run_nsga3_select(Workspace& ws, const SplitPop& pop, int M, int N, const float* refs, int H,
@@ -95,7 +97,9 @@ int workspace_init(Workspace& ws, int device, int n_max, int m_max, int h_max)
     ws.n_max = n_max;
     ws.m_max = m_max;
     ws.h_max = h_max;
-    ws.words = ceil_div(n_max, 32);
+    // row words per point, a multiple of 4 so that every row starts on a
+    // 16-byte boundary (the peel copies aligned 16-byte chunks of rows)
+    ws.words = 4 * ceil_div(n_max, 128);
     const size_t n = (size_t)n_max;
     const int nb = ceil_div(n_max, 256);
     int st = MOEA_OK;
@@ -321,6 +325,19 @@ moea_status moea_quantize_cv(const float* d_cv, float* d_out, int n, float eps_f
         eps_feas < 0.0f)
         return set_error(MOEA_ERR_INVALID_ARGUMENT, "quantize_cv: bad arguments");
     return run_quantize_cv(d_cv, d_out, n, eps_feas, clip_upper, log_alpha, bins, S(stream));
+}
+
+moea_status moea_selftest_wait_timeout(moea_workspace* w, int which, unsigned long long limit_ns, void* stream)
+{
+    CHECK_WS(w);
+    if (which < 0 || which > 2 || limit_ns == 0 || limit_ns > 2000000000ull)
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "selftest_wait_timeout: which=%d limit_ns=%llu", which,
+                         limit_ns);
+    Workspace& ws = w->ws;
+    MOEA_CUDA_TRY(cudaSetDevice(ws.device));
+    if (which < 2) MOEA_TRY(selftest_barrier_timeout(ws, which, limit_ns, S(stream)));
+    else MOEA_TRY(selftest_mbar_timeout(ws, limit_ns, S(stream)));
+    return workspace_check_status(ws, S(stream));
 }
 
 }  // extern "C"

@@ -517,9 +517,11 @@ __device__ __forceinline__ int ld_acquire_gpu(const int* p)
 // launch (counters[4] is zeroed before it): barrier number `epoch` is passed
 // when the count reaches epoch * nblocks, so no CTA resets or releases
 // anything and the wait ends one acquire load after the last arrival.
-// Waits at most ~2 s, then records kDevBarrierTimeout in the status word and
-// returns false.  Every thread of the CTA passes the same epoch.
-__device__ bool grid_barrier(int* counters, unsigned nblocks, int epoch)
+// Waits at most limit_ns (2 s in the peel), then records kDevBarrierTimeout
+// in the status word and returns false.  Every thread of the CTA passes the
+// same epoch.
+__device__ bool grid_barrier(int* counters, unsigned nblocks, int epoch,
+                             unsigned long long limit_ns = 2000000000ull)
 {
     __shared__ int s_ok;
     __syncthreads();
@@ -536,7 +538,7 @@ __device__ bool grid_barrier(int* counters, unsigned nblocks, int epoch)
         const unsigned long long t0 = global_ns();
         while (ld_acquire_gpu(counters + 4) < target) {
             if (*((volatile int*)counters + 6) != 0) { ok = 0; break; }
-            if (global_ns() - t0 > 2000000000ull) {
+            if (global_ns() - t0 > limit_ns) {
                 atomicExch(counters + 6, kDevBarrierTimeout);
                 ok = 0;
                 break;
@@ -847,18 +849,21 @@ nds_peel(const uint32_t* __restrict__ rows, int W, int n, int target, const int*
 //
 // When every warp of the grid owns at most one group of 32 positions
 // (n <= 32 * 32 * CTAs), a lane keeps its point's state across the fronts:
-// the blocker in a register and a window of kWin row words (the blocker's
-// word and those below it) in shared memory.  The window is refilled with
-// cp.async whenever the blocker moves to a lower word, so the copy lands
-// while the grid waits at the barrier and the next front's probe reads only
-// shared memory.  Rows the window cannot settle go through the CTA's
+// the blocker in a register and a window of at least kWin row words (the
+// blocker's word and those below it) in shared memory, as five aligned
+// 16-byte chunks.  The window is refilled with cp.async whenever fewer than
+// kWin of its words lie at or below the blocker, so the copy lands while the
+// grid waits at the barrier and the next front's probe reads only shared
+// memory.  Row strides are multiples of four words (the workspace rounds
+// them), which keeps every chunk 16-byte aligned.  Rows the window cannot settle go through the CTA's
 // level-ordered scan as in peel_body.  The barrier carries the front sizes:
 // a CTA adds (1 << 32) + (its free points) to one of two 64-bit words (front
 // parity), so the front's size arrives with the barrier and no block-wide
 // count is needed.  A CTA can run at most one front ahead of the slowest, so
 // the word of front k holds only fronts k, k-2, ... when it is read.
 
-constexpr int kWin = 16;  // row words cached per lane below its blocker
+constexpr int kWin = 16;       // row words cached per lane at and below its blocker
+constexpr int kWinChunks = 5;  // 16-byte chunks of a window: 20 words from a multiple of 4
 constexpr unsigned long long kPeelWaitNs = 2000000000ull;  // limit of one barrier wait
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
@@ -866,24 +871,28 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p)
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-__device__ __forceinline__ void cp_async4(uint32_t* dst, const uint32_t* src)
+__device__ __forceinline__ void cp_async16(uint4* dst, const uint32_t* src)
 {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Row words wt, wt-1, ..., wt-kWin+1 of `row` into a lane's window (stride
-// kPeelThreads); words below 0 read as empty.
-__device__ __forceinline__ void window_fill(uint32_t* win, const uint32_t* row, int wt)
+// Row words wlo .. wt of `row` into a lane's window (chunk stride
+// kPeelThreads), wlo = wt - kWin + 1 rounded down to a multiple of 4; chunks
+// below word 0 read as empty, chunks above wt are not copied.  Returns wlo.
+__device__ __forceinline__ int window_fill(uint4* win, const uint32_t* row, int wt)
 {
+    const int wlo = (wt - (kWin - 1)) & ~3;
 #pragma unroll
-    for (int i = 0; i < kWin; ++i) {
-        const int w = wt - i;
-        if (w >= 0) cp_async4(win + i * kPeelThreads, row + w);
-        else win[i * kPeelThreads] = 0u;
+    for (int c = 0; c < kWinChunks; ++c) {
+        const int w0 = wlo + 4 * c;
+        if (w0 > wt) break;
+        if (w0 >= 0) cp_async16(win + c * kPeelThreads, row + w0);
+        else win[c * kPeelThreads] = make_uint4(0u, 0u, 0u, 0u);
     }
+    return wlo;
 }
 
 // Arrival at a front barrier that also sums the fronts' sizes: adds
@@ -915,7 +924,7 @@ nds_peel_owned(const uint32_t* __restrict__ rows, int W, int n, int target, cons
 {
     extern __shared__ uint32_t smem[];
     uint32_t* U = smem;                              // unassigned positions, one bit each
-    uint32_t* s_win = smem + ((W + 3) & ~3);         // [kWin][kPeelThreads] lane windows
+    uint4* s_win = reinterpret_cast<uint4*>(smem + ((W + 3) & ~3));  // [kWinChunks][kPeelThreads]
     __shared__ int s_nscan, s_ntask, s_cnt, s_ok, s_ck, s_total;
     __shared__ int s_sq[kScanQueue], s_sw[kScanQueue], s_found[kScanQueue];
     static_assert(kScanQueue >= kPeelThreads, "every owned point must fit the scan queue");
@@ -939,15 +948,12 @@ nds_peel_owned(const uint32_t* __restrict__ rows, int W, int n, int target, cons
     const int g = warp * nblocks + blockIdx.x;
     const int q = g * 32 + lane;
     bool alive = q < nf;
-    int b = -1, wtop = -1;
-    uint32_t* win = s_win + threadIdx.x;
+    int b = -1, wlo = 0;
+    uint4* win = s_win + threadIdx.x;
     const uint32_t* row = rows + (size_t)(alive ? q : 0) * W;
     if (alive) {
         b = blocker0[q];
-        if (b >= 0) {
-            wtop = b >> 5;
-            window_fill(win, row, wtop);
-        }
+        if (b >= 0) wlo = window_fill(win, row, b >> 5);
     }
     cp_async_commit();
     __syncthreads();
@@ -975,16 +981,25 @@ nds_peel_owned(const uint32_t* __restrict__ rows, int W, int n, int target, cons
             if (b < 0) {
                 is_free = true;
             } else if (!((U[b >> 5] >> (b & 31)) & 1u)) {
+                // the window's chunks from the top, each ANDed with the same
+                // four words of U (16-byte shared loads, no data-dependent
+                // branch); row words above the blocker's word are masked:
+                // beyond q's own word they are not part of the row
                 const int w = b >> 5;
-                const int lo = max(wtop - (kWin - 1), 0);
+                const int lo = max(wlo, 0);
+                const uint4* U4 = reinterpret_cast<const uint4*>(U);
                 int hit = -1;
-                for (int i = wtop - w; i < kWin; ++i) {
-                    const int ww = wtop - i;
-                    if (ww < 0) break;
-                    const uint32_t bits = win[i * kPeelThreads] & U[ww];
-                    if (bits) {
-                        hit = ww * 32 + (31 - __clz(bits));
-                        break;
+#pragma unroll
+                for (int c = kWinChunks - 1; c >= 0; --c) {
+                    const int w0 = wlo + 4 * c;
+                    if (w0 >= 0 && w0 <= w) {
+                        const uint4 v = win[c * kPeelThreads];
+                        const uint4 u = U4[w0 >> 2];
+                        const uint32_t m[4] = {v.x & u.x, w0 + 1 <= w ? v.y & u.y : 0u,
+                                               w0 + 2 <= w ? v.z & u.z : 0u, w0 + 3 <= w ? v.w & u.w : 0u};
+#pragma unroll
+                        for (int j = 3; j >= 0; --j)
+                            if (hit < 0 && m[j]) hit = (w0 + j) * 32 + (31 - __clz(m[j]));
                     }
                 }
                 if (hit >= 0) {
@@ -1030,15 +1045,23 @@ nds_peel_owned(const uint32_t* __restrict__ rows, int W, int n, int target, cons
                     const int w = top - lane - 32 * i;
                     acc[i] = (w >= 0 && w > top - kScanChunk) ? (__ldg(srow + w) & U[w]) : 0u;
                 }
+                // every loaded word is consumed (no load left in flight)
+                int si = -1;
+                unsigned snz = 0u;
+                uint32_t sel = 0u;
 #pragma unroll
                 for (int i = 0; i < kScanChunk / 32; ++i) {
                     const unsigned nz = __ballot_sync(0xFFFFFFFFu, acc[i] != 0u);
-                    if (nz) {
-                        const int src = __ffs(nz) - 1;
-                        const uint32_t bb = __shfl_sync(0xFFFFFFFFu, acc[i], src);
-                        if (lane == 0) atomicMax(s_found + lo, (top - src - 32 * i) * 32 + (31 - __clz(bb)));
-                        break;
+                    if (si < 0 && nz) {
+                        si = i;
+                        snz = nz;
+                        sel = acc[i];
                     }
+                }
+                if (si >= 0) {
+                    const int src = __ffs(snz) - 1;
+                    const uint32_t bb = __shfl_sync(0xFFFFFFFFu, sel, src);
+                    if (lane == 0) atomicMax(s_found + lo, (top - src - 32 * si) * 32 + (31 - __clz(bb)));
                 }
             }
             __syncthreads();
@@ -1049,11 +1072,9 @@ nds_peel_owned(const uint32_t* __restrict__ rows, int W, int n, int target, cons
             if (f >= 0) b = f;
             else is_free = true;
         }
-        // a blocker in a lower word: refill the window for the next front
-        if (alive && !is_free && b >= 0 && (b >> 5) != wtop) {
-            wtop = b >> 5;
-            window_fill(win, row, wtop);
-        }
+        // fewer than kWin window words at or below the blocker: refill the
+        // window for the next front
+        if (alive && !is_free && b >= 0 && (b >> 5) - wlo < kWin - 1) wlo = window_fill(win, row, b >> 5);
         cp_async_commit();
         // 3. members of front k: the front's mask and the CTA's count
         const unsigned fm = __ballot_sync(0xFFFFFFFFu, is_free);
@@ -1116,7 +1137,7 @@ nds_peel_owned(const uint32_t* __restrict__ rows, int W, int n, int target, cons
 // Shared memory of nds_peel_owned beyond its static arrays.
 size_t peel_owned_smem(int W)
 {
-    return (size_t)(((W + 3) & ~3) + kWin * kPeelThreads) * sizeof(uint32_t);
+    return (size_t)((W + 3) & ~3) * sizeof(uint32_t) + (size_t)kWinChunks * kPeelThreads * sizeof(uint4);
 }
 
 // Run heads among the infeasible class-2 positions (sorted by violation).
@@ -1563,7 +1584,30 @@ void launch_fused_tiles(const BatchInst* d_inst, const FusedBucket& b, cudaStrea
     fused_tiles<M><<<b.tile_blocks, kTileThreads, 0, s>>>(d_inst, b.d_ids, b.d_tile_prefix, b.count);
 }
 
+// Self-test of the peel's two barrier waits with a short limit: every CTA
+// arrives, but the barrier asks for one arrival more than the grid has, so
+// the wait runs out and records kDevBarrierTimeout.  which 0: the counted
+// barrier of nds_peel_owned; 1: grid_barrier of nds_peel.
+__global__ void selftest_barrier_wait(int* counters, int which, unsigned long long limit_ns)
+{
+    if (which == 0) {
+        if (threadIdx.x == 0)
+            counted_arrive(reinterpret_cast<unsigned long long*>(counters + 16), 0u,
+                           (unsigned long long)gridDim.x + 1ull, counters + 6, limit_ns);
+    } else {
+        grid_barrier(counters, gridDim.x + 1u, 1, limit_ns);
+    }
+}
+
 }  // namespace
+
+int selftest_barrier_timeout(Workspace& ws, int which, unsigned long long limit_ns, cudaStream_t stream)
+{
+    nds_reset_counters<<<1, 32, 0, stream>>>(ws.counters);
+    selftest_barrier_wait<<<2, 32, 0, stream>>>(ws.counters, which, limit_ns);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
 
 size_t cub_temp_bytes_needed(int n_max)
 {
@@ -1671,7 +1715,7 @@ int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_f
     // lane-owned points when every warp of the grid holds at most one group
     // of 32 positions and the rows are 16-byte aligned
     const bool owned = ws.peel_owned_grid > 0 && ceil_div(n, 32) <= 32 * min(grid, ws.peel_owned_grid) &&
-                       Wp >= kWin;
+                       Wp >= kWin && (Wp & 3) == 0;
     if (owned) {
         if (grid > ws.peel_owned_grid) grid = ws.peel_owned_grid;
         const int* b0 = ws.blocker;
@@ -1733,7 +1777,11 @@ int configure_peel(Workspace& ws)
     // the lane-owned peel: one CTA per SM
     ws.peel_owned_grid = 0;
     const size_t osmem = peel_owned_smem(ws.words);
-    if (ws.words >= kWin) {
+    int optin = 0;
+    MOEA_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ws.device));
+    cudaFuncAttributes ofa = {};
+    MOEA_CUDA_TRY(cudaFuncGetAttributes(&ofa, (const void*)nds_peel_owned));
+    if (ws.words >= kWin && osmem + ofa.sharedSizeBytes <= (size_t)optin) {
         MOEA_TRY(raise_dynamic_smem((const void*)nds_peel_owned, osmem));
         int oper = 0;
         MOEA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&oper, nds_peel_owned, kPeelThreads, osmem));

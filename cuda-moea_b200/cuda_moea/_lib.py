@@ -115,6 +115,7 @@ _SIGNATURES = [
     ("moea_normalize", c_int, [vp, vp, vp, c_int, c_int, vp, vp, vp]),
     ("moea_associate", c_int, [vp, vp, vp, c_int, c_int, c_int, vp, vp, c_int, vp]),
     ("moea_associate_static", c_int, [vp, vp, c_int, c_int, c_int, vp, vp, vp]),
+    ("moea_selftest_wait_timeout", c_int, [vp, c_int, ctypes.c_ulonglong, vp]),
     ("moea_igd", c_int, [vp, vp, c_int, c_int, vp, c_int, c_int, vp, ctypes.POINTER(ctypes.c_double), vp]),
     ("moea_niching", c_int, [vp, c_u64, ctypes.POINTER(c_u64), vp, vp, vp, vp, c_int, c_int, vp, vp]),
     ("moea_nsga3_select", c_int, [vp, vp, vp, c_int, c_int, vp, c_int, c_u64, ctypes.POINTER(c_u64),

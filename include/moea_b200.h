@@ -633,6 +633,17 @@ int moea_native_prepare(void* p, float* d_vars, float* d_objs, float* d_cv, int 
                         int max_generations, void* stream, int* h_changed);
 void moea_native_reset(void* p);
 
+/* Diagnostic for the bounded device waits.  Runs one of them against a
+ * condition that never completes, with a limit of limit_ns (1 ns .. 2 s),
+ * and reports what a caller of the real kernel would see: which 0 is the
+ * counted front barrier of the lane-owned peel, 1 the grid barrier of the
+ * general peel (both report MOEA_ERR_DEVICE_TIMEOUT "front peeling"), 2 the
+ * mbarrier wait of the tensor-core association (MOEA_ERR_DEVICE_TIMEOUT
+ * "association").  The wait gives up, the kernel returns and the workspace
+ * stays usable; nothing faults.  No counterpart in the reference, whose
+ * device waits are unbounded. */
+moea_status moea_selftest_wait_timeout(moea_workspace* ws, int which, unsigned long long limit_ns, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
