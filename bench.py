@@ -165,17 +165,28 @@ def cpu_generation_time(n: int, threads: int, seed: int = 1):
     mate = O.philox_stream(seed64, 0, 2, n)
     cand = np.stack([mate[:, 0] % n, mate[:, 1] % n], 1).astype(np.int32)
     pidx = O.tournament(cand, fronts, cv)
-    # the product's draw layout: one crossover block per pair element (SBX
-    # draws and both children's mutation tests), a mutation block for the
-    # amplitudes
-    cx = O.philox_stream(seed64, 0, 3, (n // 2) * D_VAR)
-    mu = O.philox_stream(seed64, 0, 4, (n // 2) * D_VAR)
+    # the product's draw layout: one crossover block per four variables of a
+    # pair (spread draw and sign per word; the crossover probability is 1 and
+    # the copy probability 0, so no test or copy blocks), mutation at
+    # geometric sites with limit pm_prob / D
+    pairs, D4 = n // 2, (D_VAR + 3) // 4
     unit = lambda u: (u >> 8).astype(np.float32) * np.float32(1.0 / 16777216.0)
-    off = O.sbx(x, pidx, bounds, np.stack([unit(cx[:, 0]), unit(cx[:, 1])], 1),
-                (cx[:, 0] & 1).astype(np.int32), unit(cx[:, 2]), 30.0, 1.0, 0.0, n)
-    low = ((cx[:, 1] & 0xFF) << 24) | ((cx[:, 2] & 0xFF) << 16) | ((cx[:, 3] & 0xFF) << 8)
-    um = np.stack([unit(cx[:, 3]), unit(mu[:, 0]), unit(low), unit(mu[:, 1])], 1).reshape(n // 2, D_VAR, 2, 2)
-    um = um.transpose(0, 2, 1, 3).reshape(n * D_VAR, 2)
+    cx = O.philox_stream(seed64, 0, 3, pairs * D4).reshape(pairs, D4 * 4)[:, :D_VAR].reshape(-1)
+    off = O.sbx(x, pidx, bounds, np.stack([unit(cx), np.zeros_like(unit(cx))], 1), (cx & 1).astype(np.int32),
+                np.zeros(pairs * D_VAR, np.float32), 30.0, 1.0, 0.0, n)
+    limit = np.float32(1.0) / np.float32(D_VAR)
+    log_keep = float(np.log1p(-np.float64(limit)))
+    um = np.zeros((n * D_VAR, 2), np.float32)
+    um[:, 0] = 2.0
+    site, live, k = np.full(n, -1, np.int64), np.ones(n, bool), 0
+    while live.any():
+        w = O.philox_stream(seed64, 0, 4, (k + 1) * n)[k * n:]
+        u = ((w[:, 0] >> 8) + 1).astype(np.float64) * (1.0 / 16777216.0)
+        site = np.where(live, site + 1 + np.minimum(np.floor(np.log(u) / log_keep), D_VAR).astype(np.int64), site)
+        live &= site < D_VAR
+        c = np.nonzero(live)[0]
+        um[c * D_VAR + site[c]] = np.stack([np.zeros(len(c), np.float32), unit(w[c, 1])], 1)
+        k += 1
     off = O.pm(off, bounds, um, 20.0, 1.0)
     of, ocv = O.evaluate("DTLZ1", off, M_OBJ)
     O.nsga3_select(np.concatenate([cv, ocv]), np.concatenate([f, of], 1), refs, seed64, 0, ideal)

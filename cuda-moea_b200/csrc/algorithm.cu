@@ -90,8 +90,7 @@ __global__ void gather_next(const float* __restrict__ vars_a, const float* __res
         const float* src = (s < pop.n_a) ? vars_a + (size_t)s * D : vars_b + (size_t)(s - pop.n_a) * D;
         float* dst = vars + (size_t)r * D;
         if (vec == 4) {
-            for (int u = lane; u < units; u += lanes)
-                reinterpret_cast<float4*>(dst)[u] = __ldg(reinterpret_cast<const float4*>(src) + u);
+            copy_units4(reinterpret_cast<float4*>(dst), reinterpret_cast<const float4*>(src), units, lane, lanes);
         } else {
             for (int u = lane; u < units; u += lanes) dst[u] = __ldg(src + u);
         }

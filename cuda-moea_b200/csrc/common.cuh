@@ -84,6 +84,8 @@ enum RngTag : uint32_t {
     kTagMating = 2,
     kTagCrossover = 3,
     kTagMutation = 4,
+    kTagCrossTest = 5,   // SBX crossover test draws (only when the crossover probability is below 1)
+    kTagCopy = 6,        // SBX variable copy draws (only when the copy probability is above 0)
 };
 
 __host__ __device__ inline void rng_block(uint64_t seed, uint64_t element, uint32_t generation,

@@ -158,6 +158,24 @@ int run_extract(Workspace& ws, const int* fronts, int n, const int* d_max_front,
 int run_normalize_split(Workspace& ws, const SplitPop& pop, const int* nds_gidx,
                         const int* sizes, const float* ideal, int M, cudaStream_t stream);
 
+// Copy of `units` 16-byte words by the threads lane = 0 .. lanes-1 of a
+// group, four loads in flight per thread (a row of a large-D population is
+// otherwise copied one dependent load/store pair at a time).
+__device__ __forceinline__ void copy_units4(float4* __restrict__ dst, const float4* __restrict__ src, int units,
+                                           int lane, int lanes)
+{
+    int u = lane;
+    for (; u + 3 * lanes < units; u += 4 * lanes) {
+        const float4 a = __ldg(src + u), b = __ldg(src + u + lanes);
+        const float4 c = __ldg(src + u + 2 * lanes), d = __ldg(src + u + 3 * lanes);
+        dst[u] = a;
+        dst[u + lanes] = b;
+        dst[u + 2 * lanes] = c;
+        dst[u + 3 * lanes] = d;
+    }
+    for (; u < units; u += lanes) dst[u] = __ldg(src + u);
+}
+
 // Margin of the dot^2 candidate filter of the association for a point with
 // |x|^2 = xx.  For directions with | |r|^2 - 1 | <= delta, the reference's
 // FP32 distance (association.cu:139-170) differs from xx - dot^2 by at most

@@ -52,7 +52,10 @@ __device__ __forceinline__ void sbx_pair(float x1, float x2, float u1, float u2,
         return;
     }
     const float power = 1.0f / (1.0f + eta);
-    float beta = u1 < 0.5f ? powf(2.0f * u1, power) : powf(1.0f / (2.0f - 2.0f * u1), power);
+    // one powf on the selected base (the same value as calling it in either
+    // branch, without a warp running both when its lanes disagree)
+    const float base = u1 < 0.5f ? 2.0f * u1 : 1.0f / (2.0f - 2.0f * u1);
+    float beta = powf(base, power);
     beta *= 2 * sign - 1;
     const float midpoint = 0.5f * (x1 + x2);
     const float delta = 0.5f * beta * (x1 - x2);
@@ -156,100 +159,145 @@ __global__ void mating_philox(const float* __restrict__ cv, const int* __restric
     mating_child(i, cv, rank, active, seed, gen, pidx);
 }
 
-// 24-bit uniform from the low bytes of three draws (bits the SBX draws of
-// the same block leave unused).
-__device__ __forceinline__ float low_bytes_unit(uint32_t a, uint32_t b, uint32_t c)
-{
-    return (float)(((a & 0xFFu) << 16) | ((b & 0xFFu) << 8) | (c & 0xFFu)) * (1.0f / 16777216.0f);
-}
-
-// SBX + PM for pair element e = p*D + d.  One Philox block (tag crossover)
-// gives the SBX draws (u1 and the sign from word 0, u2 from word 1, the copy
-// draw from word 2) and both children's mutation test draws (word 3, and the
-// unused low bytes of words 1-3).  A second block (tag mutation) is computed
-// only where a child mutates, with probability pm_prob/D per child: at large
-// D almost every element costs one block instead of two.
+// ---- variation with Philox draws ------------------------------------------
 //
-// kCross / kMutate select the passes: both (the fused variation), crossover
-// alone (children written unmutated) or mutation alone (children read from
-// off and mutated in place).  The draws are the same in every form, so
-// crossover followed by mutation equals the fused pass bit for bit.
-template <bool kCross, bool kMutate>
-__device__ __forceinline__ void variation_element(long long e, int p, int d,
-                                                  const float* __restrict__ parents,
-                                                  const int* __restrict__ pidx,
-                                                  const float* __restrict__ bounds,
-                                                  float* __restrict__ off, int pairs, int D,
-                                                  float eta_c, float sbx_prob, float copy_prob,
-                                                  int mutate, float eta_m, float pm_prob,
-                                                  uint64_t seed, uint32_t gen)
-{
-    const float lo = bounds[2 * d], hi = bounds[2 * d + 1];
-    const int ca = 2 * p, cb = ca + 1;
-    uint32_t r[4];
-    rng_block(seed, (uint64_t)e, gen, kTagCrossover, r);
-    float c1, c2 = 0.0f;
-    if (kCross) {
-        if (p < pairs) {
-            const float x1 = parents[(size_t)pidx[ca] * D + d];
-            const float x2 = parents[(size_t)pidx[cb] * D + d];
-            sbx_pair(x1, x2, u32_to_unit(r[0]), u32_to_unit(r[1]), (int)(r[0] & 1u),
-                     u32_to_unit(r[2]), eta_c, sbx_prob, copy_prob, lo, hi, c1, c2);
-        } else {
-            c1 = parents[(size_t)pidx[ca] * D + d];  // odd population: last child copies its parent
-        }
-    } else {
-        c1 = off[(size_t)ca * D + d];
-        if (p < pairs) c2 = off[(size_t)cb * D + d];
-    }
-    bool changed = kCross;
-    if (kMutate && mutate) {
-        // the reference's test, polynomial_mutation.cu:34
-        const float limit = pm_prob / static_cast<float>(D);
-        const float ta = u32_to_unit(r[3]);
-        const float tb = low_bytes_unit(r[1], r[2], r[3]);
-        const bool ma = ta < limit, mb = p < pairs && tb < limit;
-        if (ma || mb) {
-            uint32_t m[4];
-            rng_block(seed, (uint64_t)e, gen, kTagMutation, m);
-            if (ma) c1 = pm_value(c1, ta, u32_to_unit(m[0]), eta_m, pm_prob, D, lo, hi);
-            if (mb) c2 = pm_value(c2, tb, u32_to_unit(m[1]), eta_m, pm_prob, D, lo, hi);
-            changed = true;
-        }
-    }
-    if (!changed) return;  // mutation pass: untouched children stay as they are
-    off[(size_t)ca * D + d] = c1;
-    if (p < pairs) off[(size_t)cb * D + d] = c2;
-}
+// Draw layout (this project's own stream; the same in the fused pass, the
+// crossover-only pass followed by the mutation-only pass, and the batched
+// form):
+//
+//  crossover of pair p, variables 4j .. 4j+3: block b = p * ceil(D/4) + j of
+//    tag kTagCrossover; word i gives variable 4j+i its spread draw
+//    u1 = unit(w) and its sign (w & 1).  Only when sbx_prob < 1 the block b
+//    of tag kTagCrossTest gives the crossover test u2 (word i), and only when
+//    copy_prob > 0 the block b of tag kTagCopy gives the copy draw.  Skipping
+//    those draws changes nothing: u2 < 1 <= sbx_prob always passes and
+//    copy < copy_prob <= 0 never holds.
+//  mutation of child c: its mutated variables are drawn as geometric gaps,
+//    which gives every variable an independent chance limit = pm_prob / D (in
+//    FP32, the reference's test, polynomial_mutation.cu:34).  Draw k of child
+//    c is block k * n_off + c of tag kTagMutation: gap = floor(ln u / ln(1 -
+//    limit)) in FP64 with u = ((w0 >> 8) + 1) 2^-24, the site is the last
+//    site + 1 + gap, and unit(w1) is the site's amplitude draw.
+//
+// One block per four variables (instead of one per variable) and no per
+// variable mutation test: at large D the variation is then bound by its
+// powf and its HBM stream, not by Philox rounds.
 
-template <bool kCross, bool kMutate>
-__global__ void variation_philox(const float* __restrict__ parents, const int* __restrict__ pidx,
-                                 const float* __restrict__ bounds, float* __restrict__ off,
-                                 int n_off, int D, float sbx_eta0, float sbx_eta1, float sbx_prob,
-                                 float copy_prob, int mutate, float pm_eta0, float pm_eta1,
-                                 float pm_prob, int total, uint64_t seed,
-                                 const int* __restrict__ d_gen, uint32_t gen_host)
+__device__ __forceinline__ void crossover_group(int t, int p, int j, const float* __restrict__ parents,
+                                                const int* __restrict__ pidx, const float* __restrict__ bounds,
+                                                float* __restrict__ off, int pairs, int D, bool vec, float eta_c,
+                                                float sbx_prob, float copy_prob, uint64_t seed, uint32_t gen)
 {
-    const int pairs = n_off / 2;
-    const long long count = (long long)(pairs + (n_off & 1)) * D;
-    const uint32_t gen = d_gen ? (uint32_t)*d_gen : gen_host;
-    const float eta_c = annealed_eta(sbx_eta0, sbx_eta1, (int)gen, total);
-    const float eta_m = annealed_eta(pm_eta0, pm_eta1, (int)gen, total);
-    if (count <= 0x7FFFFFFFll) {  // 32-bit row/column split
-        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < (int)count; e += gridDim.x * blockDim.x) {
-            const int p = e / D;
-            variation_element<kCross, kMutate>(e, p, e - p * D, parents, pidx, bounds, off, pairs, D, eta_c,
-                                               sbx_prob, copy_prob, mutate, eta_m, pm_prob, seed, gen);
-        }
+    const int ca = 2 * p, cb = ca + 1;
+    const int d0 = 4 * j;
+    const int cnt = min(4, D - d0);
+    const float* xa = parents + (size_t)pidx[ca] * D + d0;
+    if (p >= pairs) {  // odd population: the last child copies its parent
+        for (int i = 0; i < cnt; ++i) off[(size_t)ca * D + d0 + i] = xa[i];
         return;
     }
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < count;
-         e += (long long)gridDim.x * blockDim.x)
-        variation_element<kCross, kMutate>(e, (int)(e / D), (int)(e % D), parents, pidx, bounds, off, pairs, D,
-                                           eta_c, sbx_prob, copy_prob, mutate, eta_m, pm_prob, seed, gen);
+    const float* xb = parents + (size_t)pidx[cb] * D + d0;
+    float a[4], bv[4], lo[4], hi[4];
+    if (vec) {
+        const float4 a4 = __ldg(reinterpret_cast<const float4*>(xa));
+        const float4 b4 = __ldg(reinterpret_cast<const float4*>(xb));
+        const float4 l01 = __ldg(reinterpret_cast<const float4*>(bounds + 2 * d0));
+        const float4 l23 = __ldg(reinterpret_cast<const float4*>(bounds + 2 * d0 + 4));
+        a[0] = a4.x; a[1] = a4.y; a[2] = a4.z; a[3] = a4.w;
+        bv[0] = b4.x; bv[1] = b4.y; bv[2] = b4.z; bv[3] = b4.w;
+        lo[0] = l01.x; hi[0] = l01.y; lo[1] = l01.z; hi[1] = l01.w;
+        lo[2] = l23.x; hi[2] = l23.y; lo[3] = l23.z; hi[3] = l23.w;
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const bool in = i < cnt;
+            a[i] = in ? xa[i] : 0.0f;
+            bv[i] = in ? xb[i] : 0.0f;
+            lo[i] = in ? bounds[2 * (d0 + i)] : 0.0f;
+            hi[i] = in ? bounds[2 * (d0 + i) + 1] : 0.0f;
+        }
+    }
+    uint32_t r[4], rt[4] = {0u, 0u, 0u, 0u}, rc[4] = {0u, 0u, 0u, 0u};
+    rng_block(seed, (uint64_t)t, gen, kTagCrossover, r);
+    if (sbx_prob < 1.0f) rng_block(seed, (uint64_t)t, gen, kTagCrossTest, rt);
+    if (copy_prob > 0.0f) rng_block(seed, (uint64_t)t, gen, kTagCopy, rc);
+    float c1[4], c2[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        sbx_pair(a[i], bv[i], u32_to_unit(r[i]), u32_to_unit(rt[i]), (int)(r[i] & 1u), u32_to_unit(rc[i]), eta_c,
+                 sbx_prob, copy_prob, lo[i], hi[i], c1[i], c2[i]);
+    float* oa = off + (size_t)ca * D + d0;
+    float* ob = off + (size_t)cb * D + d0;
+    if (vec) {
+        *reinterpret_cast<float4*>(oa) = make_float4(c1[0], c1[1], c1[2], c1[3]);
+        *reinterpret_cast<float4*>(ob) = make_float4(c2[0], c2[1], c2[2], c2[3]);
+    } else {
+        for (int i = 0; i < cnt; ++i) {
+            oa[i] = c1[i];
+            ob[i] = c2[i];
+        }
+    }
 }
 
-// ---- fused batch: mating then variation of every instance (blockIdx.y) ----
+__global__ void crossover_philox(const float* __restrict__ parents, const int* __restrict__ pidx,
+                                 const float* __restrict__ bounds, float* __restrict__ off, int n_off, int D,
+                                 bool vec, float sbx_eta0, float sbx_eta1, float sbx_prob, float copy_prob,
+                                 int total, uint64_t seed, const int* __restrict__ d_gen, uint32_t gen_host)
+{
+    const int pairs = n_off / 2;
+    const int D4 = (D + 3) >> 2;
+    const long long count = (long long)(pairs + (n_off & 1)) * D4;
+    const uint32_t gen = d_gen ? (uint32_t)*d_gen : gen_host;
+    const float eta_c = annealed_eta(sbx_eta0, sbx_eta1, (int)gen, total);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int p = (int)(t / D4);
+        crossover_group((int)t, p, (int)(t - (long long)p * D4), parents, pidx, bounds, off, pairs, D, vec, eta_c,
+                        sbx_prob, copy_prob, seed, gen);
+    }
+}
+
+// Polynomial mutation of child c in place at its geometric sites (layout
+// above).  Each step moves the site by at least one, so a child takes at most
+// D + 1 steps.
+__device__ __forceinline__ void mutate_child(int c, float* __restrict__ off, const float* __restrict__ bounds,
+                                             int n_off, int D, float eta_m, float pm_prob, uint64_t seed,
+                                             uint32_t gen)
+{
+    const float limit = pm_prob / static_cast<float>(D);
+    if (!(limit > 0.0f)) return;
+    const double log_keep = limit >= 1.0f ? 0.0 : log1p(-(double)limit);
+    float* row = off + (size_t)c * D;
+    long long site = -1;
+    for (long long k = 0;; ++k) {
+        uint32_t w[4];
+        rng_block(seed, (uint64_t)k * (uint64_t)n_off + (uint64_t)c, gen, kTagMutation, w);
+        long long gap = 0;
+        if (log_keep < 0.0) {
+            const double u = (double)((w[0] >> 8) + 1u) * (1.0 / 16777216.0);
+            const double g = floor(log(u) / log_keep);
+            gap = g < (double)D ? (long long)g : (long long)D;
+        }
+        site += 1 + gap;
+        if (site >= D) return;
+        const int d = (int)site;
+        // test draw 0 < limit: the site mutates (pm_value's own test passes)
+        row[d] = pm_value(row[d], 0.0f, u32_to_unit(w[1]), eta_m, pm_prob, D, bounds[2 * d], bounds[2 * d + 1]);
+    }
+}
+
+__global__ void mutation_philox(float* __restrict__ off, const float* __restrict__ bounds, int n_off, int D,
+                                float pm_eta0, float pm_eta1, float pm_prob, int total, uint64_t seed,
+                                const int* __restrict__ d_gen, uint32_t gen_host)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_off) return;
+    const uint32_t gen = d_gen ? (uint32_t)*d_gen : gen_host;
+    const float eta_m = annealed_eta(pm_eta0, pm_eta1, (int)gen, total);
+    mutate_child(c, off, bounds, n_off, D, eta_m, pm_prob, seed, gen);
+}
+
+// ---- fused batch: mating, crossover and mutation of every instance (blockIdx.y) ----
 __global__ void fused_mating(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
 {
     const BatchInst& I = insts[ids[blockIdx.y]];
@@ -258,19 +306,31 @@ __global__ void fused_mating(const BatchInst* __restrict__ insts, const int* __r
     mating_child(i, I.cvP, I.tournament ? I.rankP : nullptr, I.N, I.seed, (uint32_t)*I.d_gen, I.pidx);
 }
 
-__global__ void fused_variation(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+__global__ void fused_crossover(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
 {
     const BatchInst& I = insts[ids[blockIdx.y]];
     const int pairs = I.N / 2;
-    const long long count = (long long)(pairs + (I.N & 1)) * I.D;
+    const int D4 = (I.D + 3) >> 2;
+    const int count = (pairs + (I.N & 1)) * D4;  // fused instances hold at most 4096 x 263 variables
     const uint32_t gen = (uint32_t)*I.d_gen;
     const float eta_c = annealed_eta(I.sbx_eta0, I.sbx_eta1, (int)gen, I.T);
-    const float eta_m = annealed_eta(I.pm_eta0, I.pm_eta1, (int)gen, I.T);
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < (int)count; e += gridDim.x * blockDim.x) {
-        const int p = e / I.D;  // fused instances hold at most 4096 x 263 elements
-        variation_element<true, true>(e, p, e - p * I.D, I.varsP, I.pidx, I.bounds, I.varsO, pairs, I.D, eta_c,
-                                      I.sbx_prob, I.sbx_copy, I.mutate, eta_m, I.pm_prob, I.seed, gen);
+    const bool vec = (I.D & 3) == 0 && ((uintptr_t)I.varsP & 15) == 0 && ((uintptr_t)I.varsO & 15) == 0 &&
+                     ((uintptr_t)I.bounds & 15) == 0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+        const int p = t / D4;
+        crossover_group(t, p, t - p * D4, I.varsP, I.pidx, I.bounds, I.varsO, pairs, I.D, vec, eta_c, I.sbx_prob,
+                        I.sbx_copy, I.seed, gen);
     }
+}
+
+__global__ void fused_mutation(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    const BatchInst& I = insts[ids[blockIdx.y]];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= I.N || !I.mutate) return;
+    const uint32_t gen = (uint32_t)*I.d_gen;
+    const float eta_m = annealed_eta(I.pm_eta0, I.pm_eta1, (int)gen, I.T);
+    mutate_child(c, I.varsO, I.bounds, I.N, I.D, eta_m, I.pm_prob, I.seed, gen);
 }
 
 __global__ void rng_blocks_kernel(uint64_t seed, uint32_t gen, uint32_t tag, long long count,
@@ -320,21 +380,21 @@ int run_variation_pass(int passes, const float* parents, const int* pidx, const 
                        int mutate, float pm_eta0, float pm_eta1, float pm_prob, int total,
                        uint64_t seed, const int* d_gen, uint32_t gen, cudaStream_t stream)
 {
-    const long long count = (long long)(n_off / 2 + (n_off & 1)) * D;
-    const int grid = grid_for(count, 256);
-    if (passes == kPassBoth)
-        variation_philox<true, true><<<grid, 256, 0, stream>>>(
-            parents, pidx, bounds, off, n_off, D, sbx_eta0, sbx_eta1, sbx_prob, copy_prob, mutate,
-            pm_eta0, pm_eta1, pm_prob, total, seed, d_gen, gen);
-    else if (passes == kPassCrossover)
-        variation_philox<true, false><<<grid, 256, 0, stream>>>(
-            parents, pidx, bounds, off, n_off, D, sbx_eta0, sbx_eta1, sbx_prob, copy_prob, 0,
-            pm_eta0, pm_eta1, pm_prob, total, seed, d_gen, gen);
-    else
-        variation_philox<false, true><<<grid, 256, 0, stream>>>(
-            parents, pidx, bounds, off, n_off, D, sbx_eta0, sbx_eta1, sbx_prob, copy_prob, 1,
-            pm_eta0, pm_eta1, pm_prob, total, seed, d_gen, gen);
-    MOEA_CUDA_TRY(cudaGetLastError());
+    if (passes & kPassCrossover) {
+        const long long count = (long long)(n_off / 2 + (n_off & 1)) * ((D + 3) / 4);
+        // 16-byte loads and stores when every row and the bounds are aligned
+        const bool vec = (D & 3) == 0 && ((uintptr_t)parents & 15) == 0 && ((uintptr_t)off & 15) == 0 &&
+                         ((uintptr_t)bounds & 15) == 0;
+        crossover_philox<<<grid_for(count, 256), 256, 0, stream>>>(parents, pidx, bounds, off, n_off, D, vec,
+                                                                   sbx_eta0, sbx_eta1, sbx_prob, copy_prob, total,
+                                                                   seed, d_gen, gen);
+        MOEA_CUDA_TRY(cudaGetLastError());
+    }
+    if ((passes & kPassMutation) && mutate && n_off > 0) {
+        mutation_philox<<<ceil_div(n_off, 128), 128, 0, stream>>>(off, bounds, n_off, D, pm_eta0, pm_eta1, pm_prob,
+                                                                  total, seed, d_gen, gen);
+        MOEA_CUDA_TRY(cudaGetLastError());
+    }
     return MOEA_OK;
 }
 
@@ -350,8 +410,9 @@ int run_variation(const float* parents, const int* pidx, const float* bounds, fl
 int fused_reproduce(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s)
 {
     fused_mating<<<dim3(ceil_div(g.max_N, 256), g.count), 256, 0, s>>>(d_inst, g.d_ids);
-    const long long per = (long long)(g.max_N / 2 + 1) * g.max_D;
-    fused_variation<<<dim3((unsigned)grid_for(per, 256, 64), g.count), 256, 0, s>>>(d_inst, g.d_ids);
+    const long long per = (long long)(g.max_N / 2 + 1) * ((g.max_D + 3) / 4);
+    fused_crossover<<<dim3((unsigned)grid_for(per, 256, 64), g.count), 256, 0, s>>>(d_inst, g.d_ids);
+    fused_mutation<<<dim3(ceil_div(g.max_N, 128), g.count), 128, 0, s>>>(d_inst, g.d_ids);
     MOEA_CUDA_TRY(cudaGetLastError());
     return MOEA_OK;
 }

@@ -235,12 +235,14 @@ __global__ void rvea_update(SplitPop pop, const float* __restrict__ vars_a,
             const int s = survivors[r];
             const float* src = (s < pop.n_a) ? vars_a + (size_t)s * D : vars_b + (size_t)(s - pop.n_a) * D;
             if ((D & 3) == 0) {
-                const float4* s4 = reinterpret_cast<const float4*>(src);
-                float4* d4 = reinterpret_cast<float4*>(dst);
-                for (int d = threadIdx.x; d < (D >> 2); d += blockDim.x) d4[d] = __ldg(s4 + d);
+                copy_units4(reinterpret_cast<float4*>(dst), reinterpret_cast<const float4*>(src), D >> 2,
+                            threadIdx.x, blockDim.x);
             } else {
                 for (int d = threadIdx.x; d < D; d += blockDim.x) dst[d] = __ldg(src + d);
             }
+        } else if ((D & 3) == 0) {
+            const float4 nan4 = make_float4(CUDART_NAN_F, CUDART_NAN_F, CUDART_NAN_F, CUDART_NAN_F);
+            for (int d = threadIdx.x; d < (D >> 2); d += blockDim.x) reinterpret_cast<float4*>(dst)[d] = nan4;
         } else {
             for (int d = threadIdx.x; d < D; d += blockDim.x) dst[d] = CUDART_NAN_F;
         }

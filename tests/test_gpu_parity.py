@@ -382,35 +382,24 @@ def test_fused_reproduce_matches_composed_oracle(st, oracle):
     """The fused Philox reproduction against the oracle's tournament, SBX and
     PM fed with the oracle's own Philox stream in the product's draw layout
     (stated in tests/draws.py); tolerance for the host powf."""
+    import draws
     rng = np.random.default_rng(9)
-    for n, D, seed, gen in [(300, 13, 2024, 5), (301, 3, 77, 2)]:
+    for n, D, seed, gen, sbx_prob, copy_prob, pm_prob in [(300, 13, 2024, 5, 0.9, 0.0, 1.0),
+                                                          (301, 3, 77, 2, 1.0, 0.5, 1.0),
+                                                          (64, 8, 5, 1, 1.0, 0.0, 8.0)]:
         parents = rng.random((n, D)).astype(np.float32)
         bounds = np.tile([0.0, 1.0], D).astype(np.float32)
         cv = np.where(rng.random(n) < 0.2, rng.random(n), 0).astype(np.float32)
         rank = rng.integers(0, 4, n).astype(np.int32)
         off_g, pidx_g = st.reproduce(_t(parents), _t(cv), _t(rank), n, _t(bounds), n, seed=seed,
-                                     generation=gen, sbx_prob=0.9)
-
-        def unit(u):
-            return (u >> 8).astype(np.float32) * np.float32(1.0 / 16777216.0)
-        mate = oracle.philox_stream(seed, gen, 2, n)
-        cand = np.stack([mate[:, 0] % n, mate[:, 1] % n], 1).astype(np.int32)
+                                     generation=gen, sbx_prob=sbx_prob, sbx_copy_prob=copy_prob, pm_prob=pm_prob)
+        cand = draws.mating_candidates_np(oracle, seed, gen, n, n)
         pidx_w = oracle.tournament(cand, rank, cv)
         np.testing.assert_array_equal(pidx_g.cpu().numpy(), pidx_w)
-        pairs, units = n // 2, n // 2 + n % 2
-        cx = oracle.philox_stream(seed, gen, 3, units * D)
-        mu = oracle.philox_stream(seed, gen, 4, units * D)
-        sb = cx[: pairs * D]
-        u = np.stack([unit(sb[:, 0]), unit(sb[:, 1])], 1)
-        off_w = oracle.sbx(parents, pidx_w, bounds, u, (sb[:, 0] & 1).astype(np.int32), unit(sb[:, 2]),
-                           30.0, 0.9, 0.0, n)
-        low = ((cx[:, 1] & 0xFF) << 24) | ((cx[:, 2] & 0xFF) << 16) | ((cx[:, 3] & 0xFF) << 8)
-        um = np.zeros((units * 2, D, 2), np.float32)
-        um[0::2, :, 0] = unit(cx[:, 3]).reshape(units, D)
-        um[0::2, :, 1] = unit(mu[:, 0]).reshape(units, D)
-        um[1::2, :, 0] = unit(low).reshape(units, D)
-        um[1::2, :, 1] = unit(mu[:, 1]).reshape(units, D)
-        off_w = oracle.pm(off_w, bounds, um[:n].reshape(n * D, 2), 20.0, 1.0)
+        u, sign, copy = draws.crossover_draws_np(oracle, seed, gen, n, D, sbx_prob, copy_prob)
+        off_w = oracle.sbx(parents, pidx_w, bounds, u, sign, copy, 30.0, sbx_prob, copy_prob, n)
+        um = draws.mutation_draws_np(oracle, seed, gen, n, D, pm_prob)
+        off_w = oracle.pm(off_w, bounds, um, 20.0, pm_prob)
         np.testing.assert_allclose(off_g.cpu().numpy(), off_w, rtol=5e-6, atol=5e-7)
 
 
