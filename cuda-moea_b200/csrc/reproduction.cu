@@ -258,31 +258,47 @@ __global__ void crossover_philox(const float* __restrict__ parents, const int* _
 }
 
 // Polynomial mutation of child c in place at its geometric sites (layout
-// above).  Each step moves the site by at least one, so a child takes at most
-// D + 1 steps.
-__device__ __forceinline__ void mutate_child(int c, float* __restrict__ off, const float* __restrict__ bounds,
-                                             int n_off, int D, float eta_m, float pm_prob, uint64_t seed,
-                                             uint32_t gen)
+// above), by the four lanes sub = 0..3 of a lane group: draws k = 4i + sub
+// are evaluated side by side, their gaps summed with shuffles, and every lane
+// mutates its own site (sites are distinct).  Each draw moves the site by at
+// least one, so a child takes at most D/4 + 1 rounds.  All four lanes of the
+// group call this together (c and `active` uniform within the group).
+__device__ __forceinline__ void mutate_child4(int c, bool active, int sub, float* __restrict__ off,
+                                              const float* __restrict__ bounds, int n_off, int D, float eta_m,
+                                              float pm_prob, uint64_t seed, uint32_t gen)
 {
     const float limit = pm_prob / static_cast<float>(D);
-    if (!(limit > 0.0f)) return;
     const double log_keep = limit >= 1.0f ? 0.0 : log1p(-(double)limit);
+    const unsigned group = 0xFu << (threadIdx.x & 28u);
     float* row = off + (size_t)c * D;
-    long long site = -1;
-    for (long long k = 0;; ++k) {
-        uint32_t w[4];
-        rng_block(seed, (uint64_t)k * (uint64_t)n_off + (uint64_t)c, gen, kTagMutation, w);
-        long long gap = 0;
-        if (log_keep < 0.0) {
-            const double u = (double)((w[0] >> 8) + 1u) * (1.0 / 16777216.0);
-            const double g = floor(log(u) / log_keep);
-            gap = g < (double)D ? (long long)g : (long long)D;
+    long long site = -1;  // the group's last site
+    bool live = active && limit > 0.0f;
+    for (long long k0 = 0; __any_sync(group, live); k0 += 4) {
+        uint32_t w[4] = {0u, 0u, 0u, 0u};
+        long long step = 1;
+        if (live) {
+            rng_block(seed, (uint64_t)(k0 + sub) * (uint64_t)n_off + (uint64_t)c, gen, kTagMutation, w);
+            if (log_keep < 0.0) {
+                const double u = (double)((w[0] >> 8) + 1u) * (1.0 / 16777216.0);
+                const double g = floor(log(u) / log_keep);
+                step += g < (double)D ? (long long)g : (long long)D;
+            }
         }
-        site += 1 + gap;
-        if (site >= D) return;
-        const int d = (int)site;
-        // test draw 0 < limit: the site mutates (pm_value's own test passes)
-        row[d] = pm_value(row[d], 0.0f, u32_to_unit(w[1]), eta_m, pm_prob, D, bounds[2 * d], bounds[2 * d + 1]);
+        // inclusive sum of the steps over the group's lanes 0..sub
+        long long acc = step;
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) {
+            const long long v = __shfl_up_sync(group, acc, o, 4);
+            if (sub >= o) acc += v;
+        }
+        const long long my_site = site + acc;
+        if (live && my_site < D) {
+            const int d = (int)my_site;
+            // test draw 0 < limit: the site mutates (pm_value's own test passes)
+            row[d] = pm_value(row[d], 0.0f, u32_to_unit(w[1]), eta_m, pm_prob, D, bounds[2 * d], bounds[2 * d + 1]);
+        }
+        site = __shfl_sync(group, my_site, 3, 4);
+        live = live && site < D;
     }
 }
 
@@ -290,11 +306,11 @@ __global__ void mutation_philox(float* __restrict__ off, const float* __restrict
                                 float pm_eta0, float pm_eta1, float pm_prob, int total, uint64_t seed,
                                 const int* __restrict__ d_gen, uint32_t gen_host)
 {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n_off) return;
+    const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 2);
     const uint32_t gen = d_gen ? (uint32_t)*d_gen : gen_host;
     const float eta_m = annealed_eta(pm_eta0, pm_eta1, (int)gen, total);
-    mutate_child(c, off, bounds, n_off, D, eta_m, pm_prob, seed, gen);
+    mutate_child4(c < n_off ? c : 0, c < n_off, (int)(threadIdx.x & 3u), off, bounds, n_off, D, eta_m, pm_prob,
+                  seed, gen);
 }
 
 // ---- fused batch: mating, crossover and mutation of every instance (blockIdx.y) ----
@@ -326,11 +342,12 @@ __global__ void fused_crossover(const BatchInst* __restrict__ insts, const int* 
 __global__ void fused_mutation(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
 {
     const BatchInst& I = insts[ids[blockIdx.y]];
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= I.N || !I.mutate) return;
+    if (!I.mutate) return;  // uniform over the block
+    const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 2);
     const uint32_t gen = (uint32_t)*I.d_gen;
     const float eta_m = annealed_eta(I.pm_eta0, I.pm_eta1, (int)gen, I.T);
-    mutate_child(c, I.varsO, I.bounds, I.N, I.D, eta_m, I.pm_prob, I.seed, gen);
+    mutate_child4(c < I.N ? c : 0, c < I.N, (int)(threadIdx.x & 3u), I.varsO, I.bounds, I.N, I.D, eta_m, I.pm_prob,
+                  I.seed, gen);
 }
 
 __global__ void rng_blocks_kernel(uint64_t seed, uint32_t gen, uint32_t tag, long long count,
@@ -391,8 +408,8 @@ int run_variation_pass(int passes, const float* parents, const int* pidx, const 
         MOEA_CUDA_TRY(cudaGetLastError());
     }
     if ((passes & kPassMutation) && mutate && n_off > 0) {
-        mutation_philox<<<ceil_div(n_off, 128), 128, 0, stream>>>(off, bounds, n_off, D, pm_eta0, pm_eta1, pm_prob,
-                                                                  total, seed, d_gen, gen);
+        mutation_philox<<<ceil_div(4 * n_off, 128), 128, 0, stream>>>(off, bounds, n_off, D, pm_eta0, pm_eta1,
+                                                                      pm_prob, total, seed, d_gen, gen);
         MOEA_CUDA_TRY(cudaGetLastError());
     }
     return MOEA_OK;
@@ -412,7 +429,7 @@ int fused_reproduce(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s
     fused_mating<<<dim3(ceil_div(g.max_N, 256), g.count), 256, 0, s>>>(d_inst, g.d_ids);
     const long long per = (long long)(g.max_N / 2 + 1) * ((g.max_D + 3) / 4);
     fused_crossover<<<dim3((unsigned)grid_for(per, 256, 64), g.count), 256, 0, s>>>(d_inst, g.d_ids);
-    fused_mutation<<<dim3(ceil_div(g.max_N, 128), g.count), 128, 0, s>>>(d_inst, g.d_ids);
+    fused_mutation<<<dim3(ceil_div(4 * g.max_N, 128), g.count), 128, 0, s>>>(d_inst, g.d_ids);
     MOEA_CUDA_TRY(cudaGetLastError());
     return MOEA_OK;
 }
