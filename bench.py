@@ -309,8 +309,10 @@ def run_reference(args) -> None:
         "n_gpus": args.gpus, "steps": len(times), "warmup": 0,
         "ms_per_step": 1000.0 * total / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "population": N_POP, "directions": 32640,
-                   "device": "host CPU"},
+        "config": {"workload": WORKLOAD, "population": N_POP, "merged": 2 * N_POP, "directions": 32640,
+                   "l2": "host CPU run: no device cache between generations",
+                   "parallelism": "host threads (OpenMP)", "cuda_graph": False},
+        "device": "host CPU",
         "cpu_baseline": {"value": value, "unit": "gen/s", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "gen/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
