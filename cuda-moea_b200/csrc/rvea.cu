@@ -52,44 +52,47 @@ __global__ void translate_kernel(SplitPop pop, int M, const float* __restrict__ 
     for (int m = 0; m < M; ++m) t[(size_t)m * t_stride + i] = fmaxf(pop.obj(m, i) - zmin[m], 1e-32f);
 }
 
+// A warp per point: lane l takes the directions l, l+32, ... with the same
+// FMA order over m as a sequential scan, keeps the first maximum it meets,
+// and the warp reduces to the largest cosine with the smallest direction
+// index on ties, which is the sequential scan's `if (c > best)` result.
 template <int M>
 __global__ void __launch_bounds__(256)
 partition_kernel(const float* __restrict__ t, int t_stride, int n, const float* __restrict__ refs,
                  int K, const int* __restrict__ d_active, int n_active_host, int n_parent,
                  float* __restrict__ theta, int* __restrict__ idx)
 {
-    constexpr int kPartTile = (M <= 8) ? 1024 : 512;
-    __shared__ float s_ref[M][kPartTile];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < n;
+    const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;  // uniform over the warp
     float x[M];
     float sqr = 0.f;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
-        const float v = valid ? t[(size_t)m * t_stride + i] : 0.f;
+        const float v = t[(size_t)m * t_stride + i];
         x[m] = v;
         sqr = fmaf(v, v, sqr);
     }
     const float inv_norm = rsqrtf(sqr + 1e-12f);
     float best = -CUDART_INF_F;
     int bj = -1;
-    for (int j0 = 0; j0 < K; j0 += kPartTile) {
-        const int cnt = min(kPartTile, K - j0);
-        __syncthreads();
-        for (int u = threadIdx.x; u < cnt; u += blockDim.x)
+    for (int j = lane; j < K; j += 32) {
+        float dot = 0.f;
 #pragma unroll
-            for (int m = 0; m < M; ++m) s_ref[m][u] = refs[(size_t)m * K + j0 + u];
-        __syncthreads();
-        if (!valid) continue;
-        for (int u = 0; u < cnt; ++u) {
-            float dot = 0.f;
+        for (int m = 0; m < M; ++m) dot = fmaf(x[m], __ldg(refs + (size_t)m * K + j), dot);
+        const float c = dot * inv_norm;
+        if (c > best) { best = c; bj = j; }
+    }
 #pragma unroll
-            for (int m = 0; m < M; ++m) dot = fmaf(x[m], s_ref[m][u], dot);
-            const float c = dot * inv_norm;
-            if (c > best) { best = c; bj = j0 + u; }
+    for (int o = 16; o; o >>= 1) {
+        const float ob = __shfl_xor_sync(0xFFFFFFFFu, best, o);
+        const int oj = __shfl_xor_sync(0xFFFFFFFFu, bj, o);
+        if (ob > best || (ob == best && oj >= 0 && (bj < 0 || oj < bj))) {
+            best = ob;
+            bj = oj;
         }
     }
-    if (!valid) return;
+    if (lane != 0) return;
     theta[i] = (best > -CUDART_INF_F) ? acosf(fminf(fmaxf(best, 0.f), 1.f)) : CUDART_INF_F;
     const int n_active = d_active ? *d_active : n_active_host;
     idx[i] = (i >= n_active && i < n_parent) ? K : bj;
@@ -350,7 +353,7 @@ int run_rvea_partition(const float* t, int t_stride, int n, const float* refs, i
                        const int* d_active, int n_active, int n_parent, float* theta, int* idx,
                        cudaStream_t s)
 {
-    MOEA_DISPATCH_M(M, (partition_kernel<MM><<<ceil_div(n, 256), 256, 0, s>>>(
+    MOEA_DISPATCH_M(M, (partition_kernel<MM><<<ceil_div(n, 8), 256, 0, s>>>(
                            t, t_stride, n, refs, K, d_active, n_active, n_parent, theta, idx)));
     MOEA_CUDA_TRY(cudaGetLastError());
     return MOEA_OK;
