@@ -61,6 +61,10 @@ int run_rvea_apd(const float* t, int t_stride, int n, const float* theta, const 
 float rvea_penalty_scale(int M, int gen, int max_gen, float alpha);
 int run_rvea_elitism(Workspace& ws, const int* idx, const SplitPop& pop, const float* apd, int N,
                      int K, int* survivors, int* d_active, cudaStream_t s);
+bool rvea_block_eligible(int n, int M, int K);
+int run_rvea_select_block(const SplitPop& pop, const float* refs, int M, int K, const float* gamma, int* d_active,
+                          int N, const float* ps_table, const int* d_gen, float ps_host, float* t, int t_stride,
+                          float* zmin, float* theta, int* idx, float* apd, int* survivors, cudaStream_t s);
 int run_rvea_update(const SplitPop& pop, const float* vars_a, const float* vars_b,
                     const int* survivors, const int* d_active, int N, int D, int M, float* vars,
                     float* objs, float* cv, cudaStream_t s);
@@ -680,12 +684,18 @@ struct moea_algorithm {
                 vars[P], vars[O], pop, survivors, ws.fronts, N, D, M, vars[X], objs[X], cv[X], rank[X]);
             MOEA_CUDA_TRY(cudaGetLastError());
         } else {
-            MOEA_TRY(run_rvea_translate(pop, M, t_buf, 2 * N, zmin, stream));
-            MOEA_TRY(run_rvea_partition(t_buf, 2 * N, 2 * N, refs, M, H, d_active, N, N, theta, part_idx,
-                                        stream));
-            MOEA_TRY(run_rvea_apd(t_buf, 2 * N, 2 * N, theta, gamma, part_idx, M, H, ps_table, d_gen, 0.0f,
-                                  apd, stream));
-            MOEA_TRY(run_rvea_elitism(ws, part_idx, pop, apd, N, H, survivors, d_active, stream));
+            if (rvea_block_eligible(2 * N, M, H)) {
+                // small merged populations: the whole selection in one CTA
+                MOEA_TRY(run_rvea_select_block(pop, refs, M, H, gamma, d_active, N, ps_table, d_gen, 0.0f, t_buf,
+                                               2 * N, zmin, theta, part_idx, apd, survivors, stream));
+            } else {
+                MOEA_TRY(run_rvea_translate(pop, M, t_buf, 2 * N, zmin, stream));
+                MOEA_TRY(run_rvea_partition(t_buf, 2 * N, 2 * N, refs, M, H, d_active, N, N, theta, part_idx,
+                                            stream));
+                MOEA_TRY(run_rvea_apd(t_buf, 2 * N, 2 * N, theta, gamma, part_idx, M, H, ps_table, d_gen, 0.0f,
+                                      apd, stream));
+                MOEA_TRY(run_rvea_elitism(ws, part_idx, pop, apd, N, H, survivors, d_active, stream));
+            }
             MOEA_TRY(run_rvea_update(pop, vars[P], vars[O], survivors, d_active, N, D, M, vars[X], objs[X],
                                      cv[X], stream));
         }

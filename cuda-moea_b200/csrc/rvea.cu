@@ -98,23 +98,35 @@ partition_kernel(const float* __restrict__ t, int t_stride, int n, const float* 
     idx[i] = (i >= n_active && i < n_parent) ? K : bj;
 }
 
+// gamma_j: the angle to the nearest other direction.  The directions are
+// staged in shared memory tiles (every thread reads every direction).
 template <int M>
 __global__ void gamma_kernel(const float* __restrict__ refs, int K, float* __restrict__ gamma)
 {
+    constexpr int kTile = 512;
+    __shared__ float s_t[M][kTile];
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= K) return;
-    if (K == 1) { gamma[j] = CUDART_PI_F; return; }
     float q[M];
 #pragma unroll
-    for (int m = 0; m < M; ++m) q[m] = refs[(size_t)m * K + j];
+    for (int m = 0; m < M; ++m) q[m] = j < K ? refs[(size_t)m * K + j] : 0.f;
     float mx = -CUDART_INF_F;
-    for (int k = 0; k < K; ++k) {
-        if (k == j) continue;
-        float dot = 0.f;
+    for (int k0 = 0; k0 < K; k0 += kTile) {
+        const int cnt = min(kTile, K - k0);
+        __syncthreads();
+        for (int u = threadIdx.x; u < cnt; u += blockDim.x)
 #pragma unroll
-        for (int m = 0; m < M; ++m) dot = fmaf(q[m], __ldg(refs + (size_t)m * K + k), dot);
-        mx = fmaxf(mx, dot);
+            for (int m = 0; m < M; ++m) s_t[m][u] = refs[(size_t)m * K + k0 + u];
+        __syncthreads();
+        for (int u = 0; u < cnt; ++u) {
+            if (k0 + u == j) continue;
+            float dot = 0.f;
+#pragma unroll
+            for (int m = 0; m < M; ++m) dot = fmaf(q[m], s_t[m][u], dot);
+            mx = fmaxf(mx, dot);
+        }
     }
+    if (j >= K) return;
+    if (K == 1) { gamma[j] = CUDART_PI_F; return; }
     gamma[j] = (mx > -CUDART_INF_F) ? acosf(fminf(fmaxf(mx, 0.f), 1.f)) : CUDART_PI_F;
 }
 
@@ -317,6 +329,225 @@ __global__ void adapt_kernel(const float* __restrict__ v0, const float* __restri
         v[(size_t)m * K + j] = us ? sc[m] * is : (ub ? base[m] * ib : (m == 0 ? 1.f : 0.f));
 }
 
+// ---- the selection of a small merged population in three launches --------
+//
+// For 2N <= kRveaBlockPoints merged points and K <= kRveaBlockDirs directions
+// the staged translate (two launches), partition, APD and elitism (about ten
+// launches with two library sorts and a scan) become three launches:
+//   rvea_translate_block  one CTA: zmin and the translated objectives;
+//   partition_apd_kernel  a warp per point: the partition of partition_kernel
+//                         and, on lane 0, the APD of apd_kernel;
+//   rvea_elite_block      one CTA: each direction's winner, the survivors in
+//                         ascending order and the active count.
+// Every value comes from the same expressions in the same order as the staged
+// kernels, and the elitism keeps the same survivors:
+//   - the winner of direction j is the point with the smallest
+//     (flag, metric, index) among those partitioned to j: the head of j's run
+//     in the staged stable sort by (j, flag, metric), found here with a
+//     shared-memory atomicMin on the packed key;
+//   - with W winners, 0 < W <= N keeps them all; W > N keeps the N smallest
+//     winners by (flag, metric, index), and W = 0 keeps the N smallest points
+//     by (direction, flag, metric, index), both by counting ranks (rare cases,
+//     where the staged path sorts);
+//   - the active count is min(W, N), or N when W = 0.
+constexpr int kRveaBlockThreads = 1024;
+constexpr int kRveaBlockPoints = 4096;
+constexpr int kRveaBlockDirs = 4096;
+
+template <int M>
+__global__ void __launch_bounds__(kRveaBlockThreads, 1)
+rvea_translate_block(SplitPop pop, float* __restrict__ t, int t_stride, float* __restrict__ zmin)
+{
+    __shared__ float s_zw[M][32];
+    __shared__ float s_z[M];
+    const int n = pop.n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nthreads = blockDim.x, nwarps = nthreads >> 5;
+    // zmin: fminf is order independent on the GPU, so this equals zmin_kernel
+    float z[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) z[m] = CUDART_INF_F;
+    for (int i = tid; i < n; i += nthreads)
+#pragma unroll
+        for (int m = 0; m < M; ++m) z[m] = fminf(z[m], pop.obj(m, i));
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        float v = z[m];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_down_sync(0xFFFFFFFFu, v, o));
+        if (lane == 0) s_zw[m][warp] = v;
+    }
+    __syncthreads();
+    if (tid < M) {
+        float r = CUDART_INF_F;
+        for (int w = 0; w < nwarps; ++w) r = fminf(r, s_zw[tid][w]);
+        s_z[tid] = r;
+        zmin[tid] = r;
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += nthreads)
+#pragma unroll
+        for (int m = 0; m < M; ++m) t[(size_t)m * t_stride + i] = fmaxf(pop.obj(m, i) - s_z[m], 1e-32f);
+}
+
+// partition_kernel with apd_kernel on the warp's lane 0.
+template <int M>
+__global__ void __launch_bounds__(256)
+partition_apd_kernel(const float* __restrict__ t, int t_stride, int n, const float* __restrict__ refs, int K,
+                     const int* __restrict__ d_active, int n_parent, const float* __restrict__ gamma,
+                     const float* __restrict__ ps_table, const int* __restrict__ d_gen, float ps_host,
+                     float* __restrict__ theta, int* __restrict__ idx, float* __restrict__ apd)
+{
+    const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;  // uniform over the warp
+    float x[M];
+    float sqr = 0.f;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        const float v = t[(size_t)m * t_stride + i];
+        x[m] = v;
+        sqr = fmaf(v, v, sqr);
+    }
+    const float inv_norm = rsqrtf(sqr + 1e-12f);
+    float best = -CUDART_INF_F;
+    int bj = -1;
+    for (int j = lane; j < K; j += 32) {
+        float dot = 0.f;
+#pragma unroll
+        for (int m = 0; m < M; ++m) dot = fmaf(x[m], __ldg(refs + (size_t)m * K + j), dot);
+        const float c = dot * inv_norm;
+        if (c > best) { best = c; bj = j; }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        const float ob = __shfl_xor_sync(0xFFFFFFFFu, best, o);
+        const int oj = __shfl_xor_sync(0xFFFFFFFFu, bj, o);
+        if (ob > best || (ob == best && oj >= 0 && (bj < 0 || oj < bj))) {
+            best = ob;
+            bj = oj;
+        }
+    }
+    if (lane != 0) return;
+    const float th = (best > -CUDART_INF_F) ? acosf(fminf(fmaxf(best, 0.f), 1.f)) : CUDART_INF_F;
+    theta[i] = th;
+    const int r = (i >= *d_active && i < n_parent) ? K : bj;
+    idx[i] = r;
+    // apd_kernel: its norm is the same FMA sum over the translated values
+    const float penalty_scale = ps_table ? ps_table[*d_gen] : ps_host;
+    const float norm = sqrtf(sqr);
+    float a;
+    if (norm > 1e-12f) {
+        if (r < 0 || r >= K) {
+            a = kMetricMax;
+        } else {
+            const float theta_safe = fminf(fmaxf(th, 0.f), CUDART_PI_F);
+            const float gamma_safe = fmaxf(gamma[r], 1e-6f);
+            const float v = (1.f + penalty_scale * theta_safe / gamma_safe) * norm;
+            a = (!isfinite(v) || v < 0.f) ? kMetricMax : v;
+        }
+    } else {
+        a = 0.f;
+    }
+    apd[i] = a;
+}
+
+__global__ void __launch_bounds__(kRveaBlockThreads, 1)
+rvea_elite_block(SplitPop pop, const int* __restrict__ idx, const float* __restrict__ apd, int K, int N,
+                 int* __restrict__ d_active, int* __restrict__ survivors)
+{
+    extern __shared__ unsigned long long s_key[];  // max(K, n): winners, then the W = 0 keys
+    __shared__ unsigned char s_flag[kRveaBlockPoints];
+    __shared__ int s_red[32];
+    __shared__ int s_w;
+    const int n = pop.n, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nthreads = blockDim.x, nwarps = nthreads >> 5;
+    for (int j = tid; j < K; j += nthreads) s_key[j] = ~0ull;
+    for (int i = tid; i < n; i += nthreads) s_flag[i] = 0;
+    __syncthreads();
+    for (int i = tid; i < n; i += nthreads) {
+        const int r = idx[i];
+        if (r >= 0 && r < K) {
+            uint32_t flag;
+            const uint32_t mb = metric_bits(pop.cvv(i), apd[i], flag);
+            atomicMin(&s_key[r], ((unsigned long long)flag << 63) | ((unsigned long long)mb << 32) | (uint32_t)i);
+        }
+    }
+    __syncthreads();
+    int wl = 0;
+    for (int j = tid; j < K; j += nthreads) wl += s_key[j] != ~0ull ? 1 : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wl += __shfl_down_sync(0xFFFFFFFFu, wl, o);
+    if (lane == 0) s_red[warp] = wl;
+    __syncthreads();
+    if (tid == 0) {
+        int w = 0;
+        for (int k = 0; k < nwarps; ++k) w += s_red[k];
+        s_w = w;
+    }
+    __syncthreads();
+    const int W = s_w;
+    const int active = W > 0 ? min(W, N) : N;
+    if (W > 0 && W <= N) {
+        for (int j = tid; j < K; j += nthreads)
+            if (s_key[j] != ~0ull) s_flag[(uint32_t)s_key[j]] = 1;
+    } else if (W > N) {
+        // the N smallest winners (keys are distinct: they hold the index)
+        for (int j = tid; j < K; j += nthreads) {
+            const unsigned long long kj = s_key[j];
+            if (kj == ~0ull) continue;
+            int rank = 0;
+            for (int j2 = 0; j2 < K; ++j2) rank += s_key[j2] < kj ? 1 : 0;
+            if (rank < N) s_flag[(uint32_t)kj] = 1;
+        }
+    } else {
+        // no winner: the N smallest points by (direction, flag, metric), then index
+        for (int i = tid; i < n; i += nthreads) {
+            uint32_t flag;
+            const uint32_t mb = metric_bits(pop.cvv(i), apd[i], flag);
+            s_key[i] = ((unsigned long long)(uint32_t)idx[i] << 32) | ((unsigned long long)flag << 31) | mb;
+        }
+        __syncthreads();
+        for (int i = tid; i < n; i += nthreads) {
+            const unsigned long long ki = s_key[i];
+            int rank = 0;
+            for (int i2 = 0; i2 < n; ++i2) {
+                const unsigned long long k2 = s_key[i2];
+                rank += (k2 < ki || (k2 == ki && i2 < i)) ? 1 : 0;
+            }
+            if (rank < N) s_flag[i] = 1;
+        }
+    }
+    __syncthreads();
+    // the ascending survivor list: each thread counts a run of consecutive
+    // flags, a block scan gives the run's offset
+    const int per = (n + nthreads - 1) / nthreads;
+    const int b0 = tid * per, b1 = min(n, b0 + per);
+    int c = 0;
+    for (int i = b0; i < b1; ++i) c += s_flag[i];
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) s_red[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int v = lane < nwarps ? s_red[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xFFFFFFFFu, v, o);
+            if (lane >= o) v += u;
+        }
+        s_red[lane] = v;  // inclusive over the warps
+    }
+    __syncthreads();
+    int pos = incl - c + (warp > 0 ? s_red[warp - 1] : 0);
+    for (int i = b0; i < b1; ++i)
+        if (s_flag[i]) survivors[pos++] = i;
+    if (tid == 0) *d_active = active;
+}
+
 #define MOEA_DISPATCH_M(M, CALL)                                                      \
     switch (M) {                                                                      \
     case 1: { constexpr int MM = 1; CALL; } break;                                   \
@@ -372,6 +603,28 @@ int run_rvea_apd(const float* t, int t_stride, int n, const float* theta, const 
 {
     MOEA_DISPATCH_M(M, (apd_kernel<MM><<<ceil_div(n, 256), 256, 0, s>>>(
                            t, t_stride, n, theta, gamma, idx, K, ps_table, d_gen, ps_host, apd)));
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+// Whether the three-launch selection applies, and its launches.  Writes the
+// same t / zmin / theta / idx / apd values, survivors and active count as the
+// staged translate, partition, APD and elitism.
+bool rvea_block_eligible(int n, int M, int K)
+{
+    return n >= 1 && n <= kRveaBlockPoints && K >= 1 && K <= kRveaBlockDirs && M >= 1 && M <= 16;
+}
+
+int run_rvea_select_block(const SplitPop& pop, const float* refs, int M, int K, const float* gamma, int* d_active,
+                          int N, const float* ps_table, const int* d_gen, float ps_host, float* t, int t_stride,
+                          float* zmin, float* theta, int* idx, float* apd, int* survivors, cudaStream_t s)
+{
+    const int n = pop.n;
+    MOEA_DISPATCH_M(M, (rvea_translate_block<MM><<<1, kRveaBlockThreads, 0, s>>>(pop, t, t_stride, zmin)));
+    MOEA_DISPATCH_M(M, (partition_apd_kernel<MM><<<ceil_div(n, 8), 256, 0, s>>>(
+                           t, t_stride, n, refs, K, d_active, N, gamma, ps_table, d_gen, ps_host, theta, idx, apd)));
+    const size_t smem = sizeof(unsigned long long) * (size_t)(K > n ? K : n);
+    rvea_elite_block<<<1, kRveaBlockThreads, smem, s>>>(pop, idx, apd, K, N, d_active, survivors);
     MOEA_CUDA_TRY(cudaGetLastError());
     return MOEA_OK;
 }
