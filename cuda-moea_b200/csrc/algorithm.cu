@@ -67,7 +67,8 @@ int run_rvea_select_block(const SplitPop& pop, const float* refs, int M, int K, 
                           float* zmin, float* theta, int* idx, float* apd, int* survivors, cudaStream_t s);
 int run_rvea_update(const SplitPop& pop, const float* vars_a, const float* vars_b,
                     const int* survivors, const int* d_active, int N, int D, int M, float* vars,
-                    float* objs, float* cv, cudaStream_t s);
+                    float* objs, float* cv, cudaStream_t s, int* nan_rows = nullptr);
+int run_fill_int(int* p, int count, int value, cudaStream_t s);
 int run_rvea_adapt(const float* v0, const float* objs, int stride, const int* d_active,
                    int n_active, int M, int K, float* range_tmp, float* v, cudaStream_t s);
 int das_dennis(int mode, int n, int M, std::vector<float>& out);
@@ -232,6 +233,12 @@ struct moea_algorithm {
     int* survivors = nullptr;
     int* frontzero = nullptr;
     int frontzero_count = 0;
+    // RVEA: per population slot, the first row from which every row is known
+    // to hold the dead-slot NaN sentinels (N: nothing known).  The update
+    // fills only the dead rows below it.  Reset whenever the rows may have
+    // been written outside the update (start, snapshot load, a population
+    // view handed out).
+    int* nan_rows = nullptr;
     uint64_t seed = 0;
     uint32_t epoch = 0;
     int generation = 0;
@@ -272,7 +279,7 @@ struct moea_algorithm {
         void* ptrs[] = {vars[0], vars[1], vars[2], objs[0], objs[1], objs[2], cv[0], cv[1], cv[2],
                         rank[0], rank[1], rank[2], cv_sort[0], cv_sort[1], bounds, parent_idx, refs,
                         refs0, gamma, ideal_last, d_gen, d_active, ps_table, cv_table, t_buf, theta,
-                        apd, part_idx, zmin, survivors, frontzero};
+                        apd, part_idx, zmin, survivors, frontzero, nan_rows};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         std::memset(vars, 0, sizeof(vars));
@@ -281,7 +288,7 @@ struct moea_algorithm {
         std::memset(rank, 0, sizeof(rank));
         cv_sort[0] = cv_sort[1] = nullptr;
         bounds = refs = refs0 = gamma = ideal_last = ps_table = t_buf = theta = apd = zmin = nullptr;
-        parent_idx = d_gen = d_active = cv_table = part_idx = survivors = frontzero = nullptr;
+        parent_idx = d_gen = d_active = cv_table = part_idx = survivors = frontzero = nan_rows = nullptr;
         if (ws_ready) { workspace_free(ws); ws_ready = false; }
         if (own_stream && stream) { cudaStreamDestroy(stream); stream = nullptr; }
     }
@@ -471,6 +478,7 @@ struct moea_algorithm {
         MOEA_TRY(dmalloc(&zmin, (size_t)M));
         MOEA_TRY(dmalloc(&survivors, (size_t)2 * N));
         MOEA_TRY(dmalloc(&frontzero, (size_t)N));
+        MOEA_TRY(dmalloc(&nan_rows, 3));
         std::vector<float> hb(2 * (size_t)D);
         for (int d = 0; d < D; ++d) {
             hb[2 * d] = lower.empty() ? 0.0f : lower[d];
@@ -601,6 +609,7 @@ struct moea_algorithm {
         last_prepared_target = L.last_prepared_target;
         ideal_ready = L.ideal_ready != 0;
         frontzero_count = 0;
+        MOEA_TRY(forget_nan_rows());
         drop_graphs();  // captured generations hold the seed of their epoch
         if (fused_single) MOEA_TRY(describe_single_fused());
         return MOEA_OK;
@@ -622,6 +631,7 @@ struct moea_algorithm {
         MOEA_CUDA_TRY(cudaMemcpyAsync(d_gen, &zero, sizeof(int), cudaMemcpyHostToDevice, stream));
         MOEA_CUDA_TRY(cudaMemcpyAsync(d_active, &N, sizeof(int), cudaMemcpyHostToDevice, stream));
         MOEA_CUDA_TRY(cudaMemsetAsync(ws.offset_dev, 0, sizeof(unsigned long long), stream));
+        MOEA_TRY(forget_nan_rows());
         ideal_ready = false;
         last_prepared_target = -2;
         MOEA_TRY(prepare());
@@ -630,6 +640,12 @@ struct moea_algorithm {
     }
 
     uint64_t gen_seed() const { return seed ^ ((uint64_t)epoch << 48); }
+
+    // No slot's rows are known to hold the sentinels any more.
+    int forget_nan_rows()
+    {
+        return nan_rows ? run_fill_int(nan_rows, 3, N, stream) : MOEA_OK;
+    }
 
     // Reproduction, evaluation and selection of one generation: the part that
     // is replayed from a CUDA graph.
@@ -697,7 +713,7 @@ struct moea_algorithm {
                 MOEA_TRY(run_rvea_elitism(ws, part_idx, pop, apd, N, H, survivors, d_active, stream));
             }
             MOEA_TRY(run_rvea_update(pop, vars[P], vars[O], survivors, d_active, N, D, M, vars[X], objs[X],
-                                     cv[X], stream));
+                                     cv[X], stream, nan_rows + X));
         }
         bump_generation<<<1, 1, 0, stream>>>(d_gen);
         MOEA_CUDA_TRY(cudaGetLastError());
@@ -988,6 +1004,8 @@ moea_status moea_algorithm_view(moea_algorithm* a, moea_population_view* v)
     v->graph_active = (a->graph[0] || a->graph[1]) ? 1 : 0;
     v->last_max_front = -1;
     if (!a->initialized) return MOEA_OK;
+    // the caller may write the rows it is given
+    MOEA_TRY(a->forget_nan_rows());
     v->d_variables = a->vars[a->P];
     v->d_objectives = a->objs[a->P];
     v->d_constraints = a->cv[a->P];

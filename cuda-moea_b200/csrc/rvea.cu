@@ -11,6 +11,8 @@
 // The reference reads the winner count back to the host every generation
 // (elitism_selection.cu:256-257); here the count stays on the device and the
 // truncation, the active count and the sentinel rows are decided there.
+#include <algorithm>
+
 #include <cub/cub.cuh>
 
 #include <math_constants.h>
@@ -237,29 +239,46 @@ __global__ void elite_select(const int* __restrict__ first_vals, const int* __re
 // Next parents: survivor rows of the variables (one row per block iteration,
 // float4 when D is a multiple of 4), then objectives and violations; rows at
 // or beyond `active` get the sentinels.
+// Next parents: survivor rows of the variables, rows at or beyond `active`
+// the NaN sentinels, then objectives and violations (sentinels past
+// `active`).  The rows are cut into work items of kUpdateChunk variables, so
+// a large D spreads over every SM whatever the active count.  Dead rows at or
+// beyond *nan_rows already hold the sentinels and are skipped (all dead rows
+// are written when nan_rows is null).
+constexpr int kUpdateChunk = 8192;
+
 __global__ void rvea_update(SplitPop pop, const float* __restrict__ vars_a,
                             const float* __restrict__ vars_b, const int* __restrict__ survivors,
-                            const int* __restrict__ d_active, int N, int D, int M,
-                            float* __restrict__ vars, float* __restrict__ objs,
-                            float* __restrict__ cv)
+                            const int* __restrict__ d_active, const int* __restrict__ nan_rows, int N, int D,
+                            int M, float* __restrict__ vars, float* __restrict__ objs, float* __restrict__ cv)
 {
     const int active = *d_active;
-    for (int r = blockIdx.x; r < N; r += gridDim.x) {
+    const int fill_end = nan_rows ? min(N, *nan_rows) : N;
+    const int per_row = (D + kUpdateChunk - 1) / kUpdateChunk;
+    const long long items = (long long)N * per_row;
+    const bool vec = (D & 3) == 0;
+    for (long long w = blockIdx.x; w < items; w += gridDim.x) {
+        const int r = (int)(w / per_row);
+        const int d0 = (int)(w - (long long)r * per_row) * kUpdateChunk;
+        const int d1 = min(D, d0 + kUpdateChunk);
         float* dst = vars + (size_t)r * D;
         if (r < active) {
             const int s = survivors[r];
             const float* src = (s < pop.n_a) ? vars_a + (size_t)s * D : vars_b + (size_t)(s - pop.n_a) * D;
-            if ((D & 3) == 0) {
-                copy_units4(reinterpret_cast<float4*>(dst), reinterpret_cast<const float4*>(src), D >> 2,
-                            threadIdx.x, blockDim.x);
+            if (vec) {
+                copy_units4(reinterpret_cast<float4*>(dst + d0), reinterpret_cast<const float4*>(src + d0),
+                            (d1 - d0) >> 2, threadIdx.x, blockDim.x);
             } else {
-                for (int d = threadIdx.x; d < D; d += blockDim.x) dst[d] = __ldg(src + d);
+                for (int d = d0 + threadIdx.x; d < d1; d += blockDim.x) dst[d] = __ldg(src + d);
             }
-        } else if ((D & 3) == 0) {
-            const float4 nan4 = make_float4(CUDART_NAN_F, CUDART_NAN_F, CUDART_NAN_F, CUDART_NAN_F);
-            for (int d = threadIdx.x; d < (D >> 2); d += blockDim.x) reinterpret_cast<float4*>(dst)[d] = nan4;
-        } else {
-            for (int d = threadIdx.x; d < D; d += blockDim.x) dst[d] = CUDART_NAN_F;
+        } else if (r < fill_end) {
+            if (vec) {
+                const float4 nan4 = make_float4(CUDART_NAN_F, CUDART_NAN_F, CUDART_NAN_F, CUDART_NAN_F);
+                for (int u = (d0 >> 2) + threadIdx.x; u < (d1 >> 2); u += blockDim.x)
+                    reinterpret_cast<float4*>(dst)[u] = nan4;
+            } else {
+                for (int d = d0 + threadIdx.x; d < d1; d += blockDim.x) dst[d] = CUDART_NAN_F;
+            }
         }
     }
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N; e += gridDim.x * blockDim.x) {
@@ -273,6 +292,18 @@ __global__ void rvea_update(SplitPop pop, const float* __restrict__ vars_a,
             cv[r] = kSentinel;
         }
     }
+}
+
+// After an update: every row from the active count on holds the sentinels.
+__global__ void rvea_mark_nan_rows(int* __restrict__ nan_rows, const int* __restrict__ d_active)
+{
+    *nan_rows = *d_active;
+}
+
+__global__ void fill_int_kernel(int* __restrict__ p, int count, int value)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) p[i] = value;
 }
 
 __global__ void zrange_kernel(const float* __restrict__ objs, int stride, const int* __restrict__ d_n,
@@ -666,10 +697,19 @@ int run_rvea_elitism(Workspace& ws, const int* idx, const SplitPop& pop, const f
 
 int run_rvea_update(const SplitPop& pop, const float* vars_a, const float* vars_b,
                     const int* survivors, const int* d_active, int N, int D, int M, float* vars,
-                    float* objs, float* cv, cudaStream_t s)
+                    float* objs, float* cv, cudaStream_t s, int* nan_rows)
 {
-    const int blocks = N < 148 * 16 ? (N > 0 ? N : 1) : 148 * 16;
-    rvea_update<<<blocks, 256, 0, s>>>(pop, vars_a, vars_b, survivors, d_active, N, D, M, vars, objs, cv);
+    const long long items = (long long)N * ((D + kUpdateChunk - 1) / kUpdateChunk);
+    const int blocks = (int)std::max(1ll, std::min(items, (long long)148 * 16));
+    rvea_update<<<blocks, 256, 0, s>>>(pop, vars_a, vars_b, survivors, d_active, nan_rows, N, D, M, vars, objs, cv);
+    if (nan_rows) rvea_mark_nan_rows<<<1, 1, 0, s>>>(nan_rows, d_active);
+    MOEA_CUDA_TRY(cudaGetLastError());
+    return MOEA_OK;
+}
+
+int run_fill_int(int* p, int count, int value, cudaStream_t s)
+{
+    fill_int_kernel<<<(count + 255) / 256, 256, 0, s>>>(p, count, value);
     MOEA_CUDA_TRY(cudaGetLastError());
     return MOEA_OK;
 }

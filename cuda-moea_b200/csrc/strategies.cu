@@ -53,7 +53,7 @@ int run_rvea_elitism(Workspace& ws, const int* idx, const SplitPop& pop, const f
                      int K, int* survivors, int* d_active, cudaStream_t s);
 int run_rvea_update(const SplitPop& pop, const float* vars_a, const float* vars_b,
                     const int* survivors, const int* d_active, int N, int D, int M, float* vars,
-                    float* objs, float* cv, cudaStream_t s);
+                    float* objs, float* cv, cudaStream_t s, int* nan_rows = nullptr);
 int run_rvea_adapt(const float* v0, const float* objs, int stride, const int* d_active,
                    int n_active, int M, int K, float* range_tmp, float* v, cudaStream_t s);
 int run_gather_next(const float* vars_a, const float* vars_b, const SplitPop& pop, const int* survivors,

@@ -261,3 +261,28 @@ def test_small_population_fused_equals_staged(problem, D, M, N, graphs):
         torch.testing.assert_close(x[0], y[0], rtol=0, atol=0, msg=f"variables, generation {g}")
         torch.testing.assert_close(x[1], y[1], rtol=0, atol=0, msg=f"objectives, generation {g}")
         torch.testing.assert_close(x[2], y[2], rtol=0, atol=0, msg=f"fronts, generation {g}")
+
+
+@pytest.mark.parametrize("D", [12, 20001])
+def test_rvea_dead_rows_without_views_equal_rows_with_views(D):
+    """The RVEA update skips dead rows that already hold the NaN sentinels
+    from an earlier generation of the same slot, and writes them again once a
+    population view has been handed out.  A run that takes no view until its
+    end must equal, bit for bit and NaN rows included, a run that takes one
+    every generation.  D=20001 cuts rows into several update work items and
+    leaves no 16-byte row alignment."""
+    def run(view_each):
+        algo = cm.RVEA(population_size=120, max_generations=12, problem=cm.DTLZ2(D, 3), seed=99,
+                       print_progress=False)
+        algo.initialize()
+        for _ in range(12):
+            algo.step()
+            if view_each:
+                algo.population_view()
+        r = algo.result()
+        return (r.variables, r.objectives, r.constraints, r.active_count)
+    a, b = run(True), run(False)
+    for x, y in zip(a[:3], b[:3]):
+        assert torch.equal(x.view(torch.int32), y.view(torch.int32))
+    assert a[3] == b[3]
+    assert a[3] < 120 and torch.isnan(a[0][a[3]:]).all()
