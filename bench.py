@@ -14,6 +14,9 @@ between timed steps the L2 cache is flushed by writing a 256 MiB buffer
 (a single instance does not shard), value = total generations/s,
 max-over-ranks time; the batched record shards its instances over the ranks.
 
+The default line also carries `rvea_large_d` (RVEA DTLZ2 M=8 D=131072 N=1024,
+10 timed generations) and the batched record.
+
 Other workloads (--workload): dtlz2-small (N=92), rvea-large-d (D=131072),
 c1dtlz1-m10 and constrained-batch (ten objectives, 275 two-layer
 directions, 64 seeds per batched launch), dtlz2-m8 (tensor-core
@@ -504,8 +507,11 @@ def precision_form(torch, cm, seed: int, gens: int = 4):
     return out
 
 
-def other_workload(args, torch, cm):
-    w = OTHER_WORKLOADS[args.workload]
+def measure_workload(name, steps, warmup, seed, torch, cm):
+    """One of OTHER_WORKLOADS timed like the headline: `steps` generations
+    after `warmup`, CUDA events on the algorithm's stream, L2 flushed before
+    every timed generation, clocks sampled during the timed region."""
+    w = OTHER_WORKLOADS[name]
     kind, D, M = w["problem"]
     kw = {}
     if w["dirs"] and w["dirs"][0] == "dd":
@@ -513,16 +519,16 @@ def other_workload(args, torch, cm):
     elif w["dirs"]:
         kw["reference_directions"] = cm.UserDefinedDirections(cm.two_layer_directions(M, *w["dirs"][1:]))
     algo = cm.Algorithm(w["algo"], population_size=w["N"], max_generations=w["T"],
-                        problem=getattr(cm, kind)(D, M), seed=args.seed, print_progress=False, **kw)
+                        problem=getattr(cm, kind)(D, M), seed=seed, print_progress=False, **kw)
     stream = torch.cuda.current_stream()
     algo.initialize()
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         algo.step()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(args.steps)]
+              for _ in range(steps)]
     torch.cuda.synchronize()
-    with ClockSampler(0) as clocks:
+    with ClockSampler(torch.cuda.current_device()) as clocks:
         for e0, e1 in events:
             flush.fill_(1)
             e0.record(stream)
@@ -531,28 +537,35 @@ def other_workload(args, torch, cm):
         torch.cuda.synchronize()
     total_ms = sum(e0.elapsed_time(e1) for e0, e1 in events)
     graph_on, kernels = algo.graph_info
-    out = {"metric": f"{w['algo']} gen/s", "value": args.steps / (total_ms / 1e3), "unit": "gen/s",
-           "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+    out = {"metric": f"{w['algo']} gen/s", "value": steps / (total_ms / 1e3), "unit": "gen/s",
+           "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": total_ms / steps,
            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
            "config": {"workload": w["desc"], "cuda_graph": graph_on, "kernels_per_generation": kernels,
                       "l2": "flushed (256 MiB write) before every timed generation"},
            "clocks": clocks.summary()}
-    if args.workload in ("dtlz2-m8", "c1dtlz1-m10"):
+    if name in ("dtlz2-m8", "c1dtlz1-m10"):
         out["stages_ms"] = dict(algo.profile_step())
-    if args.workload == "rvea-large-d":
-        # streamed bytes of one generation's variation + evaluation: read the two
-        # parents of every child and write the child (8 N D), read the child for
-        # the objectives (4 N D)
-        stages = dict(algo.profile_step())
-        t = stages.get("variation", 0.0) + stages.get("evaluate", 0.0)
-        bytes_ = 12.0 * w["N"] * D
+    if name == "rvea-large-d":
+        # the generation's streamed bytes, 8 N D: the variation reads two
+        # parents and writes two children per pair element (8 N D); the
+        # evaluation reads the children, the survivor update reads and writes
+        # the surviving rows (both bounded by further 4 N D each, not counted)
+        bytes_ = 8.0 * w["N"] * D
         hbm, kind_ = _peaks()
-        out["stages_ms"] = stages
-        out["roofline"] = {"kernel": "variation_philox + dtlz_block_rows", "bound": "hbm",
-                           "achieved": bytes_ / (t / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
-                           "frac": bytes_ / (t / 1e3) / 1e9 / hbm, "peak_source": kind_,
+        ms = total_ms / steps
+        out["roofline"] = {"kernel": "whole generation (crossover_philox, mutation_philox, dtlz_block_rows, "
+                                     "RVEA selection, rvea_update)", "bound": "hbm",
+                           "achieved": bytes_ / (ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                           "frac": bytes_ / (ms / 1e3) / 1e9 / hbm, "peak_source": kind_,
                            "algorithmic_bytes": bytes_}
-    print(json.dumps(out))
+        out["stages_ms"] = dict(algo.profile_step())
+    del algo
+    torch.cuda.empty_cache()
+    return out
+
+
+def other_workload(args, torch, cm):
+    print(json.dumps(measure_workload(args.workload, args.steps, args.warmup, args.seed, torch, cm)))
 
 
 QUALITY = ("DTLZ2 M=3 D=12, N=1024 (RVEA: 990), 500 generations, seeds 0..29: the reference's published "
@@ -696,6 +709,7 @@ def main() -> None:
     ap.add_argument("--batch-instances", type=int, default=256)
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the association-search comparison")
+    ap.add_argument("--no-rvea", action="store_true", help="skip the RVEA large-D record")
     ap.add_argument("--workload", default="dtlz1-n32768",
                     choices=["dtlz1-n32768", "constrained-batch", "quality", *OTHER_WORKLOADS])
     ap.add_argument("--quality-seeds", type=int, default=30)
@@ -825,9 +839,16 @@ def main() -> None:
     if not args.no_precision:
         precision = precision_form(torch, cm, replica_seed(args.seed, rank))
 
+    # RVEA at large D (the HBM-streaming workload) as a record of the line
+    rvea = None
+    if not args.no_rvea:
+        algo = None
+        torch.cuda.empty_cache()
+        rvea = measure_workload("rvea-large-d", 10, 3, replica_seed(args.seed, rank), torch, cm)
+
     batched = None
     if not args.no_batch:
-        del algo
+        algo = None
         torch.cuda.empty_cache()
         batched = batched_measure(args, torch, cm, world, rank)
 
@@ -860,6 +881,7 @@ def main() -> None:
             "cpu_baseline": cpu,
             "precision_form": precision,
             "batched": batched,
+            "rvea_large_d": rvea,
         }
         print(json.dumps(out))
     if world > 1:
