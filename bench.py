@@ -474,6 +474,10 @@ PRECISION_WORKLOADS = [
      "N": N_POP, "partitions": PARTITIONS, "modes": (0, 1, 2)},
     {"desc": "many objectives: DTLZ2 M=8 D=17 N=6436, 6435 directions", "problem": "DTLZ2", "D": 17, "M": 8,
      "N": 6436, "partitions": 8, "modes": (1, 2)},
+    # the constrained config: below the default's 2^24-pair threshold the
+    # default takes the FP32 scan; both are timed here
+    {"desc": "constrained, ten objectives: C1-DTLZ1 M=10 D=14 N=16384, two-layer (3,2) directions (275)",
+     "problem": "C1DTLZ1", "D": 14, "M": 10, "N": 16384, "two_layer": (3, 2), "modes": (1, 2)},
 ]
 
 
@@ -487,9 +491,10 @@ def precision_form(torch, cm, seed: int, gens: int = 4):
         rec = {"workload": w["desc"], "associate_ms": {}, "identical_runs": True}
         ref = None
         for mode in w["modes"]:
+            dirs = (cm.UserDefinedDirections(cm.two_layer_directions(w["M"], *w["two_layer"]))
+                    if "two_layer" in w else cm.DasDennisDirections(w["partitions"]))
             algo = cm.NSGA3(population_size=w["N"], max_generations=gens + 4, problem=getattr(cm, w["problem"])(w["D"], w["M"]),
-                            reference_directions=cm.DasDennisDirections(w["partitions"]), seed=seed,
-                            print_progress=False,
+                            reference_directions=dirs, seed=seed, print_progress=False,
                             environment_selector=cm.NSGA3EnvironmentSelector(association_mode=mode))
             algo.initialize()
             for _ in range(gens):

@@ -1242,6 +1242,7 @@ struct moea_batch {
     // the schedule: group of each instance (fused mode), and how it was chosen
     std::vector<int> group_of;
     int schedule_source = 0;    // 0 pair-test LPT, 1 autotuned now, 2 autotuned earlier (cache)
+    std::vector<double> inst_cost;  // measured generation of each instance alone (autotuner), or empty
     float tuned_ms = 0.0f;      // measured generation of the chosen schedule (autotuner)
     float default_ms = 0.0f;    // measured generation of the default schedule (autotuner)
     float slowest_ms = 0.0f;    // the slowest instance's generation run alone (autotuner probe)
@@ -1338,6 +1339,10 @@ struct moea_batch {
             std::vector<int> ids;
             for (int i = 0; i < (int)schedule.size(); ++i)
                 if (schedule[i] == gi) ids.push_back(i);
+            // the costliest instances first: a group's CTAs start in this
+            // order, so the long ones do not start last (list scheduling)
+            if (inst_cost.size() == schedule.size())
+                std::stable_sort(ids.begin(), ids.end(), [&](int x, int y) { return inst_cost[x] > inst_cost[y]; });
             if (ids.empty()) continue;
             FusedGroup g;
             MOEA_TRY(fused_build_group(inst, ids, g));
@@ -1421,14 +1426,17 @@ struct moea_batch {
 
     // Runs `warm` generations, measures every instance alone, then times the
     // pair-test LPT schedule of the default group count and measured-cost LPT
-    // schedules of 4..count groups; *chosen receives the fastest.
+    // schedules of 1, 2, 4, ... count groups (instances in a group ordered by
+    // cost, costliest first); *chosen receives the fastest.
     int autotune(int warm, std::vector<int>* chosen, float* chosen_ms, float* dflt_ms, float* slowest,
-                 float* serial)
+                 float* serial, std::vector<double>* cost_out)
     {
         const int count = (int)inst.size();
         for (int g = 0; g < warm && generation < T - 1; ++g) MOEA_TRY(step());
         std::vector<double> measured;
         MOEA_TRY(probe_costs(measured));
+        *cost_out = measured;
+        inst_cost = measured;
         *slowest = (float)*std::max_element(measured.begin(), measured.end());
         double total = 0.0;
         for (double c : measured) total += c;
@@ -1437,7 +1445,7 @@ struct moea_batch {
         for (int i = 0; i < count; ++i) pairs[i] = (double)inst[i]->N * inst[i]->N;
         std::vector<std::vector<int>> cands;
         cands.push_back(lpt(pairs, std::max(1, std::min(fused_groups, count))));
-        for (int G = 4; G <= count; G *= 2) cands.push_back(lpt(measured, G));
+        for (int G = 1; G <= count; G *= 2) cands.push_back(lpt(measured, G));
         if ((count & (count - 1)) != 0) cands.push_back(lpt(measured, count));
         float best = 1e30f;
         for (size_t c = 0; c < cands.size(); ++c) {
@@ -1535,6 +1543,7 @@ namespace {
 
 struct TunedSchedule {
     std::vector<int> schedule;
+    std::vector<double> cost;  // each instance's generation alone
     float tuned_ms = 0.0f, default_ms = 0.0f, slowest_ms = 0.0f, serial_ms = 0.0f;
 };
 
@@ -1643,6 +1652,7 @@ moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void
         std::lock_guard<std::mutex> lock(tuning_mutex());
         auto it = tuning_cache().find(key);
         if (it != tuning_cache().end()) {
+            b->inst_cost = it->second.cost;
             st = b->setup_fused(&it->second.schedule);
             b->schedule_source = 2;
             b->tuned_ms = it->second.tuned_ms;
@@ -1655,11 +1665,12 @@ moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void
             TunedSchedule ts;
             if (st == MOEA_OK) {
                 st = scratch->autotune(std::min(10, T / 4), &ts.schedule, &ts.tuned_ms, &ts.default_ms,
-                                       &ts.slowest_ms, &ts.serial_ms);
+                                       &ts.slowest_ms, &ts.serial_ms, &ts.cost);
                 delete scratch;
             }
             if (st == MOEA_OK) {
                 tuning_cache()[key] = ts;
+                b->inst_cost = ts.cost;
                 st = b->setup_fused(&ts.schedule);
                 b->schedule_source = 1;
                 b->tuned_ms = ts.tuned_ms;
