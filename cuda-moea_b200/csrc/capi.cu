@@ -206,6 +206,15 @@ void moea_workspace_destroy(moea_workspace* ws)
 
 size_t moea_workspace_bytes(const moea_workspace* ws) { return ws ? ws->ws.bytes : 0; }
 
+moea_status moea_workspace_set_peel(moea_workspace* w, int mode)
+{
+    CHECK_WS(w);
+    if (mode != MOEA_PEEL_AUTO && mode != MOEA_PEEL_GENERAL)
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "set_peel: mode %d", mode);
+    w->ws.peel_general = mode == MOEA_PEEL_GENERAL;
+    return MOEA_OK;
+}
+
 moea_status moea_ndsort(moea_workspace* w, const float* d_cv, const float* d_objs, int M, int n,
                         int target, int* d_fronts, int* h_max_front, void* stream)
 {

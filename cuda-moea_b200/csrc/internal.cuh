@@ -82,6 +82,7 @@ struct Workspace {
     int peel_owned_grid = 0;        // CTAs of the lane-owned peel (one per SM), 0 if unavailable
     int peel_smem = 0;
     bool peel_single_cta = false;   // peel with one ordinary CTA (instances of a batch)
+    bool peel_general = false;      // always the general peel (moea_workspace_set_peel)
     uint32_t* peel_fmask = nullptr; // [3][words] members of the last three fronts (peel)
 
     // --- NSGA-III stages ---

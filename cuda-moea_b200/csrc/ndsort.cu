@@ -1714,7 +1714,7 @@ int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_f
     cfg.numAttrs = 1;
     // lane-owned points when every warp of the grid holds at most one group
     // of 32 positions and the rows are 16-byte aligned
-    const bool owned = ws.peel_owned_grid > 0 && ceil_div(n, 32) <= 32 * min(grid, ws.peel_owned_grid) &&
+    const bool owned = !ws.peel_general && ws.peel_owned_grid > 0 && ceil_div(n, 32) <= 32 * min(grid, ws.peel_owned_grid) &&
                        Wp >= kWin && (Wp & 3) == 0;
     if (owned) {
         if (grid > ws.peel_owned_grid) grid = ws.peel_owned_grid;

@@ -40,6 +40,10 @@ class Workspace:
     def nbytes(self) -> int:
         return int(lib().moea_workspace_bytes(self.handle))
 
+    def set_peel(self, general: bool) -> None:
+        """True: every sort takes the general peel; False: the automatic choice."""
+        check(lib().moea_workspace_set_peel(self.handle, 1 if general else 0))
+
     def close(self) -> None:
         if getattr(self, "handle", None) is not None and self.handle.value:
             lib().moea_workspace_destroy(self.handle)

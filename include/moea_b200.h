@@ -64,6 +64,14 @@ void moea_workspace_destroy(moea_workspace* ws);
 /* Bytes of device memory held by the workspace (the reference's selector scratch
  * pool, nat/src/selection/nsga3/kernels/dynamic_workspace.cu, reports none). */
 size_t moea_workspace_bytes(const moea_workspace* ws);
+/* Front-peeling kernel of the workspace's sorts: MOEA_PEEL_AUTO (default) takes
+ * the lane-owned peel whenever every warp of the grid holds at most one group
+ * of 32 points (up to 151,552 merged points on a B200) and the general peel
+ * beyond; MOEA_PEEL_GENERAL always takes the general one.  Both give the same
+ * fronts.  No counterpart in the reference (one peel path there). */
+#define MOEA_PEEL_AUTO 0
+#define MOEA_PEEL_GENERAL 1
+moea_status moea_workspace_set_peel(moea_workspace* ws, int mode);
 
 /* ========================================================================
  * Stage-level entry points (one hot-path stage each).

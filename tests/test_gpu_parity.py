@@ -119,6 +119,36 @@ def test_ndsort_full_size_many_fronts(st, oracle, M, n, feasible_share):
         w.close()
 
 
+@pytest.mark.parametrize("M,n,kind,cvmode", [(3, 65536, "dtlz1-thin", "feasible"), (5, 40000, "dtlz1-thin", "mixed"),
+                                            (3, 16000, "dtlz1", "mostly_infeasible"), (8, 1024, "uniform", "mixed"),
+                                            (3, 900, "ties", "nan"), (2, 97, "uniform", "all_infeasible")])
+def test_ndsort_general_and_lane_owned_peels_agree(st, oracle, M, n, kind, cvmode):
+    """The two peel kernels (the lane-owned one, default up to 151,552 points,
+    and the general one beyond) give the same fronts as the oracle on the same
+    inputs, from thin-front full-size sorts down to single-CTA grids."""
+    rng = np.random.default_rng(n * 7 + M)
+    if kind == "dtlz1-thin":
+        x = rng.random((n, M + 4)).astype(np.float32)
+        x[:, M - 1:] = (0.5 + 0.02 * rng.standard_normal((n, 5))).astype(np.float32)
+        objs, _ = oracle.evaluate("DTLZ1", x, M)
+    else:
+        objs = _population(rng, M, n, kind)
+    if cvmode == "nan":
+        objs[rng.integers(0, M), rng.integers(0, n, 2)] = np.nan
+    cv = _cv(rng, n, cvmode)
+    target = max(1, n // 2)
+    want, wmf = oracle.ndsort(cv, objs, target)
+    w = st.Workspace(max_points=n, max_objectives=M, max_directions=1)
+    try:
+        for general in (False, True, False):
+            w.set_peel(general)
+            got, gmf = st.ndsort(w, _t(cv), _t(objs), target)
+            np.testing.assert_array_equal(got.cpu().numpy(), want)
+            assert gmf == wmf
+    finally:
+        w.close()
+
+
 def test_ndsort_all_mutually_nondominated(st, ws, oracle):
     # points on a line f1 = 1 - f0: no dominance pair at all (the reference's
     # CSR queue path leaves every front at -1 in this case; the relation gives front 0)
