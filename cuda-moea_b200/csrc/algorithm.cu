@@ -1152,6 +1152,7 @@ int fused_build_group(const std::vector<moea_algorithm*>& inst, const std::vecto
     g.count = (int)ids.size();
     for (int i : ids) {
         g.max_n = std::max(g.max_n, 2 * inst[i]->N);
+        g.max_W = std::max(g.max_W, inst[i]->ws.words);
         g.max_N = std::max(g.max_N, inst[i]->N);
         g.max_D = std::max(g.max_D, inst[i]->D);
         g.max_M = std::max(g.max_M, inst[i]->M);

@@ -292,6 +292,7 @@ struct FusedBucket {
 // its instance ids, size bounds and per-M buckets.
 struct FusedGroup {
     int count = 0, max_n = 0, max_N = 0, max_D = 0, max_M = 0;
+    int max_W = 0;                       // largest row stride (words) of the group's workspaces
     int* d_ids = nullptr;                // (count) instance indices
     std::vector<FusedBucket> buckets;    // per objective count
 };

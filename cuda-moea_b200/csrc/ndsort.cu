@@ -1803,14 +1803,16 @@ int fused_tile_blocks(int M, int n)
     }
 }
 
-size_t fused_peel_smem(int n) { return (size_t)ceil_div(n, 32) * sizeof(uint32_t) + 3 * (size_t)n * sizeof(int); }
+// U takes the workspace's row words W (4 * ceil(n / 128) for a workspace of n
+// merged points), then blockers, front list and queue of n entries each.
+size_t fused_peel_smem(int W, int n) { return (size_t)W * sizeof(uint32_t) + 3 * (size_t)n * sizeof(int); }
 
 int fused_ndsort_configure()
 {
     MOEA_CUDA_TRY(cudaFuncSetAttribute(fused_lexsort, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sizeof(FusedSortStorage)));
     MOEA_CUDA_TRY(cudaFuncSetAttribute(fused_peel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)fused_peel_smem(kFusedMaxPoints)));
+                                       (int)fused_peel_smem(4 * ceil_div(kFusedMaxPoints, 128), kFusedMaxPoints)));
     return MOEA_OK;
 }
 
@@ -1835,7 +1837,7 @@ int fused_ndsort(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s)
         }
     }
     MOEA_CUDA_TRY(cudaGetLastError());
-    fused_peel<<<g.count, kFusedPeelThreads, fused_peel_smem(g.max_n), s>>>(d_inst, g.d_ids);
+    fused_peel<<<g.count, kFusedPeelThreads, fused_peel_smem(g.max_W, g.max_n), s>>>(d_inst, g.d_ids);
     fused_scatter<<<dim3(ceil_div(g.max_n, 256), g.count), 256, 0, s>>>(d_inst, g.d_ids);
     MOEA_CUDA_TRY(cudaGetLastError());
     return MOEA_OK;
