@@ -236,7 +236,8 @@ def _reference_gpu_record(steps: int):
     complete NSGA-III generation (all of its native sources compiled in place
     into oracle/_ref/libmoea_ref_algo.so, built through its C++ builder, each
     step bracketed by device synchronises) on the headline and the small
-    workload, and its stage functions (oracle/_ref/libmoea_ref.so) timed with
+    workload, looped over a sample of the batched workload's instances, and
+    its stage functions (oracle/_ref/libmoea_ref.so) timed with
     CUDA events on the fixed generation-0 merged population of
     stage_population."""
     try:
@@ -258,6 +259,15 @@ def _reference_gpu_record(steps: int):
             rec["algorithm"].append({"workload": desc, "steps": k, "warmup": warm,
                                      "gen_per_s": k / (sum(ms) / 1e3),
                                      "ms_per_gen_median": statistics.median(ms)})
+        # the batched workload: the reference runs one algorithm at a time, so
+        # its rate is the instances looped; every 8th instance, 5 steps each
+        specs = batch_specs(256)[::8]
+        tot_ms, steps_b = 0.0, 5
+        for kind, M, N, D, seed in specs:
+            tot_ms += sum(R.algo_time(0, kind, D, M, N, 0, 200, 1.0, seed, 3, steps_b))
+        rec["batched_looped"] = {"workload": BATCH_WORKLOAD, "sample": f"{len(specs)} of the 256 instances "
+                                 f"(every 8th), {steps_b} generations each after 3 warm-up",
+                                 "instance_gen_per_s": len(specs) * steps_b / (tot_ms / 1e3)}
         # stages on the fixed population
         from oracle import oracle as O
         x = stage_population(N_POP)
