@@ -45,9 +45,9 @@ METRIC = "NSGA-III gen/s @N=32768,M=3; batched instance-gen/s vs plain, identica
 WORKLOAD = "NSGA-III DTLZ1 M=3 D=7 N=32768, Das-Dennis H=254 (32640 directions), 1 generation per step"
 N_POP, D_VAR, M_OBJ, PARTITIONS = 32768, 7, 3, 254
 TILES_DRAM_BYTES = 3.00e6 + 210.55e6
-# dram__bytes_read.sum + dram__bytes_write.sum of one nds_peel launch at this
-# workload (ncu --set full, profiles/nds_peel_dtlz1_n65536.md)
-PEEL_DRAM_BYTES = 124.3e6 + 3.7e6
+# dram__bytes_read.sum + dram__bytes_write.sum of one nds_peel_owned launch at
+# this workload (ncu --set full, profiles/nds_peel_owned_dtlz1_n65536.md)
+PEEL_DRAM_BYTES = 132.83e6 + 3.92e6
 # warp instructions nds_tiles issues per (warp, 32-position word) step: one
 # step tests 32 x 32 ordered pairs (ncu instruction count,
 # profiles/nds_tiles_dtlz1_n65536.md)
@@ -134,7 +134,7 @@ def kernel_rooflines(stage_ms: dict, n_mix: int, headline: bool):
     peel = stage_ms.get("ndsort.peel")
     if peel:
         a = rel_bytes / (peel / 1e3) / 1e9
-        out.append({"kernel": "nds_peel (front peeling)", "bound": "hbm", "achieved": a, "peak": hbm,
+        out.append({"kernel": "nds_peel_owned (front peeling)", "bound": "hbm", "achieved": a, "peak": hbm,
                     "unit": "GB/s", "frac": a / hbm, "peak_source": peak_kind, "algorithmic_bytes": rel_bytes,
                     "traffic": PEEL_DRAM_BYTES if headline else None, "ms": peel})
     tiles = stage_ms.get("ndsort.dominance_tiles")
