@@ -44,13 +44,14 @@ sys.path.insert(0, str(ROOT))
 METRIC = "NSGA-III gen/s @N=32768,M=3; batched instance-gen/s vs plain, identical ranks"
 WORKLOAD = "NSGA-III DTLZ1 M=3 D=7 N=32768, Das-Dennis H=254 (32640 directions), 1 generation per step"
 N_POP, D_VAR, M_OBJ, PARTITIONS = 32768, 7, 3, 254
+# dram__bytes_read.sum + dram__bytes_write.sum of one nds_tiles launch
 TILES_DRAM_BYTES = 3.00e6 + 210.55e6
 # dram__bytes_read.sum + dram__bytes_write.sum of one nds_peel_owned launch at
 # this workload (one ncu --set full capture of the launch)
 PEEL_DRAM_BYTES = 132.83e6 + 3.92e6
 # warp instructions nds_tiles issues per (warp, 32-position word) step: one
-# step tests 32 x 32 ordered pairs (ncu instruction count,
-# of one launch at this workload)
+# step tests 32 x 32 ordered pairs (ncu instruction count of one launch at
+# this workload)
 TILES_WARP_INSTR_PER_STEP = 97
 
 
