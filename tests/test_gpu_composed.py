@@ -214,3 +214,10 @@ def test_reference_custom_strategy_smoke():
     # selecting the parents again: the population never changes
     x = result.variables
     torch.testing.assert_close(result.objectives, torch.stack((x.square().sum(1), (x - 1).square().sum(1)), 1))
+
+
+def test_composed_builtins_equal_algorithm_rvea_more_directions_than_points():
+    # 91 directions for 30 points: more winners than survivors, the truncation
+    # by (flag, metric, index) of the elitism
+    _lockstep(lambda: cm.RVEA(population_size=30, max_generations=10, problem=cm.DTLZ2(12, 3), seed=3,
+                              reference_directions=cm.DasDennisDirections(12), print_progress=False), 8)
