@@ -453,7 +453,8 @@ def batched_measure(args, torch, cm, world: int = 1, rank: int = 0):
            "graph_kernels_per_generation": batch.graph_kernels,
            "schedule": {"groups": sched["groups"], "source": sched["source"], "tuned_ms": sched["tuned_ms"],
                         "default_ms": sched["default_ms"], "slowest_instance_ms": sched["slowest_instance_ms"],
-                        "instances_serial_ms": sched["instances_serial_ms"], "tuning_and_setup_s": tune_s},
+                        "instances_serial_ms": sched["instances_serial_ms"], "tuning_and_setup_s": tune_s,
+                        "half_width_tiles_for_M": sched["half_tiles"]},
            "pair_tests_per_generation": sum((2 * s[2]) ** 2 for s in all_specs),
            "sharding": f"{world} rank(s), instances balanced by pair tests"}
     batch.close()

@@ -15,6 +15,7 @@
 //  - buffers are allocated once at initialisation (no per-generation pool
 //    allocation, dynamic_workspace.cu:3-125).
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -194,7 +195,8 @@ namespace {
 // rotation, and the launch plan of a group of instances.
 bool fused_eligible(const moea_algorithm* a);
 BatchInst fused_describe(moea_algorithm* a, int P, int X);
-int fused_build_group(const std::vector<moea_algorithm*>& inst, const std::vector<int>& ids, FusedGroup& g);
+int fused_build_group(const std::vector<moea_algorithm*>& inst, const std::vector<int>& ids, FusedGroup& g,
+                      const int* tile_shape = nullptr);
 void fused_free_group(FusedGroup& g);
 }  // namespace
 
@@ -1146,7 +1148,10 @@ BatchInst fused_describe(moea_algorithm* a, int P, int X)
     return b;
 }
 
-int fused_build_group(const std::vector<moea_algorithm*>& inst, const std::vector<int>& ids, FusedGroup& g)
+// tile_shape[m]: the dominance tile shape of the instances with m objectives
+// (nullptr: shape 0 for all).
+int fused_build_group(const std::vector<moea_algorithm*>& inst, const std::vector<int>& ids, FusedGroup& g,
+                      const int* tile_shape)
 {
     g = FusedGroup{};
     g.count = (int)ids.size();
@@ -1162,11 +1167,12 @@ int fused_build_group(const std::vector<moea_algorithm*>& inst, const std::vecto
     for (int m = 1; m <= kMaxObjectives; ++m) {
         std::vector<int> bids, prefix{0};
         int mn = 0;
+        const int shape = tile_shape ? tile_shape[m] : 0;
         for (int i : ids) {
             if (inst[i]->M != m) continue;
             bids.push_back(i);
             const int n = 2 * inst[i]->N;
-            prefix.push_back(prefix.back() + fused_tile_blocks(m, n));
+            prefix.push_back(prefix.back() + fused_tile_blocks(m, n, shape));
             mn = std::max(mn, n);
         }
         if (bids.empty()) continue;
@@ -1175,6 +1181,7 @@ int fused_build_group(const std::vector<moea_algorithm*>& inst, const std::vecto
         b.count = (int)bids.size();
         b.max_n = mn;
         b.tile_blocks = prefix.back();
+        b.shape = shape;
         MOEA_CUDA_TRY(cudaMalloc((void**)&b.d_ids, sizeof(int) * bids.size()));
         MOEA_CUDA_TRY(cudaMalloc((void**)&b.d_tile_prefix, sizeof(int) * prefix.size()));
         MOEA_CUDA_TRY(cudaMemcpy(b.d_ids, bids.data(), sizeof(int) * bids.size(), cudaMemcpyHostToDevice));
@@ -1242,6 +1249,7 @@ struct moea_batch {
     int graph_kernels = 0;
     // the schedule: group of each instance (fused mode), and how it was chosen
     std::vector<int> group_of;
+    std::array<int, kMaxObjectives + 1> tile_shape{};  // dominance tile shape per objective count
     int schedule_source = 0;    // 0 pair-test LPT, 1 autotuned now, 2 autotuned earlier (cache)
     std::vector<double> inst_cost;  // measured generation of each instance alone (autotuner), or empty
     float tuned_ms = 0.0f;      // measured generation of the chosen schedule (autotuner)
@@ -1346,7 +1354,7 @@ struct moea_batch {
                 std::stable_sort(ids.begin(), ids.end(), [&](int x, int y) { return inst_cost[x] > inst_cost[y]; });
             if (ids.empty()) continue;
             FusedGroup g;
-            MOEA_TRY(fused_build_group(inst, ids, g));
+            MOEA_TRY(fused_build_group(inst, ids, g, tile_shape.data()));
             groups.push_back(std::move(g));
             cudaStream_t gs = nullptr;
             cudaEvent_t ge = nullptr;
@@ -1375,7 +1383,7 @@ struct moea_batch {
         int st = MOEA_OK;
         for (int i = 0; i < count && st == MOEA_OK; ++i) {
             FusedGroup g;
-            st = fused_build_group(inst, std::vector<int>{i}, g);
+            st = fused_build_group(inst, std::vector<int>{i}, g, tile_shape.data());
             if (st != MOEA_OK) break;
             cudaEventRecord(e0, stream);
             st = fused_reproduce(d_inst[parity], g, stream);
@@ -1428,9 +1436,12 @@ struct moea_batch {
     // Runs `warm` generations, measures every instance alone, then times the
     // pair-test LPT schedule of the default group count and measured-cost LPT
     // schedules of 1, 2, 4, ... count groups (instances in a group ordered by
-    // cost, costliest first); *chosen receives the fastest.
+    // cost, costliest first); *chosen receives the fastest.  Then, on the
+    // chosen schedule, each objective count present tries the second
+    // dominance tile shape and keeps it where the generation got faster;
+    // *shapes receives the result.
     int autotune(int warm, std::vector<int>* chosen, float* chosen_ms, float* dflt_ms, float* slowest,
-                 float* serial, std::vector<double>* cost_out)
+                 float* serial, std::vector<double>* cost_out, std::array<int, kMaxObjectives + 1>* shapes)
     {
         const int count = (int)inst.size();
         for (int g = 0; g < warm && generation < T - 1; ++g) MOEA_TRY(step());
@@ -1458,6 +1469,17 @@ struct moea_batch {
                 *chosen = cands[c];
             }
         }
+        for (int m = 1; m <= kMaxObjectives; ++m) {
+            bool present = false;
+            for (moea_algorithm* a : inst) present |= a->M == m;
+            if (!present) continue;
+            tile_shape[m] = 1;
+            float ms = 0.0f;
+            MOEA_TRY(time_schedule(*chosen, 3, &ms));
+            if (ms < best) best = ms;
+            else tile_shape[m] = 0;
+        }
+        *shapes = tile_shape;
         *chosen_ms = best;
         return MOEA_OK;
     }
@@ -1544,6 +1566,7 @@ namespace {
 
 struct TunedSchedule {
     std::vector<int> schedule;
+    std::array<int, kMaxObjectives + 1> tile_shape{};
     std::vector<double> cost;  // each instance's generation alone
     float tuned_ms = 0.0f, default_ms = 0.0f, slowest_ms = 0.0f, serial_ms = 0.0f;
 };
@@ -1608,6 +1631,7 @@ moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void
     b->device = device;
     b->T = T;
     b->use_fused = (flags & MOEA_BATCH_NO_FUSION) == 0;
+    if (flags & MOEA_BATCH_HALF_TILES) b->tile_shape.fill(1);
     if (((flags >> 8) & 0xFF) > 0) b->fused_groups = (flags >> 8) & 0xFF;
     int st = MOEA_OK;
     cudaError_t ce = cudaSuccess;
@@ -1654,6 +1678,7 @@ moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void
         auto it = tuning_cache().find(key);
         if (it != tuning_cache().end()) {
             b->inst_cost = it->second.cost;
+            b->tile_shape = it->second.tile_shape;
             st = b->setup_fused(&it->second.schedule);
             b->schedule_source = 2;
             b->tuned_ms = it->second.tuned_ms;
@@ -1666,12 +1691,13 @@ moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void
             TunedSchedule ts;
             if (st == MOEA_OK) {
                 st = scratch->autotune(std::min(10, T / 4), &ts.schedule, &ts.tuned_ms, &ts.default_ms,
-                                       &ts.slowest_ms, &ts.serial_ms, &ts.cost);
+                                       &ts.slowest_ms, &ts.serial_ms, &ts.cost, &ts.tile_shape);
                 delete scratch;
             }
             if (st == MOEA_OK) {
                 tuning_cache()[key] = ts;
                 b->inst_cost = ts.cost;
+                b->tile_shape = ts.tile_shape;
                 st = b->setup_fused(&ts.schedule);
                 b->schedule_source = 1;
                 b->tuned_ms = ts.tuned_ms;
@@ -1703,6 +1729,17 @@ moea_status moea_batch_schedule(moea_batch* b, int* h_groups, int* h_source, flo
     if (h_default_ms) *h_default_ms = b->default_ms;
     if (h_group_of)
         for (size_t i = 0; i < b->inst.size(); ++i) h_group_of[i] = i < b->group_of.size() ? b->group_of[i] : -1;
+    return MOEA_OK;
+}
+
+moea_status moea_batch_tile_shapes(moea_batch* b, int* h_shapes, int cap)
+{
+    if (!b || (!h_shapes && cap > 0) || cap < 0) return set_error(MOEA_ERR_INVALID_ARGUMENT, "tile shapes: bad arguments");
+    for (int m = 0; m < cap; ++m) {
+        bool present = false;
+        for (moea_algorithm* a : b->inst) present |= a->M == m;
+        h_shapes[m] = (present && m <= kMaxObjectives && b->fused) ? b->tile_shape[m] : 0;
+    }
     return MOEA_OK;
 }
 

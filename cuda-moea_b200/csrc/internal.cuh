@@ -284,6 +284,7 @@ struct BatchInst {
 // Launch plan of one M value: instance ids and the prefix of their tile blocks.
 struct FusedBucket {
     int M = 0, count = 0, max_n = 0, tile_blocks = 0;
+    int shape = 0;                 // dominance tile shape (fused_tile_blocks)
     int* d_ids = nullptr;          // (count) instance indices
     int* d_tile_prefix = nullptr;  // (count + 1) first tile block of each instance
 };
@@ -301,7 +302,8 @@ int fused_reproduce(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s
 int fused_evaluate(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s);
 int fused_ndsort(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s);
 int fused_select(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s);
-int fused_tile_blocks(int M, int n);  // tile CTAs of one instance
+int fused_tile_blocks(int M, int n, int shape);  // tile CTAs of one instance in a tile shape (0, 1)
+constexpr int kTileShapes = 2;
 // Kernel attributes (shared memory opt-in) of the fused stages, set once per
 // device before any capture.
 int fused_ndsort_configure();

@@ -334,6 +334,14 @@ struct TileCfg {
     static constexpr int kMF = (M > 1) ? M - 1 : 1;   // objectives 1..M-1
 };
 
+// Words per tile CTA of a tile shape: shape 0 is TileCfg's, shape 1 half of
+// it (twice the CTAs, each with half the staged word tables).  The batch's
+// autotuner picks the shape per objective count by measured time.
+template <int M, int S>
+struct TileShape {
+    static constexpr int kPW = S == 0 ? TileCfg<M>::kPW : TileCfg<M>::kPW / 2;
+};
+
 // Count of the 32 ascending keys at shared address a that are <= v, as the
 // byte offset 4 * count: binary search with steps of 16, 8, 4, 2, 1 keys and
 // a last probe that reaches 32 only from 31.  Each probe is one shared load
@@ -372,14 +380,13 @@ __device__ __forceinline__ uint32_t ld_shared_u32(uint32_t a)
 // coalesced row segments.  The epilogue raises blocker[q] to the highest
 // dominator position seen, so that after the kernel blocker[q] == -1 exactly
 // for the points that nothing dominates (front 0).
-template <int M>
+template <int M, int PW = TileCfg<M>::kPW>
 __device__ __forceinline__ void tile_block(int bx, int by, const float* __restrict__ sf, int sf_stride,
                                            const int* __restrict__ qinfo,
                                            const uint32_t* __restrict__ ckeys,
                                            const uint32_t* __restrict__ cbits, int n, int W, int Wc,
                                            uint32_t* __restrict__ rows, int* __restrict__ blocker)
 {
-    constexpr int PW = TileCfg<M>::kPW;
     constexpr int MF = TileCfg<M>::kMF;
     const int q0 = by * kQB;
     if (q0 >= n) return;
@@ -1398,7 +1405,7 @@ __global__ void fused_chunks(const BatchInst* __restrict__ insts, const int* __r
 
 // Tile CTAs of all instances with M objectives, flattened: CTA b belongs to
 // the instance whose range [prefix[k], prefix[k+1]) contains b.
-template <int M>
+template <int M, int S>
 __global__ void __launch_bounds__(kTileThreads)
 fused_tiles(const BatchInst* __restrict__ insts, const int* __restrict__ ids,
             const int* __restrict__ prefix, int count)
@@ -1411,10 +1418,11 @@ fused_tiles(const BatchInst* __restrict__ insts, const int* __restrict__ ids,
     }
     const BatchInst& I = insts[__ldg(ids + lo)];
     const int maxw = (I.n + 31) >> 5;
-    const int gx = (maxw + TileCfg<M>::kPW - 1) / TileCfg<M>::kPW;
+    constexpr int PW = TileShape<M, S>::kPW;
+    const int gx = (maxw + PW - 1) / PW;
     const int lb = b - __ldg(prefix + lo);
-    tile_block<M>(lb % gx, lb / gx, I.sorted_f, I.n_max, I.qinfo, I.chunk_keys, I.chunk_bits, I.n, I.W, maxw,
-                  I.rows, I.blocker);
+    tile_block<M, PW>(lb % gx, lb / gx, I.sorted_f, I.n_max, I.qinfo, I.chunk_keys, I.chunk_bits, I.n, I.W, maxw,
+                      I.rows, I.blocker);
 }
 
 constexpr int kFusedPeelThreads = 1024;
@@ -1572,16 +1580,20 @@ __global__ void fused_scatter(const BatchInst* __restrict__ insts, const int* __
 }
 
 template <int M>
-int tile_blocks_of(int n)
+int tile_blocks_of(int n, int shape)
 {
     const int maxw = ceil_div(n, 32);
-    return ceil_div(maxw, TileCfg<M>::kPW) * ceil_div(n, kQB);
+    const int pw = shape == 0 ? TileShape<M, 0>::kPW : TileShape<M, 1>::kPW;
+    return ceil_div(maxw, pw) * ceil_div(n, kQB);
 }
 
 template <int M>
 void launch_fused_tiles(const BatchInst* d_inst, const FusedBucket& b, cudaStream_t s)
 {
-    fused_tiles<M><<<b.tile_blocks, kTileThreads, 0, s>>>(d_inst, b.d_ids, b.d_tile_prefix, b.count);
+    if (b.shape == 0)
+        fused_tiles<M, 0><<<b.tile_blocks, kTileThreads, 0, s>>>(d_inst, b.d_ids, b.d_tile_prefix, b.count);
+    else
+        fused_tiles<M, 1><<<b.tile_blocks, kTileThreads, 0, s>>>(d_inst, b.d_ids, b.d_tile_prefix, b.count);
 }
 
 // Self-test of the peel's two barrier waits with a short limit: every CTA
@@ -1790,10 +1802,10 @@ int configure_peel(Workspace& ws)
     return MOEA_OK;
 }
 
-int fused_tile_blocks(int M, int n)
+int fused_tile_blocks(int M, int n, int shape)
 {
     switch (M) {
-#define MOEA_TB_CASE(K) case K: return tile_blocks_of<K>(n);
+#define MOEA_TB_CASE(K) case K: return tile_blocks_of<K>(n, shape);
     MOEA_TB_CASE(1) MOEA_TB_CASE(2) MOEA_TB_CASE(3) MOEA_TB_CASE(4)
     MOEA_TB_CASE(5) MOEA_TB_CASE(6) MOEA_TB_CASE(7) MOEA_TB_CASE(8)
     MOEA_TB_CASE(9) MOEA_TB_CASE(10) MOEA_TB_CASE(11) MOEA_TB_CASE(12)

@@ -207,6 +207,7 @@ _SIGNATURES = [
     ("moea_batch_info", c_int, [vp, ip, ip, ip, ip]),
     ("moea_batch_view", c_int, [vp, c_int, ctypes.POINTER(PopulationViewC)]),
     ("moea_batch_schedule", c_int, [vp, ip, ip, fp, fp, fp, fp, ip]),
+    ("moea_batch_tile_shapes", c_int, [vp, ip, c_int]),
 ]
 
 SYMBOLS = [s[0] for s in _SIGNATURES]

@@ -22,11 +22,13 @@ class Batch:
     mating, same device and max_generations) as one batch."""
 
     def __init__(self, algorithms: Sequence[Algorithm], *, fuse: bool = True, groups: int = 0,
-                 autotune: bool = False):
+                 autotune: bool = False, half_tiles: bool = False):
         """``groups`` fixes the number of graph branches of the fused
-        generation; ``autotune`` lets the library choose the schedule by
-        timing candidates on a scratch copy of the batch (MOEA_BATCH_AUTOTUNE;
-        cached per instance mix).  Results never depend on either."""
+        generation; ``autotune`` lets the library choose the schedule and the
+        dominance tile shape per objective count by timing candidates on a
+        scratch copy of the batch (MOEA_BATCH_AUTOTUNE; cached per instance
+        mix); ``half_tiles`` uses half-width dominance tiles throughout
+        (MOEA_BATCH_HALF_TILES).  Results never depend on any of them."""
         if not algorithms:
             raise ValueError("Batch needs at least one algorithm")
         n = len(algorithms)
@@ -45,8 +47,10 @@ class Batch:
         with torch.cuda.device(self._device):
             self.stream = torch.cuda.Stream(self._device)
         handle = ctypes.c_void_p()
-        # MOEA_BATCH_NO_FUSION = 1; MOEA_BATCH_GROUPS(g) = g << 8 (0: library default)
-        flags = (0 if fuse else 1) | ((int(groups) & 0xFF) << 8) | (2 if autotune else 0)
+        # MOEA_BATCH_NO_FUSION = 1, MOEA_BATCH_AUTOTUNE = 2, MOEA_BATCH_HALF_TILES = 4;
+        # MOEA_BATCH_GROUPS(g) = g << 8 (0: library default)
+        flags = ((0 if fuse else 1) | ((int(groups) & 0xFF) << 8) | (2 if autotune else 0)
+                 | (4 if half_tiles else 0))
         check(lib().moea_batch_create(cfgs, n, ctypes.c_void_p(self.stream.cuda_stream), flags,
                                       ctypes.byref(handle)))
         self._handle = handle
@@ -113,9 +117,12 @@ class Batch:
         group_of = (ctypes.c_int * self._count)()
         check(lib().moea_batch_schedule(self._handle, ctypes.byref(g), ctypes.byref(src), ctypes.byref(t),
                                         ctypes.byref(d), ctypes.byref(slow), ctypes.byref(ser), group_of))
+        shapes = (ctypes.c_int * 17)()
+        check(lib().moea_batch_tile_shapes(self._handle, shapes, 17))
         return {"groups": g.value, "source": ("default", "autotuned", "autotuned (cached)")[src.value],
                 "tuned_ms": t.value, "default_ms": d.value, "slowest_instance_ms": slow.value,
-                "instances_serial_ms": ser.value, "group_of": list(group_of)}
+                "instances_serial_ms": ser.value, "group_of": list(group_of),
+                "half_tiles": [m for m in range(17) if shapes[m]]}
 
     def _view_struct(self, index: int) -> PopulationViewC:
         v = PopulationViewC()

@@ -569,11 +569,17 @@ typedef struct moea_batch moea_batch;
 /* Autotuned schedule (fused mode, unless MOEA_BATCH_GROUPS is given): a
  * scratch copy of the batch runs min(10, max_generations/4) generations, times
  * every instance's fused generation alone, then times the default schedule and
- * longest-processing-time schedules on those measured costs for 4, 8, ...
- * groups (graph branches); the fastest is used.  The choice is cached per
+ * longest-processing-time schedules on those measured costs for 1, 2, 4, ...
+ * groups (graph branches); the fastest is used.  On that schedule each
+ * objective count present then tries the half-width dominance tiles (below)
+ * and keeps them where the generation got faster.  The choice is cached per
  * device and instance mix for the life of the process.  Results do not depend
- * on the schedule. */
+ * on the schedule or the tile shape. */
 #define MOEA_BATCH_AUTOTUNE 2
+/* Fused mode: half-width dominance tiles for every objective count (twice the
+ * tile CTAs, each staging half the word tables).  Without it, and without
+ * MOEA_BATCH_AUTOTUNE, every objective count uses the full-width tiles. */
+#define MOEA_BATCH_HALF_TILES 4
 #define MOEA_BATCH_GROUPS(g) (((g) & 0xFF) << 8)
 moea_status moea_batch_create(const moea_algorithm_config* cfgs, int count, void* stream, int flags,
                               moea_batch** out);
@@ -594,6 +600,11 @@ moea_status moea_batch_info(moea_batch* b, int* h_count, int* h_generation, int*
  * reference. */
 moea_status moea_batch_schedule(moea_batch* b, int* h_groups, int* h_source, float* h_tuned_ms,
                                 float* h_default_ms, float* h_slowest_ms, float* h_serial_ms, int* h_group_of);
+/* Dominance tile shape of the fused generation per objective count:
+ * h_shapes[m] for m = 0 .. cap-1 (0 full-width tiles, 1 half-width; entries
+ * of objective counts absent from the batch are 0).  No counterpart in the
+ * reference. */
+moea_status moea_batch_tile_shapes(moea_batch* b, int* h_shapes, int cap);
 /* Population view of instance `index` (same contract as moea_algorithm_view). */
 moea_status moea_batch_view(moea_batch* b, int index, moea_population_view* out);
 

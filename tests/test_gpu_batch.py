@@ -123,6 +123,32 @@ def test_fused_batch_equals_branch_batch(seed, n_hi):
             np.testing.assert_array_equal(a.auxiliary_indices.cpu().numpy(), b.auxiliary_indices.cpu().numpy())
 
 
+def test_half_width_tiles_equal_full_width_tiles():
+    """The half-width dominance tiles (twice the tile CTAs, each staging half
+    the word tables) write the same dominance rows as the full-width ones, for
+    every objective count that selects its own tile width."""
+    T = 4
+    rng = np.random.default_rng(5)
+    specs = []
+    for i, M in enumerate([2, 3, 4, 5, 6, 8, 9, 10, 12]):
+        kind = KINDS[i % len(KINDS)]
+        N = int(rng.integers(46, 1200)) * 2
+        specs.append((kind, M, N, M + (19 if kind == "DTLZ7" else 9), 300 + i))
+    specs.append(("DTLZ2", 5, 4096, 14, 9))
+    full = cm.Batch([_make(s, T) for s in specs])
+    half = cm.Batch([_make(s, T) for s in specs], half_tiles=True)
+    assert full.fused and half.fused
+    assert full.schedule["half_tiles"] == []
+    assert half.schedule["half_tiles"] == sorted({s[1] for s in specs})
+    for _ in range(T):
+        full.step()
+        half.step()
+        for i in range(len(specs)):
+            a, b = full.result(i), half.result(i)
+            _same(a, b)
+            np.testing.assert_array_equal(a.auxiliary_indices.cpu().numpy(), b.auxiliary_indices.cpu().numpy())
+
+
 def test_autotuned_batch_equals_instances_and_caches_its_schedule():
     """The autotuned schedule (tuned on a scratch copy of the batch) changes
     how the generation is launched, never what it computes; a second batch of
@@ -139,6 +165,8 @@ def test_autotuned_batch_equals_instances_and_caches_its_schedule():
     again = cm.Batch([_make(s, T) for s in specs], autotune=True)
     assert again.schedule["source"] == "autotuned (cached)"
     assert again.schedule["group_of"] == sched["group_of"]
+    assert again.schedule["half_tiles"] == sched["half_tiles"]
+    assert set(sched["half_tiles"]) <= {s[1] for s in specs}
     again.close()
     for i in (0, 7, 19, 39):
         r = _make(specs[i], T).run()
