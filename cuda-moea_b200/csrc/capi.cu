@@ -8,6 +8,8 @@
 namespace moea {
 
 int configure_peel(Workspace& ws);
+size_t block_table_words(int n_max, int m_max);
+int configure_block_rows();
 int selftest_barrier_timeout(Workspace& ws, int which, unsigned long long limit_ns, cudaStream_t stream);
 int selftest_mbar_timeout(Workspace& ws, unsigned long long limit_ns, cudaStream_t stream);
 int run_normalize_inplace(Workspace& ws, float* objs, const float* ideal, int M, int n,
@@ -76,7 +78,7 @@ void free_all(Workspace& ws)
                     ws.assoc_idx, ws.assoc_dist, ws.rho, ws.sel_vals[0], ws.sel_vals[1],
                     ws.rank, ws.selected, ws.flags, ws.offset_dev, ws.cub_tmp, ws.tree_dirs,
                     ws.tree_order, ws.tree_center, ws.dir_delta, ws.chunk_keys, ws.chunk_bits,
-                    ws.scalar_d, ws.tc_dirs, ws.tc_rowmax, ws.peel_fmask};
+                    ws.block_tables, ws.scalar_d, ws.tc_dirs, ws.tc_rowmax, ws.peel_fmask};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     ws = Workspace{};
@@ -113,6 +115,7 @@ int workspace_init(Workspace& ws, int device, int n_max, int m_max, int h_max)
     A(ws.blocker, n); A(ws.front_sorted, n); A(ws.front_list, n);
     A(ws.chunk_keys, (size_t)(m_max > 1 ? m_max - 1 : 1) * ws.words * 32);
     A(ws.chunk_bits, (size_t)(m_max > 1 ? m_max - 1 : 1) * ws.words * 33);
+    if (m_max > 1) A(ws.block_tables, block_table_words(n_max, m_max));
     A(ws.counters, 32);
     A(ws.fronts, n); A(ws.nds_gidx, n); A(ws.sizes, 8);
     A(ws.chunk_counts, 2 * (size_t)ceil_div(n_max, 1024) + 2);
@@ -138,6 +141,7 @@ int workspace_init(Workspace& ws, int device, int n_max, int m_max, int h_max)
         if (e != cudaSuccess) st = set_error(MOEA_ERR_CUDA, "cudaMemset: %s", cudaGetErrorString(e));
     }
     if (st == MOEA_OK) st = configure_peel(ws);
+    if (st == MOEA_OK) st = configure_block_rows();
     if (st == MOEA_OK) st = dalloc(ws, &ws.peel_fmask, 3 * (size_t)ws.words);
     if (st != MOEA_OK) free_all(ws);
     return st;
@@ -212,6 +216,15 @@ moea_status moea_workspace_set_peel(moea_workspace* w, int mode)
     if (mode != MOEA_PEEL_AUTO && mode != MOEA_PEEL_GENERAL)
         return set_error(MOEA_ERR_INVALID_ARGUMENT, "set_peel: mode %d", mode);
     w->ws.peel_general = mode == MOEA_PEEL_GENERAL;
+    return MOEA_OK;
+}
+
+moea_status moea_workspace_set_tiles(moea_workspace* w, int mode)
+{
+    CHECK_WS(w);
+    if (mode != MOEA_TILES_AUTO && mode != MOEA_TILES_WORD)
+        return set_error(MOEA_ERR_INVALID_ARGUMENT, "set_tiles: mode %d", mode);
+    w->ws.word_tiles = mode == MOEA_TILES_WORD;
     return MOEA_OK;
 }
 

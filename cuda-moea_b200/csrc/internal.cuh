@@ -70,6 +70,8 @@ struct Workspace {
     int* run_start = nullptr;       // scanned run heads
     uint32_t* chunk_keys = nullptr; // [(m_max-1)][words*32] sorted objective keys per word
     uint32_t* chunk_bits = nullptr; // [(m_max-1)][words*33] prefix position sets per word
+    uint32_t* block_tables = nullptr;  // per block of 128 or 256 positions and objective: search
+                                       // tree of the keys and prefix sets (nds_block_rows)
     int* blocker = nullptr;         // per sorted position: last known unassigned dominator
     int* front_sorted = nullptr;    // per sorted position: front index or -1
     int* front_list = nullptr;      // members of each peeled front, front by front
@@ -83,6 +85,7 @@ struct Workspace {
     int peel_smem = 0;
     bool peel_single_cta = false;   // peel with one ordinary CTA (instances of a batch)
     bool peel_general = false;      // always the general peel (moea_workspace_set_peel)
+    bool word_tiles = false;        // dominance rows from per-word tables (moea_workspace_set_tiles)
     uint32_t* peel_fmask = nullptr; // [3][words] members of the last three fronts (peel)
 
     // --- NSGA-III stages ---

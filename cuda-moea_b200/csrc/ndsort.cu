@@ -1211,9 +1211,265 @@ __global__ void nds_reset_counters(int* counters)
     if (threadIdx.x >= 16 && threadIdx.x <= 19) counters[threadIdx.x] = 0;  // front sizes (nds_peel_owned)
 }
 
+// ---------------------------------------------------------------------------
+// 2b. dominance rows from block prefix sets (one workspace, any n)
+// ---------------------------------------------------------------------------
+//
+// For every block of B sorted positions and every objective m >= 1 one table
+// of BlockTable<B>::kSize words:
+//   E[0]          the largest of the block's B order keys;
+//   E[1 .. B-1]   the other B-1 keys as an implicit search tree (node k has
+//                 children 2k and 2k+1; the in-order walk is ascending);
+//   S[c], c = 0..B, from word B on: the positions of the c smallest keys
+//                 (bit j of word i = position 32 i + j of the block), B/32
+//                 words each.  For B = 256 the two 16-byte halves of S[c] are
+//                 swapped when bit 2 of c is set, so that the 16-byte loads
+//                 of eight lanes with different c spread over all eight bank
+//                 groups.
+// The count c of the block's keys <= v is the leaf that a log2(B)-level
+// descent of the tree reaches (go right when E[k] <= v) plus (E[0] <= v); the
+// block's positions whose objective is <= f_m(q) are then S[c], ties included
+// whatever their order.  A lane holding q thus gets B row bits of objective m
+// from log2(B) + 1 shared loads and B/128 16-byte loads, where the per-word
+// tables of nds_tiles take B/32 six-probe searches.  Positions >= n carry the
+// NaN key, above every key of a feasible q.
+template <int B>
+struct BlockTable {
+    static constexpr int kWords = B / 32;                // row words per block
+    static constexpr int kLevels = B == 256 ? 8 : 7;     // B = 2^kLevels
+    static constexpr int kSize = B + (B + 1) * kWords;   // words per (block, objective)
+};
+static_assert(BlockTable<256>::kSize % 4 == 0 && BlockTable<128>::kSize % 4 == 0,
+              "tables are copied in 16-byte chunks");
+
+// Block size by objective count: two tables of M-1 objectives (double
+// buffering) fit in shared memory with room for a second CTA up to M = 8.
+template <int M>
+struct BlockCfg {
+    static constexpr int kB = M <= 8 ? 256 : 128;
+};
+
+constexpr int kBlkThreads = 256;  // dominatees q per row CTA, one per thread
+constexpr int kBlkPerCta = 8;     // blocks of dominators per row CTA
+
+// Count of the 32 ascending keys a[] that are <= x (six probes).
+__device__ __forceinline__ int count_le32(const uint32_t* a, uint32_t x)
+{
+    int c = 0;
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1)
+        if (a[c + s - 1] <= x) c += s;
+    if (a[c] <= x) ++c;
+    return c;
+}
+
+// One CTA of B threads per (block, objective): each warp sorts its 32
+// (key, lane) pairs with a bitonic network; the rank of a key in the block is
+// its place in its warp plus, for every other warp, the count of that warp's
+// keys <= it (lower warps) or < it (higher warps), which orders equal keys
+// by position.  Then the tree placement of the sorted keys, and warp w builds
+// word w of every prefix set with one ballot per set.
+template <int B>
+__global__ void __launch_bounds__(B)
+nds_block_tables(const float* __restrict__ sf, int sf_stride, int n, int MF, uint32_t* __restrict__ tables)
+{
+    using T = BlockTable<B>;
+    constexpr int NW = B / 32;
+    __shared__ uint32_t s_sorted[NW][32];
+    __shared__ int s_rank[B];
+    const int blk = blockIdx.x / MF, m = blockIdx.x - blk * MF;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p = blk * B + threadIdx.x;
+    const uint32_t key = p < n ? dom_key(sf[(size_t)m * sf_stride + p]) : 0xFFFFFFFFu;
+    unsigned long long kv = ((unsigned long long)key << 32) | (unsigned)lane;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const unsigned long long o = __shfl_xor_sync(0xFFFFFFFFu, kv, j);
+            const bool take_min = ((lane & j) == 0) == ((lane & k) == 0);
+            kv = take_min ? (o < kv ? o : kv) : (o > kv ? o : kv);
+        }
+    }
+    const uint32_t skey = (uint32_t)(kv >> 32);
+    const int src = (int)(kv & 31ull);  // this lane holds the key of lane src
+    s_sorted[warp][lane] = skey;
+    __syncthreads();
+    int r = lane;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        if (w < warp) r += count_le32(s_sorted[w], skey);
+        else if (w > warp && skey > 0u) r += count_le32(s_sorted[w], skey - 1u);
+    }
+    s_rank[warp * 32 + src] = r;
+    uint32_t* tab = tables + ((size_t)blk * MF + m) * T::kSize;
+    if (r == B - 1) {
+        tab[0] = skey;
+    } else {
+        const int i = r + 1, h = __ffs(i) - 1;  // in-order index, height above the leaves
+        tab[(1 << (T::kLevels - 1 - h)) + (i >> (h + 1))] = skey;
+    }
+    __syncthreads();
+    const int rk = s_rank[threadIdx.x];  // rank of position 32 warp + lane
+    uint32_t* S = tab + B;
+    for (int c0 = 0; c0 <= B; c0 += 32) {
+        uint32_t mine = 0u;
+#pragma unroll 8
+        for (int cc = 0; cc < 32; ++cc) {
+            const uint32_t bits = __ballot_sync(0xFFFFFFFFu, rk < c0 + cc);
+            if (cc == lane) mine = bits;
+        }
+        const int c = c0 + lane;
+        if (c <= B) {
+            const int wj = NW == 8 ? (warp ^ (((c >> 2) & 1) << 2)) : warp;  // the half swap
+            S[c * NW + wj] = mine;
+        }
+    }
+}
+
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Rows of kBlkThreads dominatees (one per thread) against kBlkPerCta blocks of
+// B dominator positions.  The blocks' tables (all objectives) are staged in
+// shared memory with cp.async, the next block's while the current one is
+// searched.  Per block a lane descends the M-1 trees side by side, ANDs the M-1
+// prefix sets and the dup mask, and stores its B/32 row words with 16-byte
+// stores (each lane writes whole 32-byte sectors of its own row).  The lane
+// remembers the highest dominator seen and raises blocker[q] to it once.
+// Infeasible q are skipped: the peel never reaches them, so their rows are
+// never read.
+template <int M, int B>
+__global__ void __launch_bounds__(kBlkThreads)
+nds_block_rows(const float* __restrict__ sf, int sf_stride, const int* __restrict__ qinfo,
+               const uint32_t* __restrict__ tables, int n, int W, uint32_t* __restrict__ rows,
+               int* __restrict__ blocker)
+{
+    using T = BlockTable<B>;
+    constexpr int MF = M - 1;
+    constexpr int KW = T::kWords;
+    constexpr int TS = T::kSize;
+    constexpr int CH = MF * TS / 4;  // 16-byte chunks of one block's tables
+    extern __shared__ uint4 s_tab[];  // [2][CH]
+    const int q0 = blockIdx.y * kBlkThreads;
+    if (q0 >= n) return;
+    const int qend = min(q0 + kBlkThreads, n);
+    const int nb = (qend - 1 + B - 1) / B;  // blocks holding the dominators (positions < qend - 1)
+    const int b_lo = blockIdx.x * kBlkPerCta;
+    if (b_lo >= nb) return;
+    const int b_hi = min(nb, b_lo + kBlkPerCta);
+    const int q = q0 + threadIdx.x;
+    uint32_t qk[MF];
+    int dup = 0;
+    bool live = false;
+    if (q < n) {
+        const uint32_t info = (uint32_t)qinfo[q];
+        live = (info & kInfeasibleBit) == 0u;
+        dup = (int)(info & ~kInfeasibleBit);
+    }
+#pragma unroll
+    for (int m = 0; m < MF; ++m) qk[m] = live ? dom_key(sf[(size_t)m * sf_stride + q]) : 0u;
+    if (!__syncthreads_or(live)) return;
+
+    const uint4* src = reinterpret_cast<const uint4*>(tables);
+    auto stage = [&](int b, int buf) {
+        const uint4* g = src + (size_t)b * CH;
+        uint4* d = s_tab + buf * CH;
+        for (int i = threadIdx.x; i < CH; i += kBlkThreads)
+            cp_async16(d + i, reinterpret_cast<const uint32_t*>(g + i));
+        cp_async_commit();
+    };
+    stage(b_lo, 0);
+    int best = -1;
+    uint32_t* row = rows + (size_t)q * W;
+    for (int b = b_lo; b < b_hi; ++b) {
+        const int buf = (b - b_lo) & 1;
+        if (b + 1 < b_hi) {
+            stage(b + 1, buf ^ 1);
+            cp_async_wait_one();
+        } else {
+            cp_async_wait_all();
+        }
+        __syncthreads();
+        if (live) {
+            const int lo = b * B;
+            const int rem = dup - lo;  // positions of the block below dup[q]
+            uint32_t acc[KW];
+#pragma unroll
+            for (int j = 0; j < KW; ++j) acc[j] = rem > 0 ? 0xFFFFFFFFu : 0u;
+            if (rem > 0) {
+                const uint32_t* tab = reinterpret_cast<const uint32_t*>(s_tab + buf * CH);
+                int k[MF];
+#pragma unroll
+                for (int m = 0; m < MF; ++m) k[m] = 1;
+#pragma unroll
+                for (int l = 0; l < T::kLevels; ++l) {
+#pragma unroll
+                    for (int m = 0; m < MF; ++m) k[m] = 2 * k[m] + (tab[m * TS + k[m]] <= qk[m] ? 1 : 0);
+                }
+#pragma unroll
+                for (int m = 0; m < MF; ++m) {
+                    const uint32_t* E = tab + m * TS;
+                    const int c = k[m] - B + (E[0] <= qk[m] ? 1 : 0);
+                    const uint4* S = reinterpret_cast<const uint4*>(E + B) + c * (KW / 4);
+                    if constexpr (KW == 8) {
+                        const int sw = (c >> 2) & 1;
+                        const uint4 x = S[sw], y = S[sw ^ 1];
+                        acc[0] &= x.x; acc[1] &= x.y; acc[2] &= x.z; acc[3] &= x.w;
+                        acc[4] &= y.x; acc[5] &= y.y; acc[6] &= y.z; acc[7] &= y.w;
+                    } else {
+                        const uint4 x = S[0];
+                        acc[0] &= x.x; acc[1] &= x.y; acc[2] &= x.z; acc[3] &= x.w;
+                    }
+                }
+                if (rem < B) {
+#pragma unroll
+                    for (int j = 0; j < KW; ++j) {
+                        const int r = rem - 32 * j;
+                        acc[j] &= r >= 32 ? 0xFFFFFFFFu : (r <= 0 ? 0u : ((1u << r) - 1u));
+                    }
+                }
+            }
+            uint4* dst = reinterpret_cast<uint4*>(row + b * KW);
+            dst[0] = make_uint4(acc[0], acc[1], acc[2], acc[3]);
+            if constexpr (KW == 8) {
+                if (b * KW + 8 <= W) dst[1] = make_uint4(acc[4], acc[5], acc[6], acc[7]);
+            }
+#pragma unroll
+            for (int j = 0; j < KW; ++j)
+                if (acc[j]) best = lo + 32 * j + 31 - __clz(acc[j]);
+        }
+        __syncthreads();  // the buffer is staged again two blocks on
+    }
+    if (best >= 0) atomicMax(blocker + q, best);
+}
+
+template <int M>
+constexpr int block_rows_smem()
+{
+    return 2 * (M - 1) * BlockTable<BlockCfg<M>::kB>::kSize * 4;
+}
+
+template <int M>
+void launch_block_rows(const Workspace& ws, int n, cudaStream_t stream)
+{
+    constexpr int B = BlockCfg<M>::kB;
+    nds_block_tables<B><<<ceil_div(n, B) * (M - 1), B, 0, stream>>>(ws.sorted_f, ws.n_max, n, M - 1,
+                                                                     ws.block_tables);
+    const int nb = ceil_div(n - 1, B);
+    dim3 grid(ceil_div(nb, kBlkPerCta), ceil_div(n, kBlkThreads));
+    nds_block_rows<M, B><<<grid, kBlkThreads, block_rows_smem<M>(), stream>>>(
+        ws.sorted_f, ws.n_max, ws.qinfo, ws.block_tables, n, ws.words, ws.rows, ws.blocker);
+}
+
 template <int M>
 void launch_tiles(const Workspace& ws, int n, cudaStream_t stream)
 {
+    if constexpr (M > 1) {
+        if (!ws.word_tiles) {
+            launch_block_rows<M>(ws, n, stream);
+            return;
+        }
+    }
     const int nqb = ceil_div(n, kQB);
     const int maxw = ceil_div(n, 32);
     if (M > 1) {
@@ -1769,6 +2025,29 @@ static int raise_dynamic_smem(const void* func, size_t bytes)
     MOEA_CUDA_TRY(cudaFuncGetAttributes(&fa, func));
     if ((size_t)fa.maxDynamicSharedSizeBytes < bytes)
         MOEA_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return MOEA_OK;
+}
+
+// Words of block tables a workspace of n_max points and m_max objectives
+// needs for every objective count up to m_max.
+size_t block_table_words(int n_max, int m_max)
+{
+    if (m_max < 2) return 0;
+    const size_t lo = (size_t)ceil_div(n_max, 256) * (size_t)(m_max < 8 ? m_max - 1 : 7) * BlockTable<256>::kSize;
+    const size_t hi = m_max >= 9 ? (size_t)ceil_div(n_max, 128) * (size_t)(m_max - 1) * BlockTable<128>::kSize : 0;
+    return lo > hi ? lo : hi;
+}
+
+// Shared-memory limits of the block-row kernels beyond 48 KB.
+int configure_block_rows()
+{
+#define MOEA_BR_CASE(K) \
+    if (block_rows_smem<K>() > 48 * 1024) \
+        MOEA_TRY(raise_dynamic_smem((const void*)nds_block_rows<K, BlockCfg<K>::kB>, block_rows_smem<K>()));
+    MOEA_BR_CASE(2) MOEA_BR_CASE(3) MOEA_BR_CASE(4) MOEA_BR_CASE(5) MOEA_BR_CASE(6) MOEA_BR_CASE(7)
+    MOEA_BR_CASE(8) MOEA_BR_CASE(9) MOEA_BR_CASE(10) MOEA_BR_CASE(11) MOEA_BR_CASE(12) MOEA_BR_CASE(13)
+    MOEA_BR_CASE(14) MOEA_BR_CASE(15) MOEA_BR_CASE(16)
+#undef MOEA_BR_CASE
     return MOEA_OK;
 }
 

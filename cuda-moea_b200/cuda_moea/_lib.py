@@ -110,6 +110,7 @@ _SIGNATURES = [
     ("moea_workspace_destroy", None, [vp]),
     ("moea_workspace_bytes", c_size_t, [vp]),
     ("moea_workspace_set_peel", c_int, [vp, c_int]),
+    ("moea_workspace_set_tiles", c_int, [vp, c_int]),
     ("moea_ndsort", c_int, [vp, vp, vp, c_int, c_int, c_int, vp, ip, vp]),
     ("moea_nds_extract", c_int, [vp, vp, c_int, vp, c_int, vp, vp, vp]),
     ("moea_ideal_point", c_int, [vp, vp, c_int, c_int, vp, vp]),

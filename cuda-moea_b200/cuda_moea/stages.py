@@ -44,6 +44,11 @@ class Workspace:
         """True: every sort takes the general peel; False: the automatic choice."""
         check(lib().moea_workspace_set_peel(self.handle, 1 if general else 0))
 
+    def set_tiles(self, word: bool) -> None:
+        """True: every sort builds its dominance rows from the per-word tables;
+        False: from the block prefix sets (the default)."""
+        check(lib().moea_workspace_set_tiles(self.handle, 1 if word else 0))
+
     def close(self) -> None:
         if getattr(self, "handle", None) is not None and self.handle.value:
             lib().moea_workspace_destroy(self.handle)

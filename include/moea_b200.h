@@ -72,6 +72,14 @@ size_t moea_workspace_bytes(const moea_workspace* ws);
 #define MOEA_PEEL_AUTO 0
 #define MOEA_PEEL_GENERAL 1
 moea_status moea_workspace_set_peel(moea_workspace* ws, int mode);
+/* Dominance-row kernel of the workspace's sorts: MOEA_TILES_AUTO (default)
+ * builds the rows from prefix sets of blocks of 256 sorted positions (128
+ * beyond eight objectives) with search trees of their keys; MOEA_TILES_WORD
+ * from the per-word tables (32 positions) with six-probe searches.  Both give
+ * the same fronts.  No counterpart in the reference. */
+#define MOEA_TILES_AUTO 0
+#define MOEA_TILES_WORD 1
+moea_status moea_workspace_set_tiles(moea_workspace* ws, int mode);
 
 /* ========================================================================
  * Stage-level entry points (one hot-path stage each).

@@ -149,6 +149,40 @@ def test_ndsort_general_and_lane_owned_peels_agree(st, oracle, M, n, kind, cvmod
         w.close()
 
 
+@pytest.mark.parametrize("M,n,kind,cvmode", [(2, 97, "uniform", "feasible"), (3, 65536, "dtlz1-thin", "feasible"),
+                                            (3, 5000, "ties", "nan"), (4, 3001, "correlated", "mixed"),
+                                            (5, 40000, "dtlz1-thin", "mixed"), (8, 10000, "uniform", "negzero"),
+                                            (9, 4099, "uniform", "mixed"), (10, 16384, "dtlz1", "mostly_infeasible"),
+                                            (12, 257, "ties", "feasible"), (16, 2000, "correlated", "feasible"),
+                                            (3, 3, "uniform", "feasible"), (7, 129, "ties", "all_infeasible")])
+def test_ndsort_block_and_word_tiles_agree(st, oracle, M, n, kind, cvmode):
+    """The two dominance-row kernels (block prefix sets with search trees, the
+    default, and the per-word tables) give the oracle's fronts on the same
+    inputs: block sizes 256 (M <= 8) and 128 (M >= 9), ragged last blocks,
+    ties, NaN objectives and violations, infeasible majorities."""
+    rng = np.random.default_rng(n * 11 + M)
+    if kind == "dtlz1-thin":
+        x = rng.random((n, M + 4)).astype(np.float32)
+        x[:, M - 1:] = (0.5 + 0.02 * rng.standard_normal((n, 5))).astype(np.float32)
+        objs, _ = oracle.evaluate("DTLZ1", x, M)
+    else:
+        objs = _population(rng, M, n, kind)
+    if cvmode == "nan":
+        objs[rng.integers(0, M), rng.integers(0, n, 2)] = np.nan
+    cv = _cv(rng, n, cvmode)
+    target = max(1, n // 2)
+    want, wmf = oracle.ndsort(cv, objs, target)
+    w = st.Workspace(max_points=n, max_objectives=M, max_directions=1)
+    try:
+        for word in (False, True, False):
+            w.set_tiles(word)
+            got, gmf = st.ndsort(w, _t(cv), _t(objs), target)
+            np.testing.assert_array_equal(got.cpu().numpy(), want)
+            assert gmf == wmf
+    finally:
+        w.close()
+
+
 def test_ndsort_all_mutually_nondominated(st, ws, oracle):
     # points on a line f1 = 1 - f0: no dominance pair at all (the reference's
     # CSR queue path leaves every front at -1 in this case; the relation gives front 0)
