@@ -81,6 +81,7 @@ struct Workspace {
                                     // [12] last feasible front, [13] long runs of equal sort keys,
                                     // [16..19] two 64-bit barrier words carrying front sizes
     int peel_grid = 0;              // co-resident CTAs of the peel kernel
+    int sm_count = 0;               // SMs of the workspace's device
     int peel_owned_grid = 0;        // CTAs of the lane-owned peel (one per SM), 0 if unavailable
     int peel_smem = 0;
     bool peel_single_cta = false;   // peel with one ordinary CTA (instances of a batch)

@@ -36,6 +36,8 @@
 //     once over the whole sort.  Fronts are separated by a bounded grid barrier
 //     and the loop stops once `target` points are assigned, like the
 //     reference's front propagation loops (:792-843, :1070-1279).
+#include <algorithm>
+
 #include <cub/cub.cuh>
 
 #include "internal.cuh"
@@ -1242,15 +1244,20 @@ struct BlockTable {
 static_assert(BlockTable<256>::kSize % 4 == 0 && BlockTable<128>::kSize % 4 == 0,
               "tables are copied in 16-byte chunks");
 
-// Block size by objective count: two tables of M-1 objectives (double
-// buffering) fit in shared memory with room for a second CTA up to M = 8.
+// Block size by objective count: up to M = 4 the double-buffered tables of
+// 256 positions (9 KB per objective) leave room for several CTAs per SM;
+// beyond, blocks of 128 positions (2.5 KB per objective) keep the SMs full.
 template <int M>
 struct BlockCfg {
-    static constexpr int kB = M <= 8 ? 256 : 128;
+    static constexpr int kB = M <= 4 ? 256 : 128;
 };
 
-constexpr int kBlkThreads = 256;  // dominatees q per row CTA, one per thread
-constexpr int kBlkPerCta = 8;     // blocks of dominators per row CTA
+// Dominatees q per row CTA, one per thread.  Every CTA stages each of its
+// blocks' tables once, so more q per CTA mean fewer shared-memory writes per
+// row word.
+constexpr int kBlkThreads = 512;
+constexpr int kBlkPerCtaMax = 8;  // blocks of dominators per row CTA, at most
+constexpr int kBlkCtasPerSm = 8;  // row CTAs per SM the launch aims at (with fewer blocks per CTA)
 
 // Count of the 32 ascending keys a[] that are <= x (six probes).
 __device__ __forceinline__ int count_le32(const uint32_t* a, uint32_t x)
@@ -1329,8 +1336,8 @@ nds_block_tables(const float* __restrict__ sf, int sf_stride, int n, int MF, uin
 
 __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
-// Rows of kBlkThreads dominatees (one per thread) against kBlkPerCta blocks of
-// B dominator positions.  The blocks' tables (all objectives) are staged in
+// Rows of kBlkThreads dominatees (one per thread) against bpc blocks of B
+// dominator positions.  The blocks' tables (all objectives) are staged in
 // shared memory with cp.async, the next block's while the current one is
 // searched.  Per block a lane descends the M-1 trees side by side, ANDs the M-1
 // prefix sets and the dup mask, and stores its B/32 row words with 16-byte
@@ -1341,7 +1348,7 @@ __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wai
 template <int M, int B>
 __global__ void __launch_bounds__(kBlkThreads)
 nds_block_rows(const float* __restrict__ sf, int sf_stride, const int* __restrict__ qinfo,
-               const uint32_t* __restrict__ tables, int n, int W, uint32_t* __restrict__ rows,
+               const uint32_t* __restrict__ tables, int n, int W, int bpc, uint32_t* __restrict__ rows,
                int* __restrict__ blocker)
 {
     using T = BlockTable<B>;
@@ -1354,9 +1361,9 @@ nds_block_rows(const float* __restrict__ sf, int sf_stride, const int* __restric
     if (q0 >= n) return;
     const int qend = min(q0 + kBlkThreads, n);
     const int nb = (qend - 1 + B - 1) / B;  // blocks holding the dominators (positions < qend - 1)
-    const int b_lo = blockIdx.x * kBlkPerCta;
+    const int b_lo = blockIdx.x * bpc;
     if (b_lo >= nb) return;
-    const int b_hi = min(nb, b_lo + kBlkPerCta);
+    const int b_hi = min(nb, b_lo + bpc);
     const int q = q0 + threadIdx.x;
     uint32_t qk[MF];
     int dup = 0;
@@ -1453,12 +1460,23 @@ template <int M>
 void launch_block_rows(const Workspace& ws, int n, cudaStream_t stream)
 {
     constexpr int B = BlockCfg<M>::kB;
+    if (n < 2) return;  // no pairs: every blocker stays -1
     nds_block_tables<B><<<ceil_div(n, B) * (M - 1), B, 0, stream>>>(ws.sorted_f, ws.n_max, n, M - 1,
                                                                      ws.block_tables);
+    // blocks per CTA: the most (up to kBlkPerCtaMax) that still give
+    // kBlkCtasPerSm working CTAs per SM; fewer blocks per CTA overlap less
+    // staging with searching, but small sorts need the CTAs
+    const int ntiles = ceil_div(n, kBlkThreads);
     const int nb = ceil_div(n - 1, B);
-    dim3 grid(ceil_div(nb, kBlkPerCta), ceil_div(n, kBlkThreads));
+    int bpc = kBlkPerCtaMax;
+    for (; bpc > 1; bpc >>= 1) {
+        long long ctas = 0;
+        for (int t = 0; t < ntiles; ++t) ctas += ceil_div(ceil_div(std::min((t + 1) * kBlkThreads, n) - 1, B), bpc);
+        if (ctas >= (long long)kBlkCtasPerSm * ws.sm_count) break;
+    }
+    dim3 grid(ceil_div(nb, bpc), ntiles);
     nds_block_rows<M, B><<<grid, kBlkThreads, block_rows_smem<M>(), stream>>>(
-        ws.sorted_f, ws.n_max, ws.qinfo, ws.block_tables, n, ws.words, ws.rows, ws.blocker);
+        ws.sorted_f, ws.n_max, ws.qinfo, ws.block_tables, n, ws.words, bpc, ws.rows, ws.blocker);
 }
 
 template <int M>
@@ -2033,8 +2051,8 @@ static int raise_dynamic_smem(const void* func, size_t bytes)
 size_t block_table_words(int n_max, int m_max)
 {
     if (m_max < 2) return 0;
-    const size_t lo = (size_t)ceil_div(n_max, 256) * (size_t)(m_max < 8 ? m_max - 1 : 7) * BlockTable<256>::kSize;
-    const size_t hi = m_max >= 9 ? (size_t)ceil_div(n_max, 128) * (size_t)(m_max - 1) * BlockTable<128>::kSize : 0;
+    const size_t lo = (size_t)ceil_div(n_max, 256) * (size_t)(m_max < 4 ? m_max - 1 : 3) * BlockTable<256>::kSize;
+    const size_t hi = m_max >= 5 ? (size_t)ceil_div(n_max, 128) * (size_t)(m_max - 1) * BlockTable<128>::kSize : 0;
     return lo > hi ? lo : hi;
 }
 
@@ -2061,6 +2079,7 @@ int configure_peel(Workspace& ws)
                                                                 smem));
     int sms = 0;
     MOEA_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws.device));
+    ws.sm_count = sms;
     if (per_sm < 1)
         return set_error(MOEA_ERR_UNSUPPORTED, "peel kernel does not fit on an SM (smem %zu)", smem);
     ws.peel_grid = sms * (per_sm > 2 ? 2 : per_sm);

@@ -74,7 +74,7 @@ size_t moea_workspace_bytes(const moea_workspace* ws);
 moea_status moea_workspace_set_peel(moea_workspace* ws, int mode);
 /* Dominance-row kernel of the workspace's sorts: MOEA_TILES_AUTO (default)
  * builds the rows from prefix sets of blocks of 256 sorted positions (128
- * beyond eight objectives) with search trees of their keys; MOEA_TILES_WORD
+ * beyond four objectives) with search trees of their keys; MOEA_TILES_WORD
  * from the per-word tables (32 positions) with six-probe searches.  Both give
  * the same fronts.  No counterpart in the reference. */
 #define MOEA_TILES_AUTO 0

@@ -154,11 +154,12 @@ def test_ndsort_general_and_lane_owned_peels_agree(st, oracle, M, n, kind, cvmod
                                             (5, 40000, "dtlz1-thin", "mixed"), (8, 10000, "uniform", "negzero"),
                                             (9, 4099, "uniform", "mixed"), (10, 16384, "dtlz1", "mostly_infeasible"),
                                             (12, 257, "ties", "feasible"), (16, 2000, "correlated", "feasible"),
-                                            (3, 3, "uniform", "feasible"), (7, 129, "ties", "all_infeasible")])
+                                            (3, 3, "uniform", "feasible"), (3, 1, "uniform", "feasible"),
+                                            (4, 2, "ties", "feasible"), (7, 129, "ties", "all_infeasible")])
 def test_ndsort_block_and_word_tiles_agree(st, oracle, M, n, kind, cvmode):
     """The two dominance-row kernels (block prefix sets with search trees, the
     default, and the per-word tables) give the oracle's fronts on the same
-    inputs: block sizes 256 (M <= 8) and 128 (M >= 9), ragged last blocks,
+    inputs: block sizes 256 (M <= 4) and 128 (M >= 5), ragged last blocks,
     ties, NaN objectives and violations, infeasible majorities."""
     rng = np.random.default_rng(n * 11 + M)
     if kind == "dtlz1-thin":
@@ -172,7 +173,7 @@ def test_ndsort_block_and_word_tiles_agree(st, oracle, M, n, kind, cvmode):
     cv = _cv(rng, n, cvmode)
     target = max(1, n // 2)
     want, wmf = oracle.ndsort(cv, objs, target)
-    w = st.Workspace(max_points=n, max_objectives=M, max_directions=1)
+    w = st.Workspace(max_points=max(n, 2), max_objectives=M, max_directions=1)
     try:
         for word in (False, True, False):
             w.set_tiles(word)
