@@ -1336,15 +1336,27 @@ nds_block_tables(const float* __restrict__ sf, int sf_stride, int n, int MF, uin
 
 __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
+constexpr int kRowSegWords = 16;   // row words per lane collected before the stores
+constexpr int kOutStride = 20;     // shared words per lane of the collected rows (16-byte rows, no conflicts)
+
+// Rows are collected in shared memory for blocks of 256 positions (M <= 4).
+// With blocks of 128 positions the search of the M-1 >= 4 objectives
+// outweighs the stores, and the 40 KB for the collected rows would cost a
+// resident CTA per SM: each lane stores its own words.
+template <int B>
+constexpr bool collect_rows() { return B == 256; }
+
 // Rows of kBlkThreads dominatees (one per thread) against bpc blocks of B
 // dominator positions.  The blocks' tables (all objectives) are staged in
 // shared memory with cp.async, the next block's while the current one is
-// searched.  Per block a lane descends the M-1 trees side by side, ANDs the M-1
-// prefix sets and the dup mask, and stores its B/32 row words with 16-byte
-// stores (each lane writes whole 32-byte sectors of its own row).  The lane
-// remembers the highest dominator seen and raises blocker[q] to it once.
-// Infeasible q are skipped: the peel never reaches them, so their rows are
-// never read.
+// searched.  Per block a lane descends the M-1 trees side by side and ANDs the
+// M-1 prefix sets and the dup mask into its B/32 row words.  With
+// collect_rows<B>() the lane puts them into shared memory and every
+// kRowSegWords words the CTA writes the collected row segments (64 bytes per
+// row), eight rows per warp instruction, where stores by the lanes themselves
+// touch 32 rows per instruction; otherwise the lane stores them itself.  The lane remembers
+// the highest dominator seen and raises blocker[q] to it once.  Infeasible q
+// are skipped: the peel never reaches them, so their rows are never read.
 template <int M, int B>
 __global__ void __launch_bounds__(kBlkThreads)
 nds_block_rows(const float* __restrict__ sf, int sf_stride, const int* __restrict__ qinfo,
@@ -1356,7 +1368,10 @@ nds_block_rows(const float* __restrict__ sf, int sf_stride, const int* __restric
     constexpr int KW = T::kWords;
     constexpr int TS = T::kSize;
     constexpr int CH = MF * TS / 4;  // 16-byte chunks of one block's tables
-    extern __shared__ uint4 s_tab[];  // [2][CH]
+    constexpr int G = kRowSegWords / KW;  // blocks per collected segment
+    extern __shared__ uint4 s_tab[];  // [2][CH] tables, then (collect_rows) [kBlkThreads][kOutStride] row words
+    __shared__ unsigned char s_live[kBlkThreads];
+    uint32_t* s_out = reinterpret_cast<uint32_t*>(s_tab + 2 * CH);
     const int q0 = blockIdx.y * kBlkThreads;
     if (q0 >= n) return;
     const int qend = min(q0 + kBlkThreads, n);
@@ -1375,6 +1390,7 @@ nds_block_rows(const float* __restrict__ sf, int sf_stride, const int* __restric
     }
 #pragma unroll
     for (int m = 0; m < MF; ++m) qk[m] = live ? dom_key(sf[(size_t)m * sf_stride + q]) : 0u;
+    s_live[threadIdx.x] = live ? 1 : 0;
     if (!__syncthreads_or(live)) return;
 
     const uint4* src = reinterpret_cast<const uint4*>(tables);
@@ -1387,7 +1403,8 @@ nds_block_rows(const float* __restrict__ sf, int sf_stride, const int* __restric
     };
     stage(b_lo, 0);
     int best = -1;
-    uint32_t* row = rows + (size_t)q * W;
+    uint32_t* my_out = s_out + threadIdx.x * kOutStride;
+    int seg = b_lo;  // first block of the segment being collected
     for (int b = b_lo; b < b_hi; ++b) {
         const int buf = (b - b_lo) & 1;
         if (b + 1 < b_hi) {
@@ -1436,16 +1453,38 @@ nds_block_rows(const float* __restrict__ sf, int sf_stride, const int* __restric
                     }
                 }
             }
-            uint4* dst = reinterpret_cast<uint4*>(row + b * KW);
-            dst[0] = make_uint4(acc[0], acc[1], acc[2], acc[3]);
-            if constexpr (KW == 8) {
-                if (b * KW + 8 <= W) dst[1] = make_uint4(acc[4], acc[5], acc[6], acc[7]);
+            if constexpr (collect_rows<B>()) {
+                uint4* o = reinterpret_cast<uint4*>(my_out + (b - seg) * KW);
+                o[0] = make_uint4(acc[0], acc[1], acc[2], acc[3]);
+                if constexpr (KW == 8) o[1] = make_uint4(acc[4], acc[5], acc[6], acc[7]);
+            } else {
+                uint4* dst = reinterpret_cast<uint4*>(rows + (size_t)q * W + b * KW);
+                dst[0] = make_uint4(acc[0], acc[1], acc[2], acc[3]);
+                if constexpr (KW == 8) {
+                    if (b * KW + 8 <= W) dst[1] = make_uint4(acc[4], acc[5], acc[6], acc[7]);
+                }
             }
 #pragma unroll
             for (int j = 0; j < KW; ++j)
                 if (acc[j]) best = lo + 32 * j + 31 - __clz(acc[j]);
         }
-        __syncthreads();  // the buffer is staged again two blocks on
+        if (collect_rows<B>() && (b - seg + 1 == G || b + 1 == b_hi)) {
+            // the segment's words seg*KW .. seg*KW + nw - 1 of every live row:
+            // a warp writes 8 rows x 4 chunks of 16 bytes, lanes 8i .. 8i+7
+            // reading rows R+i and R+i+4 (distinct bank groups)
+            __syncthreads();
+            const int nw = (b - seg + 1) * KW;
+            for (int c = threadIdx.x; c < kBlkThreads * (kRowSegWords / 4); c += kBlkThreads) {
+                const int l = c & 31, rsel = l >> 2, part = l & 3;
+                const int r = (c >> 5) * 8 + ((rsel & 1) << 2) + (rsel >> 1);
+                const int gw = seg * KW + part * 4;
+                if (part * 4 < nw && gw + 4 <= W && s_live[r])
+                    *reinterpret_cast<uint4*>(rows + (size_t)(q0 + r) * W + gw) =
+                        *reinterpret_cast<const uint4*>(s_out + r * kOutStride + part * 4);
+            }
+            seg = b + 1;
+        }
+        __syncthreads();  // the table buffer is staged again two blocks on, the row words rewritten
     }
     if (best >= 0) atomicMax(blocker + q, best);
 }
@@ -1453,7 +1492,8 @@ nds_block_rows(const float* __restrict__ sf, int sf_stride, const int* __restric
 template <int M>
 constexpr int block_rows_smem()
 {
-    return 2 * (M - 1) * BlockTable<BlockCfg<M>::kB>::kSize * 4;
+    constexpr int B = BlockCfg<M>::kB;
+    return 2 * (M - 1) * BlockTable<B>::kSize * 4 + (collect_rows<B>() ? kBlkThreads * kOutStride * 4 : 0);
 }
 
 template <int M>
