@@ -44,15 +44,16 @@ sys.path.insert(0, str(ROOT))
 METRIC = "NSGA-III gen/s @N=32768,M=3; batched instance-gen/s vs plain, identical ranks"
 WORKLOAD = "NSGA-III DTLZ1 M=3 D=7 N=32768, Das-Dennis H=254 (32640 directions), 1 generation per step"
 N_POP, D_VAR, M_OBJ, PARTITIONS = 32768, 7, 3, 254
-# dram__bytes_read.sum + dram__bytes_write.sum of one nds_tiles launch
-TILES_DRAM_BYTES = 3.00e6 + 210.55e6
+# dram__bytes_read.sum + dram__bytes_write.sum of one nds_block_rows launch at
+# this workload (one ncu --set full capture of the launch)
+ROWS_DRAM_BYTES = 5.80e6 + 217.07e6
 # dram__bytes_read.sum + dram__bytes_write.sum of one nds_peel_owned launch at
 # this workload (one ncu --set full capture of the launch)
 PEEL_DRAM_BYTES = 132.83e6 + 3.92e6
-# warp instructions nds_tiles issues per (warp, 32-position word) step: one
-# step tests 32 x 32 ordered pairs (ncu instruction count of one launch at
-# this workload)
-TILES_WARP_INSTR_PER_STEP = 97
+# l1tex__data_pipe_lsu_wavefronts of one nds_block_rows launch at this
+# workload (shared-memory loads and stores 24.15e6, global row stores and
+# table copies the rest): the work of the unit that bounds the kernel
+ROWS_LSU_WAVEFRONTS = 29.17e6
 
 
 def _peaks():
@@ -123,10 +124,11 @@ def kernel_rooflines(stage_ms: dict, n_mix: int, headline: bool):
     - nds_peel (ndsort.peel): against the measured HBM copy bandwidth; its
       algorithmic bytes are the lower-triangle relation rows, each read at
       most once: n(n-1)/2 bits.
-    - nds_tiles (ndsort.dominance_tiles): integer compare work, so against the
-      issue-rate peak of the kernel as written: 148 SMs x 4 schedulers x
-      max SM clock warp instructions/s, TILES_WARP_INSTR_PER_STEP warp
-      instructions per 1024 pair tests; the unit is lower-triangle pair tests/s.
+    - nds_block_rows (ndsort.dominance_tiles, with the block tables): bound
+      by the LSU data pipe (shared-memory tree descents and prefix-set reads,
+      row stores), so against that pipe's peak of one wavefront per SM and
+      clock (148 SMs x max SM clock), with ROWS_LSU_WAVEFRONTS per launch;
+      the pair tests/s and the HBM fraction on the rows written go beside it.
     """
     hbm, peak_kind = _peaks()
     tri_pairs = n_mix * (n_mix - 1) / 2
@@ -139,14 +141,15 @@ def kernel_rooflines(stage_ms: dict, n_mix: int, headline: bool):
                     "unit": "GB/s", "frac": a / hbm, "peak_source": peak_kind, "algorithmic_bytes": rel_bytes,
                     "traffic": PEEL_DRAM_BYTES if headline else None, "ms": peel})
     tiles = stage_ms.get("ndsort.dominance_tiles")
-    if tiles:
-        issue_peak = 148 * 4 * 1.965e9 * 1024 / TILES_WARP_INSTR_PER_STEP
-        a = tri_pairs / (tiles / 1e3)
-        out.append({"kernel": "nds_tiles (dominance rows)", "bound": "issue", "achieved": a, "peak": issue_peak,
-                    "unit": "pair tests/s", "frac": a / issue_peak,
-                    "peak_source": "148 SMs x 4 warp instr/clk x 1965 MHz, 97 warp instr per 1024 pairs",
+    if tiles and headline:
+        lsu_peak = 148 * 1.965e9
+        a = ROWS_LSU_WAVEFRONTS / (tiles / 1e3)
+        out.append({"kernel": "nds_block_rows (dominance rows)", "bound": "lsu", "achieved": a, "peak": lsu_peak,
+                    "unit": "LSU wavefronts/s", "frac": a / lsu_peak,
+                    "peak_source": "148 SMs x 1 LSU data-pipe wavefront/clk x 1965 MHz",
+                    "pair_tests_per_s": tri_pairs / (tiles / 1e3),
                     "algorithmic_bytes": rel_bytes, "hbm_frac": rel_bytes / (tiles / 1e3) / 1e9 / hbm,
-                    "traffic": TILES_DRAM_BYTES if headline else None, "ms": tiles})
+                    "traffic": ROWS_DRAM_BYTES, "ms": tiles})
     out.sort(key=lambda r: -r["ms"])
     return out
 
