@@ -1545,14 +1545,60 @@ void launch_tiles(const Workspace& ws, int n, cudaStream_t stream)
 // fused batch: one launch per stage for every instance (n = 2N <= 8192)
 // ---------------------------------------------------------------------------
 
-using FusedSort32 = cub::BlockRadixSort<uint32_t, kFusedThreads, kFusedItems, int>;
-using FusedSort64 = cub::BlockRadixSort<uint64_t, kFusedThreads, kFusedItems, int>;
+// Block sorts with 2, 4 or 8 items per thread: the smallest that holds the
+// instance (the sort's work grows with the items).
+template <int ITEMS>
+using FusedSort32 = cub::BlockRadixSort<uint32_t, kFusedThreads, ITEMS, int>;
+template <int ITEMS>
+using FusedSort64 = cub::BlockRadixSort<uint64_t, kFusedThreads, ITEMS, int>;
 using FusedScan = cub::BlockScan<int, kFusedThreads>;
 union FusedSortStorage {
-    typename FusedSort32::TempStorage s32;
-    typename FusedSort64::TempStorage s64;
+    typename FusedSort32<kFusedItems>::TempStorage s32;
+    typename FusedSort64<kFusedItems>::TempStorage s64;
+    typename FusedSort32<4>::TempStorage s32_4;
+    typename FusedSort64<4>::TempStorage s64_4;
+    typename FusedSort32<2>::TempStorage s32_2;
+    typename FusedSort64<2>::TempStorage s64_2;
     typename FusedScan::TempStorage scan;
 };
+
+// The stable LSD passes of fused_lexsort (objectives M-1 .. 1 for class 0,
+// then class and f0) with ITEMS keys per thread (ITEMS * kFusedThreads >= n);
+// the permutation goes to I.perm[0 .. n).  Items beyond n carry keys above
+// every real key and stay behind the real ones.
+template <int ITEMS>
+__device__ __forceinline__ void fused_lex_passes(const BatchInst& I, const SplitPop& pop, int n, int M,
+                                                 FusedSortStorage& tmp)
+{
+    const int t = threadIdx.x;
+    int vals[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) vals[j] = t * ITEMS + j;
+    for (int m = M - 1; m >= 1; --m) {
+        uint32_t keys[ITEMS];
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const int pt = vals[j];
+            keys[j] = (pt < n) ? (((I.key0[pt] >> 32) == 0) ? float_order_key(pop.obj(m, pt)) : 0u)
+                               : 0xFFFFFFFFu;
+        }
+        FusedSort32<ITEMS>(*reinterpret_cast<typename FusedSort32<ITEMS>::TempStorage*>(&tmp)).Sort(keys, vals);
+        __syncthreads();
+    }
+    {
+        uint64_t keys[ITEMS];
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) keys[j] = (vals[j] < n) ? I.key0[vals[j]] : 0x3FFFFFFFFull;
+        FusedSort64<ITEMS>(*reinterpret_cast<typename FusedSort64<ITEMS>::TempStorage*>(&tmp))
+            .Sort(keys, vals, 0, 34);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int pos = t * ITEMS + j;
+        if (pos < n) I.perm[pos] = vals[j];
+    }
+}
 
 // Classification, lexicographic order, sorted objectives, dup positions and
 // peel state of one instance per CTA: the stages of run_ndsort up to the
@@ -1632,24 +1678,15 @@ fused_lexsort(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
         }
         __syncthreads();  // the shared storage is reused below
     } else {
-    for (int m = M - 1; m >= 1; --m) {
-        uint32_t keys[kFusedItems];
+        if (n <= 2 * kFusedThreads) fused_lex_passes<2>(I, pop, n, M, tmp);
+        else if (n <= 4 * kFusedThreads) fused_lex_passes<4>(I, pop, n, M, tmp);
+        else fused_lex_passes<kFusedItems>(I, pop, n, M, tmp);
+        __syncthreads();  // the permutation in I.perm, written by every thread
 #pragma unroll
         for (int j = 0; j < kFusedItems; ++j) {
-            const int pt = vals[j];
-            keys[j] = (pt < n) ? (((I.key0[pt] >> 32) == 0) ? float_order_key(pop.obj(m, pt)) : 0u)
-                               : 0xFFFFFFFFu;
+            const int pos = t * kFusedItems + j;
+            vals[j] = (pos < n) ? I.perm[pos] : pos;
         }
-        FusedSort32(tmp.s32).Sort(keys, vals);
-        __syncthreads();
-    }
-    {
-        uint64_t keys[kFusedItems];
-#pragma unroll
-        for (int j = 0; j < kFusedItems; ++j) keys[j] = (vals[j] < n) ? I.key0[vals[j]] : 0x3FFFFFFFFull;
-        FusedSort64(tmp.s64).Sort(keys, vals, 0, 34);
-        __syncthreads();
-    }
     }
 #pragma unroll
     for (int j = 0; j < kFusedItems; ++j) {

@@ -951,10 +951,15 @@ int sm_count(int device)
 // fused batch: selection stages of every instance, one launch per stage
 // ---------------------------------------------------------------------------
 
-using FusedSortK64 = cub::BlockRadixSort<uint64_t, kFusedThreads, kFusedItems, int>;
+// Block sorts of the last front's members with 2, 4 or 8 items per thread:
+// the smallest that holds the front (the sort's work grows with the items).
+template <int ITEMS>
+using FusedSortK64 = cub::BlockRadixSort<uint64_t, kFusedThreads, ITEMS, int>;
 using FusedScanInt = cub::BlockScan<int, kFusedThreads>;
 union FusedSelStorage {
-    typename FusedSortK64::TempStorage sort;
+    typename FusedSortK64<2>::TempStorage sort2;
+    typename FusedSortK64<4>::TempStorage sort4;
+    typename FusedSortK64<kFusedItems>::TempStorage sort8;
     typename FusedScanInt::TempStorage scan;
 };
 
@@ -1106,23 +1111,75 @@ fused_assoc(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
 // Run starts of the sorted keys (by direction index, the high word) into
 // rs[] for this thread's items at positions < n; the keys are staged in
 // `stage`, which holds n entries.
-__device__ __forceinline__ void fused_run_starts(const uint64_t (&keys)[kFusedItems], uint64_t* stage, int n,
-                                                 FusedScanInt::TempStorage& tmp, int (&rs)[kFusedItems])
+template <int ITEMS>
+__device__ __forceinline__ void fused_run_starts(const uint64_t (&keys)[ITEMS], uint64_t* stage, int n,
+                                                 FusedScanInt::TempStorage& tmp, int (&rs)[ITEMS])
 {
     const int t = threadIdx.x;
 #pragma unroll
-    for (int j = 0; j < kFusedItems; ++j)
-        if (t * kFusedItems + j < n) stage[t * kFusedItems + j] = keys[j];
+    for (int j = 0; j < ITEMS; ++j)
+        if (t * ITEMS + j < n) stage[t * ITEMS + j] = keys[j];
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < kFusedItems; ++j) {
-        const int pos = t * kFusedItems + j;
+    for (int j = 0; j < ITEMS; ++j) {
+        const int pos = t * ITEMS + j;
         const bool h = pos < n &&
                        (pos == 0 || (uint32_t)(keys[j] >> 32) != (uint32_t)(stage[pos - 1] >> 32));
         rs[j] = h ? pos : 0;
     }
     FusedScanInt(tmp).InclusiveScan(rs, rs, cub::Max());
     __syncthreads();
+}
+
+// The three niching stages of a last front of nl > kFusedThreads members as
+// stable block sorts with ITEMS keys per thread (ITEMS * kFusedThreads >= nl).
+template <int ITEMS>
+__device__ __forceinline__ void fused_niching_sorted(const BatchInst& I, FusedSelStorage& tmp, int np, int nl,
+                                                     int nrem, int H, unsigned long long off)
+{
+    using Sort = FusedSortK64<ITEMS>;
+    typename Sort::TempStorage& sort_tmp = *reinterpret_cast<typename Sort::TempStorage*>(&tmp);
+    const int t = threadIdx.x;
+    uint64_t keys[ITEMS];
+    int vals[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int p = t * ITEMS + j;
+        keys[j] = (p < nl) ? (((uint64_t)(uint32_t)I.assoc_idx[np + p] << 32) |
+                              __float_as_uint(I.assoc_dist[np + p]))
+                           : ~0ull;
+        vals[j] = p;
+    }
+    __syncthreads();  // rho complete
+    for (int stage = 1; stage <= 3; ++stage) {
+        Sort(sort_tmp).Sort(keys, vals);
+        __syncthreads();
+        if (stage == 3) break;
+        int rs[ITEMS];
+        fused_run_starts<ITEMS>(keys, I.key64, I.n, tmp.scan, rs);
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const int p = t * ITEMS + j;
+            if (p >= nl) continue;
+            const uint32_t ref = (uint32_t)(keys[j] >> 32);
+            const int r_i = (int)ref;
+            const int rho_r = (r_i >= 0 && r_i < H) ? I.rho[r_i] : 0;
+            const int rank = p - rs[j];
+            if (stage == 1) {
+                const uint32_t rnd = splitmix_u32(off + (uint64_t)p, I.nich_seed);
+                const uint32_t low = (rho_r == 0 && rank == 0) ? 0u : (rnd | 1u);
+                keys[j] = ((uint64_t)ref << 32) | low;
+            } else {
+                const uint32_t rnd = splitmix_u32(off + (uint64_t)nl + (uint64_t)p, I.nich_seed);
+                keys[j] = ((uint64_t)(uint32_t)(rho_r + rank) << 32) | rnd;
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const int i = t * ITEMS + j;
+        if (i < nrem && i < nl) I.selected[np + i] = I.nds_gidx[np + vals[j]];
+    }
 }
 
 // Niche selection of one instance per CTA: run_niching with block sorts.
@@ -1204,47 +1261,12 @@ fused_niching(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
             __syncthreads();
         }
         if (t < nrem && t < nl) I.selected[np + t] = I.nds_gidx[np + s_val[cur * kFusedThreads + t]];
+    } else if (nl <= 2 * kFusedThreads) {
+        fused_niching_sorted<2>(I, tmp, np, nl, nrem, H, off);
+    } else if (nl <= 4 * kFusedThreads) {
+        fused_niching_sorted<4>(I, tmp, np, nl, nrem, H, off);
     } else {
-    uint64_t keys[kFusedItems];
-    int vals[kFusedItems];
-#pragma unroll
-    for (int j = 0; j < kFusedItems; ++j) {
-        const int p = t * kFusedItems + j;
-        keys[j] = (p < nl) ? (((uint64_t)(uint32_t)I.assoc_idx[np + p] << 32) |
-                              __float_as_uint(I.assoc_dist[np + p]))
-                           : ~0ull;
-        vals[j] = p;
-    }
-    __syncthreads();  // rho complete
-    for (int stage = 1; stage <= 3; ++stage) {
-        FusedSortK64(tmp.sort).Sort(keys, vals);
-        __syncthreads();
-        if (stage == 3) break;
-        int rs[kFusedItems];
-        fused_run_starts(keys, I.key64, I.n, tmp.scan, rs);
-#pragma unroll
-        for (int j = 0; j < kFusedItems; ++j) {
-            const int p = t * kFusedItems + j;
-            if (p >= nl) continue;
-            const uint32_t ref = (uint32_t)(keys[j] >> 32);
-            const int r_i = (int)ref;
-            const int rho_r = (r_i >= 0 && r_i < H) ? I.rho[r_i] : 0;
-            const int rank = p - rs[j];
-            if (stage == 1) {
-                const uint32_t rnd = splitmix_u32(off + (uint64_t)p, I.nich_seed);
-                const uint32_t low = (rho_r == 0 && rank == 0) ? 0u : (rnd | 1u);
-                keys[j] = ((uint64_t)ref << 32) | low;
-            } else {
-                const uint32_t rnd = splitmix_u32(off + (uint64_t)nl + (uint64_t)p, I.nich_seed);
-                keys[j] = ((uint64_t)(uint32_t)(rho_r + rank) << 32) | rnd;
-            }
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < kFusedItems; ++j) {
-        const int i = t * kFusedItems + j;
-        if (i < nrem && i < nl) I.selected[np + i] = I.nds_gidx[np + vals[j]];
-    }
+        fused_niching_sorted<kFusedItems>(I, tmp, np, nl, nrem, H, off);
     }
     if (t == 0) *I.offset = off + 2ull * (unsigned long long)nl;
 }
