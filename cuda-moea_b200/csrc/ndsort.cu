@@ -50,7 +50,7 @@ constexpr int kTileThreads = 256;
 constexpr int kPeelThreads = 1024;
 constexpr int kScanQueue = 1024;   // rows per CTA and front for the chunked scan
 constexpr int kProbeWords = 16;    // row words probed below an assigned blocker
-constexpr int kScanChunk = 256;    // words per chunk (8 per lane)
+constexpr int kScanChunk = 512;    // words per chunk (16 per lane)
 constexpr uint32_t kInfeasibleBit = 0x80000000u;
 
 // ---------------------------------------------------------------------------
