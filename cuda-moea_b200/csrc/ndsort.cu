@@ -859,7 +859,7 @@ nds_peel(const uint32_t* __restrict__ rows, int W, int n, int target, const int*
 // When every warp of the grid owns at most one group of 32 positions
 // (n <= 32 * 32 * CTAs), a lane keeps its point's state across the fronts:
 // the blocker in a register and a window of at least kWin row words (the
-// blocker's word and those below it) in shared memory, as five aligned
+// blocker's word and those below it) in shared memory, as three aligned
 // 16-byte chunks.  The window is refilled with cp.async whenever fewer than
 // kWin of its words lie at or below the blocker, so the copy lands while the
 // grid waits at the barrier and the next front's probe reads only shared
@@ -871,8 +871,8 @@ nds_peel(const uint32_t* __restrict__ rows, int W, int n, int target, const int*
 // count is needed.  A CTA can run at most one front ahead of the slowest, so
 // the word of front k holds only fronts k, k-2, ... when it is read.
 
-constexpr int kWin = 16;       // row words cached per lane at and below its blocker
-constexpr int kWinChunks = 5;  // 16-byte chunks of a window: 20 words from a multiple of 4
+constexpr int kWin = 8;        // row words cached per lane at and below its blocker
+constexpr int kWinChunks = 3;  // 16-byte chunks of a window: 12 words from a multiple of 4
 constexpr unsigned long long kPeelWaitNs = 2000000000ull;  // limit of one barrier wait
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
