@@ -5,8 +5,8 @@
 // Same result (front index per point, -1 past the stop rule, index of the last
 // front), different mechanism:
 //
-//  1. Sort of the points by (class, f0 | cv, S) with one 64-bit radix sort,
-//     S the top 30 bits of the order key of the FP32 sum f1 + ... + f_{M-1}.
+//  1. Sort of the points by (class, f0 | cv, S) with one 56-bit radix sort,
+//     S the top 22 bits of the order key of the FP32 sum f1 + ... + f_{M-1}.
 //     Class 0 = feasible, 1 = feasible with a NaN objective, 2 = infeasible,
 //     3 = infeasible with NaN violation.  FP32 addition rounds monotonically,
 //     so a feasible dominator p of q has f0(p) <= f0(q) and S(p) <= S(q); runs
@@ -52,13 +52,22 @@ constexpr int kScanQueue = 1024;   // rows per CTA and front for the chunked sca
 constexpr int kProbeWords = 16;    // row words probed below an assigned blocker
 constexpr int kScanChunk = 512;    // words per chunk (16 per lane)
 constexpr uint32_t kInfeasibleBit = 0x80000000u;
+// Sort key: class (2 bits), the order key of f0 or of the violation (32
+// bits), the top kSortSBits bits of the order key of S.  22 bits of S keep
+// runs of equal keys as rare as 30 did while saving a radix pass; with 14
+// the runs grew and the tie fix-up cost more than the pass it saved.
+constexpr int kSortSBits = 22;
+constexpr int kSortKeyBits = 2 + 32 + kSortSBits;
+constexpr int kSortClassShift = 32 + kSortSBits;
 
 // ---------------------------------------------------------------------------
 // 1. classification and lexicographic sort
 // ---------------------------------------------------------------------------
 
 // key0[i] = class << 32 | order key of f0 (class 0) or cv (class 2);
-// skey[i] = class << 62 | that key << 30 | S (class 0), the sort key.
+// skey[i] = class << 54 | that key << 22 | S (class 0), the sort key of
+// kSortKeyBits bits (seven radix passes of 8 bits), S the top 22 bits of the
+// order key of the FP32 sum f1 + ... + f_{M-1}.
 __global__ void nds_classify(SplitPop pop, int M, uint64_t* __restrict__ key0, uint64_t* __restrict__ skey,
                              int* __restrict__ perm, int* __restrict__ feasible_count)
 {
@@ -83,7 +92,7 @@ __global__ void nds_classify(SplitPop pop, int M, uint64_t* __restrict__ key0, u
             if (cls == 2u) val = float_order_key(cv);
         }
         key0[i] = ((uint64_t)cls << 32) | val;
-        skey[i] = ((uint64_t)cls << 62) | ((uint64_t)val << 30) | s30;
+        skey[i] = ((uint64_t)cls << kSortClassShift) | ((uint64_t)val << kSortSBits) | (s30 >> (30 - kSortSBits));
         perm[i] = i;
         feasible_class = cls <= 1u;
         infeasible2 = cls == 2u;
@@ -125,7 +134,7 @@ __global__ void nds_tie_fix(SplitPop pop, int M, const uint64_t* __restrict__ sk
     const int n = pop.n;
     if (pos >= n) return;
     const uint64_t k = skey[pos];
-    if ((k >> 62) != 0u || (pos > 0 && skey[pos - 1] == k)) return;
+    if ((k >> kSortClassShift) != 0u || (pos > 0 && skey[pos - 1] == k)) return;
     int L = 1;
     while (L <= kTieShort && pos + L < n && skey[pos + L] == k) ++L;
     if (L == 1) return;
@@ -2004,7 +2013,7 @@ int run_ndsort(Workspace& ws, const SplitPop& pop, int M, int target, int* out_f
     const uint64_t* key0 = ws.key0;
     size_t tmp = ws.cub_bytes;
     MOEA_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws.cub_tmp, tmp, ws.key64[0], ws.key64[1], ws.perm[0],
-                                                  ws.perm[1], n, 0, 64, stream));
+                                                  ws.perm[1], n, 0, kSortKeyBits, stream));
     // runs of equal keys in class 0 into lexicographic order; ws.run_start
     // holds the list of long runs until the dup scan below overwrites it
     nds_tie_fix<<<G, T, 0, stream>>>(pop, M, ws.key64[1], ws.perm[1], ws.run_start, ws.counters + 13);
