@@ -49,7 +49,7 @@ N_POP, D_VAR, M_OBJ, PARTITIONS = 32768, 7, 3, 254
 ROWS_DRAM_BYTES = 5.80e6 + 217.07e6
 # dram__bytes_read.sum + dram__bytes_write.sum of one nds_peel_owned launch at
 # this workload (one ncu --set full capture of the launch)
-PEEL_DRAM_BYTES = 132.83e6 + 3.92e6
+PEEL_DRAM_BYTES = 134.72e6 + 3.56e6
 # l1tex__data_pipe_lsu_wavefronts of one nds_block_rows launch at this
 # workload (shared-memory loads and stores 24.15e6, global row stores and
 # table copies the rest): the work of the unit that bounds the kernel
