@@ -54,6 +54,9 @@ PEEL_DRAM_BYTES = 134.72e6 + 3.56e6
 # workload (shared-memory loads and stores 24.15e6, global row stores and
 # table copies the rest): the work of the unit that bounds the kernel
 ROWS_LSU_WAVEFRONTS = 29.17e6
+# smsp__inst_executed.sum of the same launch: warp instructions, 32 lane-ops
+# each, for its n(n-1)/2 pair tests
+ROWS_WARP_INSTR = 86.95e6
 
 
 def _peaks():
@@ -128,7 +131,9 @@ def kernel_rooflines(stage_ms: dict, n_mix: int, headline: bool):
       by the LSU data pipe (shared-memory tree descents and prefix-set reads,
       row stores), so against that pipe's peak of one wavefront per SM and
       clock (148 SMs x max SM clock), with ROWS_LSU_WAVEFRONTS per launch;
-      the pair tests/s and the HBM fraction on the rows written go beside it.
+      the pair tests/s, the HBM fraction on the rows written and the fraction
+      of the SIMT lane-op peak (148 SMs x 128 lanes x max SM clock) at the
+      kernel's counted lane-ops per pair go beside it.
     """
     hbm, peak_kind = _peaks()
     tri_pairs = n_mix * (n_mix - 1) / 2
@@ -148,6 +153,8 @@ def kernel_rooflines(stage_ms: dict, n_mix: int, headline: bool):
                     "unit": "LSU wavefronts/s", "frac": a / lsu_peak,
                     "peak_source": "148 SMs x 1 LSU data-pipe wavefront/clk x 1965 MHz",
                     "pair_tests_per_s": tri_pairs / (tiles / 1e3),
+                    "lane_ops_per_pair": ROWS_WARP_INSTR * 32 / tri_pairs,
+                    "simt_frac": tri_pairs / (tiles / 1e3) * (ROWS_WARP_INSTR * 32 / tri_pairs) / (148 * 128 * 1.965e9),
                     "algorithmic_bytes": rel_bytes, "hbm_frac": rel_bytes / (tiles / 1e3) / 1e9 / hbm,
                     "traffic": ROWS_DRAM_BYTES, "ms": tiles})
     out.sort(key=lambda r: -r["ms"])
