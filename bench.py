@@ -20,7 +20,8 @@ The default line also carries `rvea_large_d` (RVEA DTLZ2 M=8 D=131072 N=1024,
 Other workloads (--workload): dtlz2-small (N=92), rvea-large-d (D=131072),
 c1dtlz1-m10 and constrained-batch (ten objectives, 275 two-layer
 directions, 64 seeds per batched launch), dtlz2-m8 (tensor-core
-association).
+association), dtlz1-h255 (the headline configuration with 255 partitions,
+32896 directions).
 
 `--impl reference` times the CPU restatement of the reference path (oracle/)
 on the host cores, same metric and workload (the reference itself has no CPU
@@ -483,6 +484,11 @@ OTHER_WORKLOADS = {
     "c1dtlz1-m10": dict(desc="constrained NSGA-III C1-DTLZ1 M=10 D=14 N=16384, two-layer (3,2) user "
                              "directions (275), 100-generation run",
                         algo="NSGA3", problem=("C1DTLZ1", 14, 10), N=16384, T=100, dirs=("two", 3, 2)),
+    # the headline configuration's other reading: 255 partitions give the
+    # 32896 directions its description quotes (254 give 32640)
+    "dtlz1-h255": dict(desc="NSGA-III DTLZ1 M=3 D=7 N=32768, Das-Dennis 255 partitions (32896 directions), "
+                            "50-generation run",
+                       algo="NSGA3", problem=("DTLZ1", 7, 3), N=32768, T=50, dirs=("dd", 255)),
     # many objectives: the default association is the tensor-core search here
     "dtlz2-m8": dict(desc="NSGA-III DTLZ2 M=8 D=17 N=6436, Das-Dennis H=8 (6435 directions), 100-generation run",
                      algo="NSGA3", problem=("DTLZ2", 17, 8), N=6436, T=100, dirs=("dd", 8)),
@@ -570,7 +576,7 @@ def measure_workload(name, steps, warmup, seed, torch, cm):
            "config": {"workload": w["desc"], "cuda_graph": graph_on, "kernels_per_generation": kernels,
                       "l2": "flushed (256 MiB write) before every timed generation"},
            "clocks": clocks.summary()}
-    if name in ("dtlz2-m8", "c1dtlz1-m10"):
+    if name in ("dtlz2-m8", "c1dtlz1-m10", "dtlz1-h255"):
         out["stages_ms"] = dict(algo.profile_step())
     if name == "rvea-large-d":
         # the generation's streamed bytes, 8 N D: the variation reads two
