@@ -1140,6 +1140,7 @@ BatchInst fused_describe(moea_algorithm* a, int P, int X)
     b.front_list = w.front_list; b.counters = w.counters; b.rows = w.rows; b.chunk_keys = w.chunk_keys;
     b.chunk_bits = w.chunk_bits; b.fronts = w.fronts; b.nds_gidx = w.nds_gidx; b.sizes = w.sizes;
     b.nds_objs = w.nds_objs; b.rcp_b = w.rcp_b; b.extreme = w.extreme; b.assoc_idx = w.assoc_idx;
+    b.assoc_best = w.assoc_best;
     b.assoc_dist = w.assoc_dist; b.rho = w.rho; b.selected = w.selected; b.flags = w.flags;
     b.survivors = a->survivors; b.offset = w.offset_dev;
     b.t_dirs_orig = a->refs;
@@ -1166,11 +1167,12 @@ int fused_build_group(const std::vector<moea_algorithm*>& inst, const std::vecto
     MOEA_CUDA_TRY(cudaMemcpy(g.d_ids, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
     for (int m = 1; m <= kMaxObjectives; ++m) {
         std::vector<int> bids, prefix{0};
-        int mn = 0;
+        int mn = 0, mh = 0;
         const int shape = tile_shape ? tile_shape[m] : 0;
         for (int i : ids) {
             if (inst[i]->M != m) continue;
             bids.push_back(i);
+            mh = std::max(mh, inst[i]->H);
             const int n = 2 * inst[i]->N;
             prefix.push_back(prefix.back() + fused_tile_blocks(m, n, shape));
             mn = std::max(mn, n);
@@ -1182,6 +1184,7 @@ int fused_build_group(const std::vector<moea_algorithm*>& inst, const std::vecto
         b.max_n = mn;
         b.tile_blocks = prefix.back();
         b.shape = shape;
+        b.max_H = mh;
         MOEA_CUDA_TRY(cudaMalloc((void**)&b.d_ids, sizeof(int) * bids.size()));
         MOEA_CUDA_TRY(cudaMalloc((void**)&b.d_tile_prefix, sizeof(int) * prefix.size()));
         MOEA_CUDA_TRY(cudaMemcpy(b.d_ids, bids.data(), sizeof(int) * bids.size(), cudaMemcpyHostToDevice));

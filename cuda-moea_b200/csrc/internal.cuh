@@ -279,6 +279,7 @@ struct BatchInst {
     uint32_t* rows; uint32_t* chunk_keys; uint32_t* chunk_bits;
     int* fronts; int* nds_gidx; int* sizes; float* nds_objs; float* rcp_b; int* extreme;
     int* assoc_idx; float* assoc_dist; int* rho; int* selected; int* flags; int* survivors;
+    unsigned long long* assoc_best;  // packed (d2 bits, index) minima of a direction-split scan
     unsigned long long* offset;
     const float* t_dirs_orig;  // (M, H) directions in their own order
     const float* t_dirs; const int* t_order; const float* t_center; const float* t_cos;
@@ -289,6 +290,7 @@ struct BatchInst {
 struct FusedBucket {
     int M = 0, count = 0, max_n = 0, tile_blocks = 0;
     int shape = 0;                 // dominance tile shape (fused_tile_blocks)
+    int max_H = 0;                 // most directions of an instance
     int* d_ids = nullptr;          // (count) instance indices
     int* d_tile_prefix = nullptr;  // (count + 1) first tile block of each instance
 };

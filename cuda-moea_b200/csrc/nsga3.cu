@@ -1099,6 +1099,44 @@ fused_scan(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
                         I.t_delta, nullptr, I.assoc_idx, I.assoc_dist);
 }
 
+// The same scan with the directions split into `splits` ranges (blockIdx.z),
+// merged through the packed (d2 bits, index) minimum as in the staged path;
+// fused_scan_reset before it, fused_scan_finish after.  An instance's scan
+// then runs on `splits` times the CTAs: within one fused generation the
+// instances of a group run side by side and each stage lasts as long as its
+// slowest instance, so the long scans of the many-direction instances are
+// split rather than run by one thread per point over every direction.
+template <int M>
+__global__ void __launch_bounds__(kAssocThreads)
+fused_scan_split(const BatchInst* __restrict__ insts, const int* __restrict__ ids, int splits)
+{
+    const BatchInst& I = insts[ids[blockIdx.y]];
+    assoc_scan_block<M>(blockIdx.x, blockIdx.z, I.nds_objs, I.n_max, I.rcp_b, I.t_dirs_orig, I.H, I.sizes[3],
+                        (I.H + splits - 1) / splits, I.t_delta, I.assoc_best, nullptr, nullptr);
+}
+
+__global__ void fused_scan_reset(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    const BatchInst& I = insts[ids[blockIdx.y]];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < I.sizes[3]) I.assoc_best[i] = ~0ull;
+}
+
+__global__ void fused_scan_finish(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    const BatchInst& I = insts[ids[blockIdx.y]];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= I.sizes[3]) return;
+    const unsigned long long b = I.assoc_best[i];
+    if (b == ~0ull) {
+        I.assoc_idx[i] = -1;
+        I.assoc_dist[i] = INFINITY;
+    } else {
+        I.assoc_idx[i] = (int)(unsigned)(b & 0xFFFFFFFFull);
+        I.assoc_dist[i] = sqrtf(__uint_as_float((unsigned)(b >> 32)));
+    }
+}
+
 template <int M>
 __global__ void __launch_bounds__(kTreeWarps * 32)
 fused_assoc(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
@@ -1663,6 +1701,26 @@ int fused_select_configure()
     return MOEA_OK;
 }
 
+// Association of a bucket of M > kTreeMaxObjectives instances: one thread
+// per point over every direction, or, above kFusedScanSplitLen directions,
+// the direction-split scan (at most kFusedScanMaxSplits ranges).
+constexpr int kFusedScanSplitLen = 1024;
+constexpr int kFusedScanMaxSplits = 8;
+
+template <int M>
+void fused_scan_launch(const BatchInst* d_inst, const FusedBucket& b, cudaStream_t s)
+{
+    const int splits = std::min(kFusedScanMaxSplits, std::max(1, ceil_div(b.max_H, kFusedScanSplitLen)));
+    const dim3 grid(ceil_div(b.max_n, kAssocThreads), b.count);
+    if (splits == 1) {
+        fused_scan<M><<<grid, kAssocThreads, 0, s>>>(d_inst, b.d_ids);
+        return;
+    }
+    fused_scan_reset<<<grid, kAssocThreads, 0, s>>>(d_inst, b.d_ids);
+    fused_scan_split<M><<<dim3(grid.x, grid.y, splits), kAssocThreads, 0, s>>>(d_inst, b.d_ids, splits);
+    fused_scan_finish<<<grid, kAssocThreads, 0, s>>>(d_inst, b.d_ids);
+}
+
 int fused_select(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s)
 {
     const int sort_smem = (int)sizeof(FusedSelStorage);
@@ -1675,8 +1733,7 @@ int fused_select(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s)
                 fused_assoc<K><<<dim3(ceil_div(b.max_n, kTreeWarps), b.count), kTreeWarps * 32, 0,    \
                                  s>>>(d_inst, b.d_ids);                                              \
             else                                                                                     \
-                fused_scan<K><<<dim3(ceil_div(b.max_n, kAssocThreads), b.count), kAssocThreads, 0,    \
-                                s>>>(d_inst, b.d_ids);                                               \
+                fused_scan_launch<K>(d_inst, b, s);                                                  \
             break;
         MOEA_FP_CASE(1) MOEA_FP_CASE(2) MOEA_FP_CASE(3) MOEA_FP_CASE(4)
         MOEA_FP_CASE(5) MOEA_FP_CASE(6) MOEA_FP_CASE(7) MOEA_FP_CASE(8)
