@@ -406,7 +406,7 @@ def batched_measure(args, torch, cm, world: int = 1, rank: int = 0):
     rate is all instances over the slowest rank's time."""
     all_specs = batch_specs(args.batch_instances)
     specs = [all_specs[i] for i in shard_instances(all_specs, world, rank)]
-    T = 200
+    T = args.batch_generations
 
     def make(spec):
         kind, M, N, D, seed = spec
@@ -423,7 +423,7 @@ def batched_measure(args, torch, cm, world: int = 1, rank: int = 0):
         return [e0.elapsed_time(e1) for e0, e1 in ev]
 
     t0 = time.perf_counter()
-    batch = cm.Batch([make(s) for s in specs], autotune=True)
+    batch = cm.Batch([make(s) for s in specs], autotune=not args.batch_default_schedule)
     tune_s = time.perf_counter() - t0
     torch.cuda.synchronize()
     batch_ms = timed_run(batch.step, batch.stream)
@@ -449,6 +449,8 @@ def batched_measure(args, torch, cm, world: int = 1, rank: int = 0):
     windows = {}
     for name, (lo, hi) in (("generations 1-5", (0, 5)), ("generations 96-100", (95, 100)),
                            ("generations 196-200", (195, 200))):
+        if hi > T:
+            continue
         b = over_ranks(sum(batch_ms[lo:hi]), "max", world, "cuda")
         p = over_ranks(sum(plain_ms[lo:hi]), "max", world, "cuda")
         windows[name] = {"instance_gen_per_s": n * (hi - lo) / (b / 1e3),
@@ -741,6 +743,10 @@ def main() -> None:
     ap.add_argument("--cpu-budget", type=float, default=40.0)
     ap.add_argument("--batch-instances", type=int, default=256)
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-generations", type=int, default=200,
+                    help="generations of the batched record (fewer only for launch-list captures)")
+    ap.add_argument("--batch-default-schedule", action="store_true",
+                    help="the batch's default schedule instead of the autotuned one (launch-list captures)")
     ap.add_argument("--no-precision", action="store_true", help="skip the association-search comparison")
     ap.add_argument("--no-rvea", action="store_true", help="skip the RVEA large-D record")
     ap.add_argument("--workload", default="dtlz1-n32768",
