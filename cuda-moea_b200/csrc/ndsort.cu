@@ -64,10 +64,23 @@ constexpr int kSortClassShift = 32 + kSortSBits;
 // 1. classification and lexicographic sort
 // ---------------------------------------------------------------------------
 
+// Sort key of point i of class cls with key0 low word val: class << 54 |
+// val << 22 | S (class 0), kSortKeyBits bits (seven radix passes of 8 bits),
+// S the top 22 bits of the order key of the FP32 sum f1 + ... + f_{M-1}
+// (monotone in every f_m; +inf + -inf (NaN) sorts with +inf sums).
+__device__ __forceinline__ uint64_t sort_key(const SplitPop& pop, int M, int i, uint32_t cls, uint32_t val)
+{
+    uint32_t s30 = 0;
+    if (cls == 0u) {
+        float sum = 0.0f;
+        for (int m = 1; m < M; ++m) sum = __fadd_rn(sum, pop.obj(m, i));
+        s30 = float_order_key(isnan(sum) ? INFINITY : sum) >> 2;
+    }
+    return ((uint64_t)cls << kSortClassShift) | ((uint64_t)val << kSortSBits) | (s30 >> (30 - kSortSBits));
+}
+
 // key0[i] = class << 32 | order key of f0 (class 0) or cv (class 2);
-// skey[i] = class << 54 | that key << 22 | S (class 0), the sort key of
-// kSortKeyBits bits (seven radix passes of 8 bits), S the top 22 bits of the
-// order key of the FP32 sum f1 + ... + f_{M-1}.
+// skey[i] = sort_key(i).
 __global__ void nds_classify(SplitPop pop, int M, uint64_t* __restrict__ key0, uint64_t* __restrict__ skey,
                              int* __restrict__ perm, int* __restrict__ feasible_count)
 {
@@ -75,24 +88,18 @@ __global__ void nds_classify(SplitPop pop, int M, uint64_t* __restrict__ key0, u
     bool feasible_class = false, infeasible2 = false, infeasible3 = false;
     if (i < pop.n) {
         const float cv = pop.cvv(i);
-        uint32_t cls, val = 0, s30 = 0;
+        uint32_t cls, val = 0;
         if (cv == 0.0f) {
             bool nan = false;
             for (int m = 0; m < M; ++m) nan |= isnan(pop.obj(m, i));
             cls = nan ? 1u : 0u;
-            if (!nan) {
-                val = float_order_key(pop.obj(0, i));
-                // monotone in every f_m; +inf + -inf (NaN) sorts with +inf sums
-                float sum = 0.0f;
-                for (int m = 1; m < M; ++m) sum = __fadd_rn(sum, pop.obj(m, i));
-                s30 = float_order_key(isnan(sum) ? INFINITY : sum) >> 2;
-            }
+            if (!nan) val = float_order_key(pop.obj(0, i));
         } else {
             cls = isnan(cv) ? 3u : 2u;
             if (cls == 2u) val = float_order_key(cv);
         }
         key0[i] = ((uint64_t)cls << 32) | val;
-        skey[i] = ((uint64_t)cls << kSortClassShift) | ((uint64_t)val << kSortSBits) | (s30 >> (30 - kSortSBits));
+        skey[i] = sort_key(pop, M, i, cls, val);
         perm[i] = i;
         feasible_class = cls <= 1u;
         infeasible2 = cls == 2u;
@@ -1557,63 +1564,130 @@ void launch_tiles(const Workspace& ws, int n, cudaStream_t stream)
 // Block sorts with 2, 4 or 8 items per thread: the smallest that holds the
 // instance (the sort's work grows with the items).
 template <int ITEMS>
-using FusedSort32 = cub::BlockRadixSort<uint32_t, kFusedThreads, ITEMS, int>;
-template <int ITEMS>
 using FusedSort64 = cub::BlockRadixSort<uint64_t, kFusedThreads, ITEMS, int>;
 using FusedScan = cub::BlockScan<int, kFusedThreads>;
 union FusedSortStorage {
-    typename FusedSort32<kFusedItems>::TempStorage s32;
     typename FusedSort64<kFusedItems>::TempStorage s64;
-    typename FusedSort32<4>::TempStorage s32_4;
     typename FusedSort64<4>::TempStorage s64_4;
-    typename FusedSort32<2>::TempStorage s32_2;
     typename FusedSort64<2>::TempStorage s64_2;
     typename FusedScan::TempStorage scan;
+    int list[kFusedThreads + 4];  // long runs of fused_lex_onekey
 };
 
-// The stable LSD passes of fused_lexsort (objectives M-1 .. 1 for class 0,
-// then class and f0) with ITEMS keys per thread (ITEMS * kFusedThreads >= n);
-// the permutation goes to I.perm[0 .. n).  Items beyond n carry keys above
-// every real key and stay behind the real ones.
+// The order of fused_lexsort for n > kFusedThreads, as the staged path
+// builds it: one block radix sort of the sort keys (sort_key) with ITEMS keys
+// per thread, then each run of equal keys in class 0 put in lexicographic
+// order (f1 .. f_{M-1}, index) -- runs of up to kTieShort points by one
+// thread each (insertion sort), longer ones (when not already in order) by the
+// whole CTA, each member counting the members that precede it.  One sort of
+// kSortKeyBits bits replaces M-1 stable passes of 32 bits and one of 34.  The
+// permutation goes to I.perm[0 .. n); I.key64 holds the sorted keys and
+// I.vals serves the long runs as scratch.
 template <int ITEMS>
-__device__ __forceinline__ void fused_lex_passes(const BatchInst& I, const SplitPop& pop, int n, int M,
+__device__ __forceinline__ void fused_lex_onekey(const BatchInst& I, const SplitPop& pop, int n, int M,
                                                  FusedSortStorage& tmp)
 {
     const int t = threadIdx.x;
+    uint64_t keys[ITEMS];
     int vals[ITEMS];
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j) vals[j] = t * ITEMS + j;
-    for (int m = M - 1; m >= 1; --m) {
-        uint32_t keys[ITEMS];
-#pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            const int pt = vals[j];
-            keys[j] = (pt < n) ? (((I.key0[pt] >> 32) == 0) ? float_order_key(pop.obj(m, pt)) : 0u)
-                               : 0xFFFFFFFFu;
+    for (int j = 0; j < ITEMS; ++j) {
+        const int pt = t * ITEMS + j;
+        vals[j] = pt;
+        if (pt < n) {
+            const uint64_t k0 = I.key0[pt];
+            keys[j] = sort_key(pop, M, pt, (uint32_t)(k0 >> 32), (uint32_t)k0);
+        } else {
+            keys[j] = (1ull << kSortKeyBits) - 1ull;  // above every real key
         }
-        FusedSort32<ITEMS>(*reinterpret_cast<typename FusedSort32<ITEMS>::TempStorage*>(&tmp)).Sort(keys, vals);
-        __syncthreads();
     }
-    {
-        uint64_t keys[ITEMS];
-#pragma unroll
-        for (int j = 0; j < ITEMS; ++j) keys[j] = (vals[j] < n) ? I.key0[vals[j]] : 0x3FFFFFFFFull;
-        FusedSort64<ITEMS>(*reinterpret_cast<typename FusedSort64<ITEMS>::TempStorage*>(&tmp))
-            .Sort(keys, vals, 0, 34);
-        __syncthreads();
-    }
+    FusedSort64<ITEMS>(*reinterpret_cast<typename FusedSort64<ITEMS>::TempStorage*>(&tmp))
+        .Sort(keys, vals, 0, kSortKeyBits);
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const int pos = t * ITEMS + j;
-        if (pos < n) I.perm[pos] = vals[j];
+        if (pos < n) {
+            I.key64[pos] = keys[j];
+            I.perm[pos] = vals[j];
+        }
+    }
+    __syncthreads();
+    const uint64_t* K = I.key64;
+    int* P = I.perm;
+    // short runs, one thread per run head
+    for (int pos = t; pos < n; pos += kFusedThreads) {
+        const uint64_t k = K[pos];
+        if ((k >> kSortClassShift) != 0u || (pos > 0 && K[pos - 1] == k)) continue;
+        int L = 1;
+        while (L <= kTieShort && pos + L < n && K[pos + L] == k) ++L;
+        if (L == 1 || L > kTieShort) continue;
+        for (int a = pos + 1; a < pos + L; ++a) {
+            const int v = P[a];
+            int b = a - 1;
+            while (b >= pos && tie_less(pop, M, v, P[b])) {
+                P[b + 1] = P[b];
+                --b;
+            }
+            P[b + 1] = v;
+        }
+    }
+    __syncthreads();
+    // long runs, one after another by the whole CTA (the sort storage is free)
+    int* s_heads = reinterpret_cast<int*>(&tmp);
+    int* s_misc = s_heads + kFusedThreads;  // [0] heads, [1] run end, [2] out of order
+    for (int base = 0; base < n; base += kFusedThreads) {
+        if (t == 0) s_misc[0] = 0;
+        __syncthreads();
+        const int pos = base + t;
+        if (pos < n) {
+            const uint64_t k = K[pos];
+            if ((k >> kSortClassShift) == 0u && (pos == 0 || K[pos - 1] != k) && pos + kTieShort < n &&
+                K[pos + kTieShort] == k)
+                s_heads[atomicAdd(s_misc, 1)] = pos;
+        }
+        __syncthreads();
+        const int nh = s_misc[0];
+        for (int h = 0; h < nh; ++h) {
+            const int head = s_heads[h];
+            const uint64_t k = K[head];
+            if (t == 0) {
+                s_misc[1] = n;
+                s_misc[2] = 0;
+            }
+            __syncthreads();
+            for (int a = head + 1 + t; a < n; a += kFusedThreads)
+                if (K[a] != k) {
+                    atomicMin(s_misc + 1, a);
+                    break;
+                }
+            __syncthreads();
+            const int end = s_misc[1];
+            for (int a = head + 1 + t; a < end; a += kFusedThreads)
+                if (tie_less(pop, M, P[a], P[a - 1])) s_misc[2] = 1;
+            __syncthreads();
+            if (s_misc[2]) {
+                for (int a = head + t; a < end; a += kFusedThreads) {
+                    const int v = P[a];
+                    int r = 0;
+                    for (int b = head; b < end; ++b) r += tie_less(pop, M, P[b], v) ? 1 : 0;
+                    I.vals[head + r] = v;
+                }
+                __syncthreads();
+                for (int a = head + t; a < end; a += kFusedThreads) P[a] = I.vals[a];
+            }
+            __syncthreads();
+        }
     }
 }
 
-// Classification, lexicographic order, sorted objectives, dup positions and
-// peel state of one instance per CTA: the stages of run_ndsort up to the
-// dominance rows, with the same stable LSD passes (objectives M-1..1, then
-// class and f0) done by block radix sorts.  Items beyond n carry keys above
-// every real key and stay behind the real ones.
+// Classification, sorted order, sorted objectives, dup positions and peel
+// state of one instance per CTA: the stages of run_ndsort up to the
+// dominance rows.  Instances of more than kFusedThreads points take the
+// staged path's order (fused_lex_onekey); smaller ones count ranks under the
+// lexicographic order (class and f0, f1 .. f_{M-1}, index).  Either order
+// has what the rows and the peel need (dominators first, identical vectors
+// adjacent, f0 non-decreasing in class 0), and the fronts depend on the
+// relation only.
 __global__ void __launch_bounds__(kFusedThreads)
 fused_lexsort(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
 {
@@ -1687,9 +1761,9 @@ fused_lexsort(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
         }
         __syncthreads();  // the shared storage is reused below
     } else {
-        if (n <= 2 * kFusedThreads) fused_lex_passes<2>(I, pop, n, M, tmp);
-        else if (n <= 4 * kFusedThreads) fused_lex_passes<4>(I, pop, n, M, tmp);
-        else fused_lex_passes<kFusedItems>(I, pop, n, M, tmp);
+        if (n <= 2 * kFusedThreads) fused_lex_onekey<2>(I, pop, n, M, tmp);
+        else if (n <= 4 * kFusedThreads) fused_lex_onekey<4>(I, pop, n, M, tmp);
+        else fused_lex_onekey<kFusedItems>(I, pop, n, M, tmp);
         __syncthreads();  // the permutation in I.perm, written by every thread
 #pragma unroll
         for (int j = 0; j < kFusedItems; ++j) {
