@@ -1178,6 +1178,11 @@ __device__ __forceinline__ void fused_niching_sorted(const BatchInst& I, FusedSe
     using Sort = FusedSortK64<ITEMS>;
     typename Sort::TempStorage& sort_tmp = *reinterpret_cast<typename Sort::TempStorage*>(&tmp);
     const int t = threadIdx.x;
+    // The high words are direction indices (< H) or niche counts plus ranks
+    // (< n); padding keys are all ones.  Bits above the largest of them are
+    // zero in every real key, so the sorts stop below them.
+    const unsigned hi_max = (unsigned)max(H, I.n);
+    const int end_bit = 32 + (32 - __clz(hi_max)) + 1;
     uint64_t keys[ITEMS];
     int vals[ITEMS];
 #pragma unroll
@@ -1190,7 +1195,7 @@ __device__ __forceinline__ void fused_niching_sorted(const BatchInst& I, FusedSe
     }
     __syncthreads();  // rho complete
     for (int stage = 1; stage <= 3; ++stage) {
-        Sort(sort_tmp).Sort(keys, vals);
+        Sort(sort_tmp).Sort(keys, vals, 0, end_bit);
         __syncthreads();
         if (stage == 3) break;
         int rs[ITEMS];
