@@ -1688,8 +1688,8 @@ __device__ __forceinline__ void fused_lex_onekey(const BatchInst& I, const Split
 // has what the rows and the peel need (dominators first, identical vectors
 // adjacent, f0 non-decreasing in class 0), and the fronts depend on the
 // relation only.
-__global__ void __launch_bounds__(kFusedThreads)
-fused_lexsort(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+template <bool kLarge>
+__device__ __forceinline__ void fused_lexsort_body(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
 {
     extern __shared__ __align__(16) unsigned char fused_smem[];
     FusedSortStorage& tmp = *reinterpret_cast<FusedSortStorage*>(fused_smem);
@@ -1761,14 +1761,16 @@ fused_lexsort(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
         }
         __syncthreads();  // the shared storage is reused below
     } else {
-        if (n <= 2 * kFusedThreads) fused_lex_onekey<2>(I, pop, n, M, tmp);
-        else if (n <= 4 * kFusedThreads) fused_lex_onekey<4>(I, pop, n, M, tmp);
-        else fused_lex_onekey<kFusedItems>(I, pop, n, M, tmp);
-        __syncthreads();  // the permutation in I.perm, written by every thread
+        if constexpr (kLarge) {
+            if (n <= 2 * kFusedThreads) fused_lex_onekey<2>(I, pop, n, M, tmp);
+            else if (n <= 4 * kFusedThreads) fused_lex_onekey<4>(I, pop, n, M, tmp);
+            else fused_lex_onekey<kFusedItems>(I, pop, n, M, tmp);
+            __syncthreads();  // the permutation in I.perm, written by every thread
 #pragma unroll
-        for (int j = 0; j < kFusedItems; ++j) {
-            const int pos = t * kFusedItems + j;
-            vals[j] = (pos < n) ? I.perm[pos] : pos;
+            for (int j = 0; j < kFusedItems; ++j) {
+                const int pos = t * kFusedItems + j;
+                vals[j] = (pos < n) ? I.perm[pos] : pos;
+            }
         }
     }
 #pragma unroll
@@ -1827,6 +1829,29 @@ fused_lexsort(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
         for (int c = 1; c <= 4; ++c) I.counters[c] = 0;
     }
 }
+
+__global__ void __launch_bounds__(kFusedThreads)
+fused_lexsort(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    fused_lexsort_body<true>(insts, ids);
+}
+
+// Groups whose instances all have at most kFusedThreads points: the same
+// body without the block sorts, a much smaller kernel (its instances are
+// launch- and latency-bound, and the sort code around the counting path
+// slowed them by 9%).
+__global__ void __launch_bounds__(kFusedThreads)
+fused_lexsort_small(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
+{
+    fused_lexsort_body<false>(insts, ids);
+}
+
+// Shared memory of fused_lexsort_small: the counting path's keys and
+// permutation, or the block scan's storage.
+constexpr int kFusedLexSmallSmem =
+    (int)(kFusedThreads * (sizeof(uint64_t) + sizeof(int)) > sizeof(FusedScan::TempStorage)
+              ? kFusedThreads * (sizeof(uint64_t) + sizeof(int))
+              : sizeof(FusedScan::TempStorage));
 
 __global__ void fused_chunks(const BatchInst* __restrict__ insts, const int* __restrict__ ids)
 {
@@ -2289,7 +2314,10 @@ int fused_ndsort_configure()
 int fused_ndsort(const BatchInst* d_inst, const FusedGroup& g, cudaStream_t s)
 {
     const int sort_smem = (int)sizeof(FusedSortStorage);
-    fused_lexsort<<<g.count, kFusedThreads, sort_smem, s>>>(d_inst, g.d_ids);
+    if (g.max_n <= kFusedThreads)
+        fused_lexsort_small<<<g.count, kFusedThreads, kFusedLexSmallSmem, s>>>(d_inst, g.d_ids);
+    else
+        fused_lexsort<<<g.count, kFusedThreads, sort_smem, s>>>(d_inst, g.d_ids);
     MOEA_CUDA_TRY(cudaGetLastError());
     if (g.max_M > 1) {
         const int warps = ceil_div(g.max_n, 32) * (g.max_M - 1);
